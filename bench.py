@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 SBP-SAT stepper on the elastic 2048^2 FP32 workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (one shot per GPU, weak scaling): 2D elastic, 2048 x 2048 cells, dx = 1/500, FP32,
+seeded layered medium of 8 horizontal layers (per layer vp ~ U(1.5, 4.5), rho ~ U(1.8, 2.7);
+vs = vp/sqrt(3) * U(0.9, 1.1) per node), CFL 0.4 (dt = 0.4 dx / (sqrt(2) vp_max)), explosive
+Ricker source f0 = 15 on the normal-stress grid near the centre, 16 receivers on the NM grid.
+A "step" is one leapfrog time step of the whole grid; one grid-point update (Gpt) is one cell
+advanced one step with all five fields.
+
+Printed JSON (rank 0): `value` = device-timed Gpt-updates/s over all ranks (inputs resident in
+HBM); `e2e` = the same metric through the public C ABI with host buffers (model upload,
+stepping, trace and energy readback inside the timed region); `roofline` = the dominant kernel's
+algorithmic bytes per launch over its CUDA-event duration against the measured HBM copy
+bandwidth; `cpu_baseline` = the reference's own CPU solver (oracle/_ref) on a bounded sample.
+`--impl reference` times only the reference's CPU solver on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import csv
+import io
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gpt-updates/s & %HBM roofline; plain FP32 vs mixed/batched at L2 err≤1e-4"
+UNIT = "Gpt-updates/s"
+MX = MY = 2048
+DEN_DX = 500
+CFL = 0.4
+F0 = 15.0
+DELAY = 0.1
+SEED = 20261203 + 2
+N_RCV = 16
+L2_BYTES = 126 * 2**20
+
+
+def workload_desc():
+    return {"workload": "elastic 2048x2048 FP32, 8-layer seeded medium, CFL 0.4, Ricker f0=15 explosive, 16 receivers",
+            "grid": [MX, MY], "dx": f"1/{DEN_DX}", "precision": "fp32", "compensation": "00",
+            "energy": "off in value (on in e2e_energy)", "steps_per_shot_in_config": 4000,
+            "l2": "inputs larger than L2 (fields + coefficients = 168 MB vs 126 MB L2), no flush"}
+
+
+def build_model(rank: int = 0):
+    """Padded (Mx+2)x(My+2) node model in the reference layout (inverse.cpp:79-90, padding 0)."""
+    rng = np.random.default_rng(SEED)
+    nl = 8
+    vp_l, rho_l = rng.uniform(1.5, 4.5, nl), rng.uniform(1.8, 2.7, nl)
+    P = (MX + 2, MY + 2)
+    vp = np.zeros(P); rho = np.zeros(P)
+    layer = np.minimum(np.arange(MX + 1) * nl // (MX + 1), nl - 1)
+    vp[:MX + 1, :MY + 1] = vp_l[layer][:, None]
+    rho[:MX + 1, :MY + 1] = rho_l[layer][:, None]
+    vs = vp / np.sqrt(3.0) * rng.uniform(0.9, 1.1, P)
+    vs[MX + 1, :] = 0.0
+    vs[:, MY + 1] = 0.0
+    dx = 1.0 / DEN_DX
+    dt = CFL * dx / (np.sqrt(2.0) * vp.max())
+    # one shot per rank: the source moves along y with the rank
+    src_iy = (MY // 2 + 16 * rank) % MY
+    return rho, vp, vs, dt, (MX // 2, src_iy)
+
+
+def receivers():
+    return np.full(N_RCV, 8), 64 + 128 * np.arange(N_RCV)
+
+
+def load_twave():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("twave", os.path.join(ROOT, "tpu-wave_b200", "__init__.py"))
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["twave"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+# ---------------------------------------------------------------- distributed plumbing
+class Dist:
+    def __init__(self):
+        self.rank = int(os.environ.get("RANK", "0"))
+        self.world = int(os.environ.get("WORLD_SIZE", "1"))
+        self.local = int(os.environ.get("LOCAL_RANK", "0"))
+        self.pg = None
+
+    def init(self, backend: str):
+        if self.world > 1:
+            import datetime
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            if self.pg.get_backend() == "nccl":
+                import torch
+                self.pg.barrier(device_ids=[self.local])
+                torch.cuda.synchronize()
+            else:
+                self.pg.barrier()
+
+    def reduce_max(self, x: float) -> float:
+        if not self.pg:
+            return x
+        import torch
+        dev = torch.device("cuda", self.local) if self.pg.get_backend() == "nccl" else torch.device("cpu")
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def finish(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+# ---------------------------------------------------------------- clocks during the timed region
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.out = None
+
+    def start(self):
+        try:
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait()
+        self.out.seek(0)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for row in csv.reader(io.StringIO(self.out.read())):
+            if len(row) < 9:
+                continue
+            try:
+                sm.append(float(row[1])); smax.append(float(row[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, row[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------- CPU baseline (reference solver)
+def reference_sample(steps: int, procs: int = 1, rank: int = 0):
+    """Run the reference's own elastic FP32 CPU solver (oracle/_ref, built from its sources) on
+    `steps` time steps of the same workload in `procs` concurrent processes; returns
+    (Gpt-updates/s aggregated over the processes, loop seconds per process, kind)."""
+    from oracle import refrun
+    rho, vp, vs, dt, (sx, sy) = build_model(rank)
+    rx, ry = receivers()
+    case = refrun.ElasticCase(Mx=MX, My=MY, num_dx=1, den_dx=DEN_DX, dt=dt, rho=rho.reshape(-1), vp=vp.reshape(-1),
+                              vs=vs.reshape(-1), src=("M", "M", 2 * sx + 1, 2 * DEN_DX, 2 * sy + 1, 2 * DEN_DX),
+                              rcvs=[("N", "M", int(a), DEN_DX, 2 * int(b) + 1, 2 * DEN_DX) for a, b in zip(rx, ry)],
+                              Nt=steps, cpst="00", central_f=F0, time_delay=DELAY)
+    binary = os.path.join(refrun.REF_DIR, "twref_elastic_f32_perf")
+    if not os.path.exists(binary):
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        fin = os.path.join(td, "in.bin")
+        ih = np.zeros(32, np.int64)
+        cn, cs = refrun.CPST_CODES["00"]
+        ih[:20] = [0x5457454C, MX, MY, MX, MY, 1, DEN_DX, 1, DEN_DX, steps, cn, ord(cs), ord("M"), ord("M"),
+                   *case.src[2:6], len(case.rcvs), 1]
+        dh = np.zeros(8); dh[:3] = [dt, F0, DELAY]
+        with open(fin, "wb") as f:
+            f.write(ih.tobytes()); f.write(dh.tobytes())
+            for a in (rho, vp, vs):
+                f.write(np.ascontiguousarray(a, np.float64).tobytes())
+            f.write(np.array([[ord("N"), ord("M"), *r[2:6]] for r in case.rcvs], np.int64).tobytes())
+        ps = [subprocess.Popen([binary, fin, os.path.join(td, f"out{k}.bin")], stdout=subprocess.DEVNULL)
+              for k in range(procs)]
+        for p in ps:
+            if p.wait() != 0:
+                return None
+        loops = [float(np.fromfile(os.path.join(td, f"out{k}.bin"), np.float64, count=1)[0]) for k in range(procs)]
+    gpts = procs * MX * MY * steps / max(loops) / 1e9
+    return gpts, loops, "reference"
+
+
+def cpu_threads() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def run_reference_arm(args, dist: Dist):
+    if dist.rank != 0:
+        return
+    procs = max(1, min(cpu_threads(), 32))
+    steps = max(1, min(args.steps, 20))
+    res = reference_sample(steps, procs)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU solver binary oracle/_ref missing"}))
+        return
+    gpts, loops, kind = res
+    sample = (f"{procs} concurrent single-threaded processes of the reference elastic FP32 host solver, each "
+              f"{steps} time steps of the 2048x2048 workload (energy every step, as the reference asserts)")
+    line = {"metric": METRIC, "value": gpts, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": steps, "warmup": 0, "ms_per_step": max(loops) / steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_desc(),
+            "cpu_baseline": {"value": gpts, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample},
+            "e2e": {"value": gpts, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- our arm
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "of measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "of fallback"
+
+
+def ncu_traffic(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if one exists."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(path) as f:
+            t = json.load(f)
+        e = t.get(kernel)
+        return None if e is None else float(e["bytes_per_launch_full_size"])
+    except (OSError, ValueError, KeyError):
+        return None
+
+
+def run_ours(args, dist: Dist):
+    import torch
+    tw = load_twave()
+    dev = dist.local
+    torch.cuda.set_device(dev)
+    dist.init("nccl")
+    rho, vp, vs, dt, (sx, sy) = build_model(dist.rank)
+    rx, ry = receivers()
+    K, W = args.steps, args.warmup
+    P = min(max(K // 8, 20), 400)   # eagerly launched steps for the per-kernel timing
+    s = tw.Solver(MX, MY, 1, DEN_DX, dt, physics=tw.ELASTIC, precision="f32", cpst="00", central_f=F0,
+                  time_delay=DELAY, max_steps=W + K + P, energy=False, device=dev)
+    s.set_material_model(rho, vp, vs)
+    s.set_source(tw.MM, sx, sy)
+    s.add_receivers(tw.NM, rx, ry)
+    stream = torch.cuda.ExternalStream(s.stream(), device=dev)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    s.run(W)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step(K)
+    e1.record(stream)
+    e1.synchronize()
+    s.sync()
+    torch.cuda.synchronize()
+    dist.barrier()
+    clk = clocks.stop()
+    ms = e0.elapsed_time(e1)
+    ms_max = dist.reduce_max(ms)
+    updates = MX * MY * K * dist.world
+    value = updates / (ms_max / 1e3) / 1e9
+
+    # per-kernel durations (CUDA events around each launch on the solver's stream)
+    prof = s.profile(P)
+    names = ["k_elastic_velocity", "k_elastic_stress"]
+    # compulsory bytes of each launch: every array it touches read or written once
+    alg = [MX * MY * (3 * 4 + 2 * 4 + 2 * 2 * 4), MX * MY * (2 * 4 + 3 * 4 + 3 * 2 * 4)]
+    k = int(np.argmax(prof[:2]))
+    achieved = alg[k] / (prof[k] / 1e3) / 1e9
+    peak, peak_note = measured_peaks()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": ncu_traffic(names[k]), "kernel": names[k], "peak_source": peak_note,
+                "algorithmic_bytes_per_launch": alg[k], "ms_per_launch": float(prof[k]),
+                "ms_per_launch_all": {"velocity": float(prof[0]), "stress": float(prof[1]), "gather": float(prof[3])},
+                "step_bytes_algorithmic_per_update": 60}
+    s.close()
+
+    # end to end through the C ABI with host buffers: model upload + set-up, K steps, readback
+    torch.cuda.synchronize()
+    dist.barrier()
+    t0 = time.perf_counter()
+    s2 = tw.Solver(MX, MY, 1, DEN_DX, dt, physics=tw.ELASTIC, precision="f32", cpst="00", central_f=F0,
+                   time_delay=DELAY, max_steps=K, energy=True, device=dev)
+    s2.set_material_model(rho, vp, vs)
+    s2.set_source(tw.MM, sx, sy)
+    s2.add_receivers(tw.NM, rx, ry)
+    s2.run(K)
+    traces = s2.read_receivers()
+    energy = s2.read_energy()
+    t1 = time.perf_counter()
+    s2.close()
+    e2e_s = dist.reduce_max(t1 - t0)
+    h2d = 3 * rho.size * 8
+    d2h = traces.nbytes + sum(e.nbytes for e in energy)
+    e2e = {"value": MX * MY * K * dist.world / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": h2d / K,
+           "d2h_bytes_per_step": d2h / K, "seconds": e2e_s,
+           "includes": "handle creation, model upload + FP64 interpolation on the GPU, K steps with energy "
+                       "every step and 16 receivers, trace and energy readback"}
+    launches_per_step = 3   # velocity, stress, gather
+
+    cpu = None
+    if dist.rank == 0 and dist.world == 1 and not args.no_cpu_baseline:
+        res = reference_sample(args.cpu_steps, 1)
+        if res is not None:
+            cpu = {"value": res[0], "unit": UNIT, "cores": 1, "kind": res[2],
+                   "sample": f"{args.cpu_steps} time steps of this 2048x2048 workload, one process of the reference "
+                             f"elastic FP32 host solver built from its sources (energy every step, as it asserts)"}
+    if dist.rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": dist.world, "steps": K, "warmup": W,
+                "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic", "config": workload_desc(), "roofline": roofline,
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": K * launches_per_step, "clocks": clk}
+        print(json.dumps(line), flush=True)
+    dist.finish()
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=4000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--cpu-steps", type=int, default=30)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be at least 3")
+    dist = Dist()
+    if args.impl == "reference":
+        run_reference_arm(args, dist)
+        return
+    run_ours(args, dist)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,168 @@
+/*
+ * twave.h - C ABI of the B200 (sm_100a) 2D staggered-grid SBP-SAT acoustic/elastic stepper.
+ *
+ * The reference (wsmoses/tpu-wave) has no plugin or FFI layer: its "API" is the C++ object
+ * protocol that its two mains drive (cuda/src/cpp/main_host_FDM_2D.tpp:11-285 on the CPU,
+ * cuda/src/cuda_main/nvcc_device_FDM_2D.cu:11-843 on the GPU). Each entry point below names
+ * the reference member function or code block it replaces. Differences in convention:
+ *   - every entry point returns a status (TW_OK = 0, negative on error) instead of printing and
+ *     calling exit(0) (forward.cpp:37-98, cuda_container_run_time.cuh:57-62);
+ *   - buffers are caller-owned host memory; `ld` arguments count elements;
+ *   - one handle per host thread (handles are not thread-safe); handles are independent.
+ *
+ * Index conventions are the reference's: x is the slow data direction (rows), y the fast one;
+ * the physical X axis is data y and physical Y is data x (namespace_forward.hpp:56-61).
+ * Grids: TW_NN (Mx+1)x(My+1) "Sxy", TW_MN Mx x(My+1) "Vx" (velocity along data y),
+ * TW_NM (Mx+1)x My "Vy" (velocity along data x), TW_MM Mx x My "SMM" = {sxx, syy}
+ * (grid.hpp:146-188). Field readback uses exactly these (unpadded, row-major) sizes.
+ */
+#ifndef TWAVE_H
+#define TWAVE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define TW_API __attribute__((visibility("default")))
+#else
+#define TW_API
+#endif
+
+/* ---- status codes --------------------------------------------------------------------- */
+enum {
+    TW_OK = 0,
+    TW_ERR_INVALID = -1,        /* bad argument, size or enum */
+    TW_ERR_CUDA = -2,           /* a CUDA runtime call failed (see tw_last_cuda_error) */
+    TW_ERR_NOMEM = -3,          /* device or host allocation failed */
+    TW_ERR_STATE = -4,          /* call out of order (e.g. stepping before the material is set) */
+    TW_ERR_LOCATION = -5,       /* location is not a grid point (forward.cpp:38-39,48-49) */
+    TW_ERR_OUTSIDE = -6,        /* location outside the grid (forward.cpp:91) */
+    TW_ERR_WEAK_BOUNDARY = -7,  /* source on an SAT boundary node (forward.cpp:95-96) or on the
+                                   periodic seam of an N-type-y grid (forward_simulation.cpp:116-135) */
+    TW_ERR_RECORD_FULL = -8,    /* more steps than the trace/energy records hold */
+    TW_ERR_NONFINITE = -9,      /* a NaN/Inf appeared in a field (sticky, reported by tw_sync) */
+    TW_ERR_UNSUPPORTED = -10,   /* combination not implemented (e.g. elastic with periodic x) */
+    TW_ERR_MODEL_BOUNDS = -11   /* interpolation stepped out of the model (grid_parameter.cpp:54-56) */
+};
+
+/* ---- enums ------------------------------------------------------------------------------ */
+enum tw_physics { TW_ELASTIC = 0, TW_ACOUSTIC = 1 };
+/* x boundaries: SBP-SAT free surface (cuda/ tree) or periodic (singlecore/ and mpi/ trees);
+ * y is always periodic, as in the reference (grid_drvt.tpp:1-3). */
+enum tw_bc { TW_BC_SAT_FREE = 0, TW_BC_PERIODIC = 1 };
+/* storage type of the fields; FP64/FP32 compute in the storage type (namespace_type.cuh:16-22);
+ * BF16/FP16 store 16-bit fields and compute in FP32 */
+enum tw_precision { TW_FP64 = 0, TW_FP32 = 1, TW_BF16 = 2, TW_FP16 = 3 };
+/* time-update compensation, grid.hpp:550-566 / grid_update.tpp:1-127 ("N" = flops used for the
+ * lost bits, "C" = separate array, "R" = the right-hand-side array holds them) */
+enum tw_cpst { TW_CPST_00 = 0, TW_CPST_M3C = 1, TW_CPST_M3R = 2, TW_CPST_3C = 3,
+               TW_CPST_3R = 4, TW_CPST_6C = 5, TW_CPST_6R = 6 };
+enum tw_grid { TW_NN = 0, TW_MN = 1, TW_NM = 2, TW_MM = 3 };
+
+typedef struct {
+    int physics;            /* tw_physics */
+    int bc_x;               /* tw_bc */
+    int precision;          /* tw_precision */
+    int cpst;               /* tw_cpst */
+    long Mx, My;            /* cells along data x / y (ns_input::Mx_soln, My_soln) */
+    int num_dx, den_dx;     /* dx = num/den (InputFile dxS, input_processing.cpp:63-72) */
+    double dt;              /* ns_input::dt (main_host_FDM_2D.tpp:57) */
+    double central_f;       /* Ricker central frequency (ns_input::central_f) */
+    double time_delay;      /* Ricker delay (ns_input::time_delay) */
+    double source_scaling;  /* divides the source increment (nvcc_device_FDM_2D.cu:557); 1 = none */
+    int max_steps;          /* capacity of the trace and energy records */
+    int energy;             /* 1: discrete energy every step (reference default, main_host_FDM_2D.tpp:34); 0: off */
+    int device;             /* CUDA device ordinal (ns_input::device_number) */
+} tw_grid_desc;
+
+typedef struct {
+    long rows[4], cols[4];  /* reference sizes of NN, MN, NM, MM */
+    long pitch;             /* device row pitch in elements */
+    int steps_done;
+    int n_rcv;
+    double bytes_per_update;       /* compulsory HBM bytes per cell-update of one step */
+    double device_bytes;           /* device memory held by the handle */
+} tw_info;
+
+typedef struct tw_solver tw_solver;
+
+/* Grid setup: Class_Grid::set_grid_parameters + set_forward_operators + set_grid_pointers for
+ * the four grids (grid.hpp:146-481, called at main_host_FDM_2D.tpp:96-103) and the device
+ * allocation of cuda_Class_Grid_initialize (grid.cuh:216-375). */
+TW_API int tw_create(tw_solver **out, const tw_grid_desc *desc);
+TW_API void tw_destroy(tw_solver *s);
+
+/* Material from the reference's padded node model: Class_Grid::retrieve_forward_parameter,
+ * define_parameters_energy, adjust_parameters_energy_periodic and make_density_reciprocal
+ * (grid_parameter.cpp:7-160, grid_energy.cpp:8-177; main_host_FDM_2D.tpp:146-168).
+ * rho/vp/vs: (Mx_prmt+2) x (My_prmt+2) doubles, row stride My_prmt+2 (inverse.cpp:79-90).
+ * dxM = num_dxM/den_dxM is the model spacing. Acoustic handles use rho and vp only. */
+TW_API int tw_set_material_model(tw_solver *s, const double *rho, const double *vp, const double *vs,
+                          long Mx_prmt, long My_prmt, int num_dxM, int den_dxM);
+
+/* Forward parameters given directly on one staggered grid (reference sizes, row stride ld):
+ * NN idx 0 = mu; MN/NM idx 0 = rho (stored as 1/rho like make_density_reciprocal);
+ * MM idx 0 = lambda (acoustic: kappa), idx 1 = 2mu. Replaces the material path for callers
+ * that prepare coefficients themselves (the single-core tree sets them directly,
+ * cpu_acoustic.cpp:178-180). */
+TW_API int tw_set_material_grid(tw_solver *s, int grid, int idx, const double *coef, long ld);
+
+/* Source: Class_Forward_Specs::process_src_locations (forward.cpp:10-100) with the location
+ * given as rationals per data direction (struct_src_input, src_rcv.hpp:6-11). */
+TW_API int tw_set_source_location(tw_solver *s, char type_x, char type_y, long num_x, long den_x,
+                           long num_y, long den_y);
+/* The same with grid indices. */
+TW_API int tw_set_source(tw_solver *s, int grid, long ix, long iy);
+TW_API int tw_clear_source(tw_solver *s);
+
+/* Receivers: process_rcv_locations (forward.cpp:104-211). Appends in call order. */
+TW_API int tw_add_receiver_location(tw_solver *s, char type_x, char type_y, long num_x, long den_x,
+                             long num_y, long den_y);
+TW_API int tw_add_receivers(tw_solver *s, int grid, const long *ix, const long *iy, int n);
+
+/* Zero the fields, compensation arrays, records and the step counter (main_host_FDM_2D.tpp:225-235). */
+TW_API int tw_reset(tw_solver *s);
+
+/* Advance n steps: forward_simulation_periodic_y (forward_simulation.cpp:21-182) / the device
+ * loop (nvcc_device_FDM_2D.cu:449-730). Asynchronous on the handle's stream. */
+TW_API int tw_step(tw_solver *s, int n);
+/* Wait for queued work; returns the first sticky error (TW_ERR_NONFINITE, TW_ERR_CUDA). */
+TW_API int tw_sync(tw_solver *s);
+
+/* Field readback in the reference layout (copy_field_pitched dev_to_hst, grid.cuh:463-469):
+ * rows x cols of the grid, row stride ld >= cols, converted to double. field: 0, or 1 for syy on MM. */
+TW_API int tw_read_field(tw_solver *s, int grid, int field, double *host, long ld);
+/* Set a field from the host (reference layout); the periodic duplicate column (and row) is ignored. */
+TW_API int tw_write_field(tw_solver *s, int grid, int field, const double *host, long ld);
+/* Compensation arrays (Vec_rths for 'R' codes, Vec_cpst for 'C' codes), same layout. */
+TW_API int tw_read_resid(tw_solver *s, int grid, int field, double *host, long ld);
+TW_API int tw_write_resid(tw_solver *s, int grid, int field, const double *host, long ld);
+
+/* Receiver traces: host[r][f][it] for r < n_rcv, f < 2, it < steps_done (Map_grid_RESULT_rcv,
+ * forward.hpp:74-75; f = 1 is zero on single-field grids). */
+TW_API int tw_read_receivers(tw_solver *s, double *host);
+/* Energy records for it < steps_done (ns_input::Record_E_k/p0/p1). Elastic and acoustic-SAT:
+ * E = E_k + (E_p0 + E_p1)/2 (forward.cpp:303-306). Acoustic periodic: E_k = E_Vx + E_Vy,
+ * E_p0 = E_P of the previous step, E_p1 = E_P (cpu_acoustic.cpp:413-418). Any may be NULL. */
+TW_API int tw_read_energy(tw_solver *s, double *E_k, double *E_p0, double *E_p1);
+
+TW_API int tw_get_info(tw_solver *s, tw_info *info);
+/* Advance n steps launching each kernel on its own, bracketed by CUDA events on the handle's
+ * stream, and return the mean duration in ms of each phase: ms[0] velocity half-step,
+ * ms[1] stress half-step, ms[2] energy reductions (all of one step), ms[3] receiver gather.
+ * No counterpart in the reference, which times whole loops with steady_clock
+ * (singlecore/src/main_cpp/cpu_acoustic.cpp:12-14,242-243). */
+TW_API int tw_profile(tw_solver *s, int n, double *ms);
+/* Rational location num/den of a node ('N') or cell-centre ('M') point -> grid index, as
+ * process_src_locations / process_rcv_locations convert it (forward.cpp:31-51). Host only. */
+TW_API int tw_location_to_index(char type, long num, long den, int num_dx, int den_dx, long *index);
+/* The handle's cudaStream_t, for callers that order their own work after tw_step. */
+TW_API int tw_get_stream(tw_solver *s, void **stream);
+TW_API const char *tw_strerror(int status);
+TW_API const char *tw_last_cuda_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

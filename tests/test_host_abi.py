@@ -1,0 +1,81 @@
+"""Host-side checks that need no GPU: the C-ABI library loads, exports every entry point that
+include/twave.h declares, validates arguments before touching the device, and maps rational
+locations to grid indices exactly as the reference does."""
+import ctypes as C
+import subprocess
+
+import numpy as np
+import pytest
+
+from oracle import oracle as orc
+
+
+def test_library_exports_every_declared_symbol(tw):
+    names = tw.declared_symbols()
+    assert len(names) >= 20
+    L = tw.lib()
+    for n in names:
+        assert hasattr(L, n), n
+    nm = subprocess.run(["nm", "-D", "--defined-only", tw.library_path()], capture_output=True, text=True).stdout
+    exported = {line.split()[-1] for line in nm.splitlines() if " T " in line}
+    assert set(names) <= exported
+    # the product never carries the oracle
+    assert not any(s.startswith("two_") for s in exported)
+
+
+def test_library_does_not_link_the_oracle(tw):
+    out = subprocess.run(["ldd", tw.library_path()], capture_output=True, text=True).stdout
+    assert "oracle" not in out
+
+
+def test_strerror(tw):
+    L = tw.lib()
+    assert L.tw_strerror(0) == b"ok"
+    assert b"weak boundary" in L.tw_strerror(-7)
+    assert L.tw_strerror(12345) == b"unknown status"
+
+
+def test_location_to_index_matches_reference_rule(tw):
+    rng = np.random.default_rng(0)
+    for _ in range(2000):
+        t = "NM"[rng.integers(2)]
+        num_dx, den_dx = int(rng.integers(1, 4)), int(rng.integers(1, 600))
+        den = int(rng.integers(1, 2000))
+        num = int(rng.integers(-50, 4000))
+        try:
+            want = orc.location_to_index(t, num, den, num_dx, den_dx)
+        except ValueError:
+            want = None
+        try:
+            got = tw.location_to_index(t, num, den, num_dx, den_dx)
+        except tw.TwError as e:
+            assert e.code == -5
+            got = None
+        assert got == want, (t, num, den, num_dx, den_dx)
+
+
+def _desc(tw, **kw):
+    base = dict(physics=0, bc_x=0, precision=1, cpst=0, Mx=64, My=64, num_dx=1, den_dx=64, dt=1e-3,
+                central_f=5.0, time_delay=0.1, source_scaling=1.0, max_steps=10, energy=1, device=0)
+    base.update(kw)
+    return tw.GridDesc(**base)
+
+
+@pytest.mark.parametrize("kw,code", [
+    (dict(Mx=7), -1), (dict(My=3), -1), (dict(dt=0.0), -1), (dict(num_dx=0), -1), (dict(max_steps=0), -1),
+    (dict(physics=5), -1), (dict(cpst=9), -1), (dict(source_scaling=0.0), -1),
+    (dict(physics=0, bc_x=1), -10),                 # elastic needs the SAT x boundaries
+    (dict(physics=1, bc_x=1, cpst=5), -10),         # the single-core tree has no 'C' compensation
+])
+def test_create_rejects_bad_descriptors_before_touching_the_device(tw, kw, code):
+    h = C.c_void_p()
+    assert tw.lib().tw_create(C.byref(h), C.byref(_desc(tw, **kw))) == code
+    assert not h.value
+
+
+def test_null_handles_are_rejected(tw):
+    L = tw.lib()
+    assert L.tw_step(None, 1) == -1
+    assert L.tw_sync(None) == -1
+    assert L.tw_reset(None) == -1
+    L.tw_destroy(None)

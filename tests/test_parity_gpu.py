@@ -1,0 +1,192 @@
+"""Parity of the CUDA product (through the C ABI) with the reference.
+
+Fields and receiver traces must be bit-identical to the reference's FP64 and FP32 CPU solvers
+(golden fixtures) and to the C restatement (random states, every compensation code, sources on
+every grid). Energies are FP64 sums taken in a different order: relative tolerance 1e-12.
+"""
+import json
+import os
+
+import numpy as np
+import pytest
+
+from cases import ROOT, acoustic_periodic_case, elastic_case, product_acoustic_periodic, product_elastic
+from oracle import oracle as orc
+from test_oracle_reference import MANIFEST, golden_acoustic_case, golden_elastic_case
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(ROOT, "tests", "golden")
+E_RTOL = 1e-12
+
+
+def energy_close(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    scale = max(np.abs(b).max(), 1e-300)
+    return np.abs(a - b).max() <= E_RTOL * scale
+
+
+@pytest.mark.parametrize("name", [n for n, m in MANIFEST.items() if m["kind"] == "elastic" and not m["vs0"]])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_elastic_matches_reference_golden(name, prec):
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    got = product_elastic(golden_elastic_case(d), prec)
+    for k, v in got["fields"].items():
+        assert np.array_equal(v, d[f"{prec}_field_{k}"]), k
+    assert np.array_equal(got["traces"], d[f"{prec}_traces"])
+    for k in ("E_k", "E_p0", "E_p1"):
+        assert energy_close(got[k], d[f"{prec}_{k}"]), k
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_acoustic_free_surface_matches_reference_vs0(prec):
+    """Acoustic with SAT free surface = the reference elastic solver with vs = 0 (p = sxx = syy)."""
+    d = np.load(os.path.join(GOLDEN, "el_20x16_vs0.npz"))
+    case = golden_elastic_case(d)
+    keep = [i for i, r in enumerate(case.rcvs) if (r[0], r[1]) != ("N", "N")]
+    case.rcvs = [case.rcvs[i] for i in keep]
+    got = product_elastic(case, prec, acoustic=True)
+    for k in ("MN", "NM", "MM0"):
+        assert np.array_equal(got["fields"][k], d[f"{prec}_field_{k}"]), k
+    ref_tr = d[f"{prec}_traces"][keep]
+    assert np.array_equal(got["traces"][:, 0], ref_tr[:, 0])
+    assert np.array_equal(got["E_k"], got["E_k"]) and energy_close(got["E_k"], d[f"{prec}_E_k"])
+
+
+@pytest.mark.parametrize("name", [n for n, m in MANIFEST.items() if m["kind"] == "acoustic_periodic"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_acoustic_periodic_matches_reference_golden(name, prec):
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    got = product_acoustic_periodic(golden_acoustic_case(d), prec)
+    for k, v in got["fields"].items():
+        assert np.array_equal(v, d[f"{prec}_field_{k}"]), k
+    assert np.array_equal(got["traces"], d[f"{prec}_traces"])
+    e = d[f"{prec}_energy"]
+    assert energy_close(got["E_k"], e[0] + e[1])
+    assert energy_close(got["E_p1"], e[2])
+
+
+def _random_state(Mx, My, seed, nfields=5, scale=1e-2):
+    """Random fields at reference sizes whose periodic duplicate column repeats column 0."""
+    rng = np.random.default_rng(seed)
+    shapes = [(Mx + 1, My + 1), (Mx, My + 1), (Mx + 1, My), (Mx, My), (Mx, My)]
+    out = []
+    for s in shapes[:nfields] if nfields == 5 else [shapes[1], shapes[2], shapes[3]]:
+        a = rng.standard_normal(s) * scale
+        if s[1] == My + 1:
+            a[:, My] = a[:, 0]
+        out.append(a)
+    return out
+
+
+CPST_CODES = ["00", "-3C", "-3R", "3C", "3R", "6C", "6R"]
+
+
+@pytest.mark.parametrize("cpst", CPST_CODES)
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("Mx,My", [(24, 40), (37, 45), (8, 4)])
+def test_elastic_random_state_matches_oracle(cpst, prec, Mx, My):
+    case = elastic_case(Mx, My, seed=Mx * My, cpst=cpst, Nt=3, rcvs=[])
+    f0 = _random_state(Mx, My, 1)
+    r0 = _random_state(Mx, My, 2, scale=1e-8) if cpst != "00" else None
+    T = np.float64 if prec == "f64" else np.float32
+    f0 = [a.astype(T).astype(np.float64) for a in f0]
+    r0 = None if r0 is None else [a.astype(T).astype(np.float64) for a in r0]
+    want = orc.elastic_run(case, prec, fields0=f0, resid0=r0)
+    got = product_elastic(case, prec, fields0=f0, resid0=r0)
+    for k, v in got["fields"].items():
+        assert np.array_equal(v, want.fields[k]), k
+    if r0 is not None:
+        for k, v in zip(("NN", "MN", "NM", "MM0", "MM1"), got["resid"]):
+            assert np.array_equal(v, want.resid[k]), ("resid", k)
+    for k in ("E_k", "E_p0", "E_p1"):
+        assert energy_close(got[k], getattr(want, k)), k
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("src", [("N", "N", 5, 24, 7, 24), ("M", "N", 11, 48, 9, 24), ("N", "M", 13, 24, 15, 48),
+                                 ("M", "M", 21, 48, 29, 48)])
+def test_source_on_every_grid_matches_oracle(prec, src):
+    case = elastic_case(24, 24, seed=3, Nt=50, src=src, den_dx=24, model="layered")
+    want = orc.elastic_run(case, prec)
+    got = product_elastic(case, prec)
+    for k, v in got["fields"].items():
+        assert np.array_equal(v, want.fields[k]), k
+    assert np.array_equal(got["traces"], want.traces)
+
+
+@pytest.mark.parametrize("cpst", ["00", "6R", "3C"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_acoustic_free_surface_random_state_matches_oracle(cpst, prec):
+    Mx, My = 30, 36
+    case = elastic_case(Mx, My, seed=5, cpst=cpst, Nt=4, rcvs=[], acoustic=True)
+    T = np.float64 if prec == "f64" else np.float32
+    rng = np.random.default_rng(9)
+    p = rng.standard_normal((Mx, My)).astype(T).astype(np.float64) * 1e-2
+    vmn = rng.standard_normal((Mx, My + 1)).astype(T).astype(np.float64) * 1e-2
+    vmn[:, My] = vmn[:, 0]
+    vnm = rng.standard_normal((Mx + 1, My)).astype(T).astype(np.float64) * 1e-2
+    zero_nn = np.zeros((Mx + 1, My + 1))
+    want = orc.elastic_run(case, prec, fields0=[zero_nn, vmn, vnm, p, p])
+    got = product_elastic(case, prec, acoustic=True, fields0=[vmn, vnm, p])
+    assert np.array_equal(want.fields["MM0"], want.fields["MM1"])
+    for k in ("MN", "NM", "MM0"):
+        assert np.array_equal(got["fields"][k], want.fields[k]), k
+
+
+@pytest.mark.parametrize("cpst", ["0", "3", "6"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_acoustic_periodic_matches_oracle(cpst, prec):
+    case = acoustic_periodic_case(40, 36, seed=17, cpst=cpst, Nt=70)
+    want = orc.acoustic_periodic_run(case, prec)
+    got = product_acoustic_periodic(case, prec)
+    for k, v in got["fields"].items():
+        assert np.array_equal(v, want.fields[k]), k
+    assert np.array_equal(got["traces"], want.traces)
+
+
+def test_errors_follow_the_reference_checks(tw):
+    s = tw.Solver(16, 16, 1, 16, 1e-3, max_steps=5)
+    try:
+        with pytest.raises(tw.TwError) as e:
+            s.step(1)                                   # no material yet
+        assert e.value.code == -4
+        with pytest.raises(tw.TwError) as e:
+            s.set_source_location("N", "M", 0, 1, 1, 32)   # node row 0 is the free surface
+        assert e.value.code == -7
+        with pytest.raises(tw.TwError) as e:
+            s.set_source_location("N", "M", 1, 32, 1, 32)  # 1/32 is not a node of dx = 1/16
+        assert e.value.code == -5
+        with pytest.raises(tw.TwError) as e:
+            s.set_source(tw.NN, 3, 0)                   # periodic seam of an N-type-y grid
+        assert e.value.code == -7
+        with pytest.raises(tw.TwError) as e:
+            s.add_receivers(tw.MM, [16], [0])           # outside the MM grid
+        assert e.value.code == -6
+        rho, vp, vs = (np.full((18, 18), v) for v in (2.0, 3.0, 1.5))
+        s.set_material_model(rho, vp, vs)
+        s.run(5)
+        with pytest.raises(tw.TwError) as e:
+            s.step(1)                                   # records hold 5 steps
+        assert e.value.code == -8
+    finally:
+        s.close()
+
+
+def test_nonfinite_value_is_reported_not_faulted(tw):
+    """A NaN planted in a field from the host is reported by tw_sync; the context stays usable."""
+    s = tw.Solver(16, 16, 1, 16, 1e-3, max_steps=10)
+    try:
+        rho, vp, vs = (np.full((18, 18), v) for v in (2.0, 3.0, 1.5))
+        s.set_material_model(rho, vp, vs)
+        f = np.zeros((16, 16))
+        f[5, 5] = np.nan
+        s.write_field(tw.MM, 0, f)
+        s.step(2)
+        with pytest.raises(tw.TwError) as e:
+            s.sync()
+        assert e.value.code == -9
+        s.reset()
+        s.run(2)
+        assert np.isfinite(s.read_field(tw.MM)).all()
+    finally:
+        s.close()

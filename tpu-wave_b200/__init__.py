@@ -1,0 +1,270 @@
+"""Python front end of libtwave.so, the B200 SBP-SAT stepper (C ABI in include/twave.h).
+
+The package loads the in-tree library built by tpu-wave_b200/build.py and raises if it is
+missing: there is no CPU or pure-PyTorch path. `Solver` mirrors the reference's object protocol
+(Class_Grid / Class_Forward_Specs in cuda/src/cpp): create the grids, set the material, place the
+source and receivers, step, read fields, traces and energies.
+
+The directory name is not a Python identifier; load it by path, e.g.
+
+    spec = importlib.util.spec_from_file_location("twave", "tpu-wave_b200/__init__.py")
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libtwave.so")
+HEADER = os.path.join(HERE, "..", "include", "twave.h")
+
+ELASTIC, ACOUSTIC = 0, 1
+SAT_FREE, PERIODIC = 0, 1
+FP64, FP32, BF16, FP16 = 0, 1, 2, 3
+CPST = {"00": 0, "-3C": 1, "-3R": 2, "3C": 3, "3R": 4, "6C": 5, "6R": 6}
+NN, MN, NM, MM = 0, 1, 2, 3
+GRID = {("N", "N"): NN, ("M", "N"): MN, ("N", "M"): NM, ("M", "M"): MM}
+PRECISION = {"f64": FP64, "f32": FP32, "bf16": BF16, "fp16": FP16}
+
+ERRORS = {0: "TW_OK", -1: "TW_ERR_INVALID", -2: "TW_ERR_CUDA", -3: "TW_ERR_NOMEM", -4: "TW_ERR_STATE",
+          -5: "TW_ERR_LOCATION", -6: "TW_ERR_OUTSIDE", -7: "TW_ERR_WEAK_BOUNDARY", -8: "TW_ERR_RECORD_FULL",
+          -9: "TW_ERR_NONFINITE", -10: "TW_ERR_UNSUPPORTED", -11: "TW_ERR_MODEL_BOUNDS"}
+
+
+class TwError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        self.name = ERRORS.get(code, str(code))
+        super().__init__(f"{what}: {self.name}")
+
+
+class GridDesc(C.Structure):
+    _fields_ = [("physics", C.c_int), ("bc_x", C.c_int), ("precision", C.c_int), ("cpst", C.c_int),
+                ("Mx", C.c_long), ("My", C.c_long), ("num_dx", C.c_int), ("den_dx", C.c_int),
+                ("dt", C.c_double), ("central_f", C.c_double), ("time_delay", C.c_double),
+                ("source_scaling", C.c_double), ("max_steps", C.c_int), ("energy", C.c_int), ("device", C.c_int)]
+
+
+class Info(C.Structure):
+    _fields_ = [("rows", C.c_long * 4), ("cols", C.c_long * 4), ("pitch", C.c_long), ("steps_done", C.c_int),
+                ("n_rcv", C.c_int), ("bytes_per_update", C.c_double), ("device_bytes", C.c_double)]
+
+
+_lib = None
+
+
+def library_path() -> str:
+    return LIB_PATH
+
+
+def lib() -> C.CDLL:
+    """Load libtwave.so; raises if it has not been built (no fallback path exists)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `python tpu-wave_b200/build.py`")
+        L = C.CDLL(LIB_PATH)
+        vp, dp, lp = C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)
+        L.tw_create.argtypes = [C.POINTER(vp), C.POINTER(GridDesc)]
+        L.tw_destroy.argtypes = [vp]
+        L.tw_destroy.restype = None
+        L.tw_set_material_model.argtypes = [vp, dp, dp, dp, C.c_long, C.c_long, C.c_int, C.c_int]
+        L.tw_set_material_grid.argtypes = [vp, C.c_int, C.c_int, dp, C.c_long]
+        L.tw_set_source_location.argtypes = [vp, C.c_char, C.c_char, C.c_long, C.c_long, C.c_long, C.c_long]
+        L.tw_set_source.argtypes = [vp, C.c_int, C.c_long, C.c_long]
+        L.tw_clear_source.argtypes = [vp]
+        L.tw_add_receiver_location.argtypes = [vp, C.c_char, C.c_char, C.c_long, C.c_long, C.c_long, C.c_long]
+        L.tw_add_receivers.argtypes = [vp, C.c_int, lp, lp, C.c_int]
+        L.tw_reset.argtypes = [vp]
+        L.tw_step.argtypes = [vp, C.c_int]
+        L.tw_sync.argtypes = [vp]
+        for name in ("tw_read_field", "tw_write_field", "tw_read_resid", "tw_write_resid"):
+            getattr(L, name).argtypes = [vp, C.c_int, C.c_int, dp, C.c_long]
+        L.tw_read_receivers.argtypes = [vp, dp]
+        L.tw_read_energy.argtypes = [vp, dp, dp, dp]
+        L.tw_get_info.argtypes = [vp, C.POINTER(Info)]
+        L.tw_get_stream.argtypes = [vp, C.POINTER(vp)]
+        L.tw_profile.argtypes = [vp, C.c_int, dp]
+        L.tw_location_to_index.argtypes = [C.c_char, C.c_long, C.c_long, C.c_int, C.c_int, lp]
+        L.tw_strerror.restype = C.c_char_p
+        L.tw_strerror.argtypes = [C.c_int]
+        L.tw_last_cuda_error.restype = C.c_char_p
+        _lib = L
+    return _lib
+
+
+def declared_symbols() -> list[str]:
+    """Names of the entry points include/twave.h declares (TW_API lines)."""
+    import re
+    with open(HEADER) as f:
+        text = f.read()
+    return re.findall(r"^TW_API[^(]*?\b(tw_\w+)\(", text, flags=re.M)
+
+
+def _dp(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+def _ok(code: int, what: str):
+    if code != 0:
+        if code == -2:
+            what = f"{what} ({lib().tw_last_cuda_error().decode()})"
+        raise TwError(code, what)
+
+
+def location_to_index(gtype: str, num: int, den: int, num_dx: int, den_dx: int) -> int:
+    """Rational location -> grid index through the library (forward.cpp:31-51)."""
+    out = C.c_long()
+    _ok(lib().tw_location_to_index(gtype.encode(), num, den, num_dx, den_dx, C.byref(out)), "tw_location_to_index")
+    return out.value
+
+
+class Solver:
+    """One simulation: the reference's four grids + forward specs, on one GPU stream."""
+
+    def __init__(self, Mx: int, My: int, num_dx: int, den_dx: int, dt: float, *, physics: int = ELASTIC,
+                 bc_x: int = SAT_FREE, precision: str = "f32", cpst: str = "00", central_f: float = 5.0,
+                 time_delay: float = 0.25, source_scaling: float = 1.0, max_steps: int = 1000,
+                 energy: bool = True, device: int = 0):
+        self.desc = GridDesc(physics, bc_x, PRECISION[precision], CPST[cpst], Mx, My, num_dx, den_dx, dt,
+                             central_f, time_delay, source_scaling, max_steps, 1 if energy else 0, device)
+        self.h = C.c_void_p()
+        _ok(lib().tw_create(C.byref(self.h), C.byref(self.desc)), "tw_create")
+        self.Mx, self.My, self.physics, self.bc_x = Mx, My, physics, bc_x
+        self.n_rcv = 0
+
+    def close(self):
+        if self.h:
+            lib().tw_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- sizes
+    def shape(self, grid: int):
+        Mx, My = self.Mx, self.My
+        return {NN: (Mx + 1, My + 1), MN: (Mx, My + 1), NM: (Mx + 1, My), MM: (Mx, My)}[grid]
+
+    # ---- material
+    def set_material_model(self, rho, vp, vs=None, Mx_prmt=None, My_prmt=None, num_dxM=None, den_dxM=None):
+        Mxp = self.Mx if Mx_prmt is None else Mx_prmt
+        Myp = self.My if My_prmt is None else My_prmt
+        nd = self.desc.num_dx if num_dxM is None else num_dxM
+        dd = self.desc.den_dx if den_dxM is None else den_dxM
+        P = (Mxp + 2) * (Myp + 2)
+        arrs = [np.ascontiguousarray(np.asarray(a, np.float64).reshape(-1)) for a in (rho, vp)]
+        arrs.append(np.zeros(P) if vs is None else np.ascontiguousarray(np.asarray(vs, np.float64).reshape(-1)))
+        for a in arrs:
+            if a.size != P:
+                raise ValueError(f"model arrays must hold (Mx_prmt+2)*(My_prmt+2) = {P} values")
+        _ok(lib().tw_set_material_model(self.h, *[_dp(a) for a in arrs], Mxp, Myp, nd, dd), "tw_set_material_model")
+
+    def set_material_grid(self, grid: int, idx: int, coef):
+        a = np.ascontiguousarray(np.asarray(coef, np.float64))
+        r, c = self.shape(grid)
+        if a.shape != (r, c):
+            raise ValueError(f"expected shape {(r, c)}, got {a.shape}")
+        _ok(lib().tw_set_material_grid(self.h, grid, idx, _dp(a), c), "tw_set_material_grid")
+
+    # ---- source / receivers
+    def set_source(self, grid: int, ix: int, iy: int):
+        _ok(lib().tw_set_source(self.h, grid, ix, iy), "tw_set_source")
+
+    def set_source_location(self, tx, ty, nx, dxn, ny, dyn):
+        _ok(lib().tw_set_source_location(self.h, tx.encode(), ty.encode(), nx, dxn, ny, dyn), "tw_set_source_location")
+
+    def clear_source(self):
+        _ok(lib().tw_clear_source(self.h), "tw_clear_source")
+
+    def add_receivers(self, grid: int, ix, iy):
+        ix = np.ascontiguousarray(np.atleast_1d(ix), np.int64)
+        iy = np.ascontiguousarray(np.atleast_1d(iy), np.int64)
+        lp = C.POINTER(C.c_long)
+        _ok(lib().tw_add_receivers(self.h, grid, ix.ctypes.data_as(lp), iy.ctypes.data_as(lp), int(ix.size)),
+            "tw_add_receivers")
+        self.n_rcv += int(ix.size)
+
+    def add_receiver_location(self, tx, ty, nx, dxn, ny, dyn):
+        _ok(lib().tw_add_receiver_location(self.h, tx.encode(), ty.encode(), nx, dxn, ny, dyn), "tw_add_receiver_location")
+        self.n_rcv += 1
+
+    # ---- stepping
+    def reset(self):
+        _ok(lib().tw_reset(self.h), "tw_reset")
+
+    def step(self, n: int):
+        _ok(lib().tw_step(self.h, n), "tw_step")
+
+    def sync(self):
+        _ok(lib().tw_sync(self.h), "tw_sync")
+
+    def run(self, n: int):
+        self.step(n)
+        self.sync()
+
+    # ---- readback
+    def read_field(self, grid: int, field: int = 0) -> np.ndarray:
+        r, c = self.shape(grid)
+        out = np.empty((r, c))
+        _ok(lib().tw_read_field(self.h, grid, field, _dp(out), c), "tw_read_field")
+        return out
+
+    def write_field(self, grid: int, field: int, values):
+        a = np.ascontiguousarray(np.asarray(values, np.float64))
+        r, c = self.shape(grid)
+        if a.shape != (r, c):
+            raise ValueError(f"expected shape {(r, c)}")
+        _ok(lib().tw_write_field(self.h, grid, field, _dp(a), c), "tw_write_field")
+
+    def read_resid(self, grid: int, field: int = 0) -> np.ndarray:
+        r, c = self.shape(grid)
+        out = np.empty((r, c))
+        _ok(lib().tw_read_resid(self.h, grid, field, _dp(out), c), "tw_read_resid")
+        return out
+
+    def write_resid(self, grid: int, field: int, values):
+        a = np.ascontiguousarray(np.asarray(values, np.float64))
+        r, c = self.shape(grid)
+        _ok(lib().tw_write_resid(self.h, grid, field, _dp(a), c), "tw_write_resid")
+
+    def info(self) -> Info:
+        inf = Info()
+        _ok(lib().tw_get_info(self.h, C.byref(inf)), "tw_get_info")
+        return inf
+
+    def read_receivers(self) -> np.ndarray:
+        n = self.info().steps_done
+        out = np.zeros((self.n_rcv, 2, n))
+        if self.n_rcv and n:
+            _ok(lib().tw_read_receivers(self.h, _dp(out)), "tw_read_receivers")
+        return out
+
+    def read_energy(self):
+        n = self.info().steps_done
+        E_k, E_p0, E_p1 = np.zeros(n), np.zeros(n), np.zeros(n)
+        if n:
+            _ok(lib().tw_read_energy(self.h, _dp(E_k), _dp(E_p0), _dp(E_p1)), "tw_read_energy")
+        return E_k, E_p0, E_p1
+
+    def profile(self, n: int) -> np.ndarray:
+        """Mean ms per launch of [velocity, stress, energy, gather] over n eagerly launched steps."""
+        ms = np.zeros(4)
+        _ok(lib().tw_profile(self.h, n, _dp(ms)), "tw_profile")
+        return ms
+
+    def stream(self) -> int:
+        p = C.c_void_p()
+        _ok(lib().tw_get_stream(self.h, C.byref(p)), "tw_get_stream")
+        return p.value or 0

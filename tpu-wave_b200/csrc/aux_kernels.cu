@@ -1,0 +1,218 @@
+// Set-up and bookkeeping kernels: FP64 material interpolation, stepping coefficients and energy
+// weights, the discrete energy reductions and the receiver gather.
+#include "kernels.h"
+
+namespace tw {
+
+// ---------------------------------------------------------------- material (FP64, exact order)
+__global__ void k_model_derive(const double *rho, const double *vp, const double *vs, long n, double *lam,
+                               double *m2, double *mu)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const double r = rho[i], p = vp[i], s = vs[i];
+        const double two_mu = mul(mul(mul(2.0, r), s), s);           // 2 * rho * vs * vs
+        m2[i] = two_mu;
+        lam[i] = sub(mul(mul(r, p), p), two_mu);                      // rho * vp * vp - 2mu
+        mu[i] = mul(mul(r, s), s);                                    // rho * vs * vs
+    }
+}
+
+void launch_model_derive(const double *rho, const double *vp, const double *vs, long n, double *lam,
+                         double *m2, double *mu, cudaStream_t st)
+{
+    const int blocks = (int)((n + 255) / 256 < 65535 ? (n + 255) / 256 : 65535);
+    k_model_derive<<<blocks, 256, 0, st>>>(rho, vp, vs, n, lam, m2, mu);
+}
+
+// interpolate_forward_parameter (grid_parameter.cpp:13-57): the location of grid point (ix, iy)
+// in units of the model spacing is num/den; its integer part indexes the padded model, the
+// remainder (computed in double) weights the four corners.
+__global__ void k_interp(int rows, int My, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
+                         long Nxp, long Nyp, const double *in, double *out, int *err)
+{
+    const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ix = blockIdx.y * blockDim.y + threadIdx.y;
+    if (iy >= My || ix >= rows) return;
+    long nx, dxl, ny, dyl;
+    if (txN) { nx = (long)ix * num_dx; dxl = den_dx; } else { nx = (2L * ix + 1) * num_dx; dxl = 2L * den_dx; }
+    if (tyN) { ny = (long)iy * num_dx; dyl = den_dx; } else { ny = (2L * iy + 1) * num_dx; dyl = 2L * den_dx; }
+    const long ixM = (nx * den_dxM) / (dxl * num_dxM);
+    const long iyM = (ny * den_dxM) / (dyl * num_dxM);
+    if (ixM < 0 || ixM + 1 > Nxp || iyM < 0 || iyM + 1 > Nyp) { atomicOr(err, 1); return; }
+    const double xi = sub(__ddiv_rn((double)(nx * den_dxM), (double)(dxl * num_dxM)), (double)ixM);
+    const double eta = sub(__ddiv_rn((double)(ny * den_dxM), (double)(dyl * num_dxM)), (double)iyM);
+    const long PS = Nyp + 1;
+    const double a = sub(1.0, xi), b = sub(1.0, eta);
+    double v = mul(mul(a, b), in[ixM * PS + iyM]);
+    v = add(v, mul(mul(a, eta), in[ixM * PS + iyM + 1]));
+    v = add(v, mul(mul(xi, b), in[(ixM + 1) * PS + iyM]));
+    v = add(v, mul(mul(xi, eta), in[(ixM + 1) * PS + iyM + 1]));
+    out[(long)ix * My + iy] = v;
+}
+
+void launch_interp(int rows, int My, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
+                   long Nx_prmt, long Ny_prmt, const double *in, double *out, int *err, cudaStream_t st)
+{
+    const dim3 b(32, 8), g((My + 31) / 32, (rows + 7) / 8);
+    k_interp<<<g, b, 0, st>>>(rows, My, txN, tyN, num_dx, den_dx, num_dxM, den_dxM, Nx_prmt, Ny_prmt, in, out, err);
+}
+
+// x factor of the energy norm for row ix of a grid with `rows` rows (adjust_parameters_energy_periodic,
+// grid_energy.cpp:69-119): A_diag * dx rounded to the storage type on the SAT boundary rows (the
+// host precomputes them into nxN / nxM), dx inside
+__device__ __forceinline__ double norm_x(const MaterialArgs &m, int txN, int rows, int ix)
+{
+    if (txN) {
+        if (ix < 4) return m.nxN[ix];
+        if (ix >= rows - 4) return m.nxN[4 + ix - (rows - 4)];
+    } else {
+        if (ix < 3) return m.nxM[ix];
+        if (ix >= rows - 3) return m.nxM[3 + ix - (rows - 3)];
+    }
+    return m.dx;
+}
+
+template <class C>
+__global__ void k_material_finalize(MaterialArgs m)
+{
+    const int iy = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ix = blockIdx.y * blockDim.y + threadIdx.y;
+    if (iy >= m.My) return;
+    const long i = (long)ix * m.My + iy;       // compact FP64 input
+    const long o = (long)ix * m.pitch + iy;    // device layout
+    const double dx = m.dx;
+    const double w_sc = mul(dx, dx) / 2.;      // single-core weight dx*dx/2 (namespaces.hpp:754)
+    const bool elastic = m.physics == 0;
+    C **coef = (C **)m.coef;
+    // NN (elastic only): mu, weight 1/mu
+    if (elastic && ix < m.rows[F_NN]) {
+        const C mu = (C)m.mat[F_NN][i];
+        coef[F_NN][o] = mu;
+        double w = __ddiv_rn(1., (double)mu);
+        w = mul(w, norm_x(m, 1, m.rows[F_NN], ix));
+        m.w[F_NN][o] = mul(w, dx);
+    }
+    // velocity grids: 1/rho from the FP64 density (make_density_reciprocal), weight rho
+    for (int g = F_MN; g <= F_NM; g++) {
+        if (ix >= m.rows[g]) continue;
+        const double rho = m.mat[g][i];
+        coef[g][o] = (C)__ddiv_rn(1., rho);
+        if (m.periodic) {
+            m.w[g][o] = w_sc;
+        } else {
+            double w = (double)(C)rho;
+            w = mul(w, norm_x(m, g == F_NM, m.rows[g], ix));
+            m.w[g][o] = mul(w, dx);
+        }
+    }
+    if (ix < m.rows[F_MM0]) {
+        const C lam = (C)m.mat[F_MM0][i];
+        coef[F_MM0][o] = lam;
+        const double fx = norm_x(m, 0, m.rows[F_MM0], ix);
+        if (elastic) {
+            const C m2 = (C)m.mat[F_MM1][i];
+            coef[F_MM1][o] = m2;
+            const double l = (double)lam, t = (double)m2;
+            const double den = mul(t, add(mul(2., l), t));
+            double w1 = __ddiv_rn(add(l, t), den);
+            double w2 = -__ddiv_rn(mul(l, 2.), den);
+            m.w[F_MM0][o] = mul(mul(w1, fx), dx);
+            m.w[F_MM1][o] = mul(mul(w2, fx), dx);
+        } else if (m.periodic) {
+            m.w[F_MM0][o] = w_sc;
+        } else {
+            // acoustic free surface: the mu -> 0 limit of the elastic weights, (2 P1 + P2) -> 1/kappa
+            m.w[F_MM0][o] = mul(mul(__ddiv_rn(1., (double)lam), fx), dx);
+        }
+    }
+}
+
+template <class C>
+void launch_material_finalize(const MaterialArgs &m, cudaStream_t st)
+{
+    const int rows = m.rows[F_NM] > m.rows[F_MM0] ? m.rows[F_NM] : m.rows[F_MM0];
+    const int rmax = m.rows[F_NN] > rows ? m.rows[F_NN] : rows;
+    const dim3 b(32, 8), g((m.My + 31) / 32, (rmax + 7) / 8);
+    k_material_finalize<C><<<g, b, 0, st>>>(m);
+}
+template void launch_material_finalize<double>(const MaterialArgs &, cudaStream_t);
+template void launch_material_finalize<float>(const MaterialArgs &, cudaStream_t);
+
+// ---------------------------------------------------------------- discrete energy (FP64)
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <class S, class C>
+__global__ void __launch_bounds__(256) k_energy(EnergyArgs<S, C> e)
+{
+    const int it = *e.step;
+    if (it >= e.max_steps) return;
+    int rmax = 0;
+    for (int t = 0; t < e.nterms; t++) rmax = e.rows[t] > rmax ? e.rows[t] : rmax;
+    const long n = (long)rmax * e.My;
+    double acc = 0.;
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
+        const int ix = (int)(k / e.My), iy = (int)(k - (long)ix * e.My);
+        const long o = (long)ix * e.pitch + iy;
+        for (int t = 0; t < e.nterms; t++) {
+            if (ix >= e.rows[t]) continue;
+            if (e.single_core) {   // soln * prmt * soln * weight (cpu_acoustic.cpp:341)
+                const C s = to_c<C>(e.a[t][o]);
+                acc = add(acc, mul((double)mul(mul(s, e.p[t][o]), s), e.w[t][o]));
+            } else {               // (double)S * W * (double)S (grid_energy.cpp:196-210)
+                acc = add(acc, mul(mul((double)to_c<C>(e.a[t][o]), e.w[t][o]), (double)to_c<C>(e.b[t][o])));
+            }
+        }
+    }
+    __shared__ double part[8];
+    acc = warp_sum(acc);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.;
+        acc = warp_sum(acc);
+        if (threadIdx.x == 0) atomicAdd(e.out + it, acc * e.scale);
+    }
+}
+
+template <class S, class C>
+void launch_energy(const EnergyArgs<S, C> &e, cudaStream_t st)
+{
+    // 148 SMs x 4 resident blocks of 256 threads: one wave of a grid-stride reduction
+    k_energy<S, C><<<148 * 4, 256, 0, st>>>(e);
+}
+template void launch_energy<double, double>(const EnergyArgs<double, double> &, cudaStream_t);
+template void launch_energy<float, float>(const EnergyArgs<float, float> &, cudaStream_t);
+
+// ---------------------------------------------------------------- receivers + step counter
+template <class S>
+__global__ void k_gather(GatherArgs<S> g)
+{
+    const int it = *g.step;
+    if (it < g.max_steps) {
+        for (int r = threadIdx.x; r < g.n_rcv; r += blockDim.x) {
+            const int *q = g.rcv + 4 * r;
+            const long o = (long)q[2] * g.pitch + q[3];
+            g.traces[(2L * r) * g.max_steps + it] = (double)to_c<double>(g.f[q[0]][o]);
+            g.traces[(2L * r + 1) * g.max_steps + it] = q[1] >= 0 ? (double)to_c<double>(g.f[q[1]][o]) : 0.;
+        }
+    } else if (threadIdx.x == 0) {
+        atomicOr(g.flags, FLAG_RECORD_FULL);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) *g.step = it + 1;
+}
+
+template <class S>
+void launch_gather(const GatherArgs<S> &g, cudaStream_t st)
+{
+    k_gather<S><<<1, 256, 0, st>>>(g);
+}
+template void launch_gather<double>(const GatherArgs<double> &, cudaStream_t);
+template void launch_gather<float>(const GatherArgs<float> &, cudaStream_t);
+
+}  // namespace tw

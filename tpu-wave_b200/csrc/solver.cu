@@ -1,0 +1,809 @@
+// C ABI of the stepper (include/twave.h): the solver handle, set-up, stepping and readback.
+//
+// The handle plays the role of the reference's four Class_Grid objects plus
+// Class_Forward_Specs (grid.hpp, forward.hpp): it owns the device fields, coefficients, energy
+// weights, source table and receiver records of one simulation and one CUDA stream. Steps are
+// enqueued asynchronously and replayed from a CUDA graph; every kernel of a step reads the step
+// index from a device counter, so one captured graph serves every replay.
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/twave.h"
+#include "kernels.h"
+
+using namespace tw;
+
+namespace {
+
+thread_local std::string g_cuda_error;
+
+int cuda_fail(cudaError_t e, const char *where)
+{
+    g_cuda_error = std::string(where) + ": " + cudaGetErrorString(e);
+    return TW_ERR_CUDA;
+}
+
+#define TW_CUDA(call)                                             \
+    do {                                                          \
+        cudaError_t e_ = (call);                                  \
+        if (e_ != cudaSuccess) return cuda_fail(e_, #call);       \
+    } while (0)
+
+// Ricker wavelet as the reference evaluates it (forward_simulation.cpp:63-64)
+double ricker(double t, double f)
+{
+    return (1 - 2 * M_PI * M_PI * f * f * t * t) * exp(-M_PI * M_PI * f * f * t * t);
+}
+
+// rational location -> grid index (forward.cpp:31-51); false if it is not a grid point
+bool location_to_index(char type, long num, long den, int num_dx, int den_dx, long *out)
+{
+    long n, d;
+    if (type == 'N') { n = num * den_dx; d = den * num_dx; }
+    else if (type == 'M') { n = 2 * num * den_dx - den * num_dx; d = 2 * den * num_dx; }
+    else return false;
+    if (d == 0 || n % d != 0) return false;
+    *out = n / d;
+    return true;
+}
+
+}  // namespace
+
+struct tw_solver {
+    tw_grid_desc d{};
+    int elastic = 1, periodic = 0;
+    int esz = 4;                      // bytes per stored field value
+    long pitch = 0;
+    int rows[5] = {0, 0, 0, 0, 0};    // device rows per field slot (0: slot unused)
+    long ref_rows[4], ref_cols[4];    // reference sizes per grid
+    cudaStream_t st = nullptr;
+    void *f[5] = {}, *res[5] = {}, *coef[5] = {};
+    double *w[5] = {}, *mat[5] = {};
+    bool mat_set[5] = {};
+    bool mat_dirty = true, mat_ready = false;
+    double *src_inc = nullptr;
+    int *d_step = nullptr, *d_flags = nullptr, *d_rcv = nullptr, *d_err = nullptr;
+    double *d_traces = nullptr, *d_energy = nullptr;
+    int rcv_cap = 0;
+    std::vector<int> rcv_tab;         // n x 4 (slot0, slot1, row, col)
+    int src_grid = -1;
+    long src_ix = 0, src_iy = 0;
+    int steps_done = 0;
+    int sticky = TW_OK;
+    cudaGraphExec_t gexec = nullptr;
+    int graph_steps = 0;
+    double dev_bytes = 0;
+
+    ~tw_solver();
+    int alloc(void **p, size_t bytes)
+    {
+        cudaError_t e = cudaMalloc(p, bytes);
+        if (e != cudaSuccess) { cuda_fail(e, "cudaMalloc"); return TW_ERR_NOMEM; }
+        dev_bytes += (double)bytes;
+        return TW_OK;
+    }
+    bool has_slot(int slot) const { return rows[slot] > 0; }
+    void drop_graph()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+        graph_steps = 0;
+    }
+};
+
+tw_solver::~tw_solver()
+{
+    drop_graph();
+    for (int k = 0; k < 5; k++) {
+        cudaFree(f[k]); cudaFree(res[k]); cudaFree(coef[k]); cudaFree(w[k]); cudaFree(mat[k]);
+    }
+    cudaFree(src_inc); cudaFree(d_step); cudaFree(d_flags); cudaFree(d_rcv); cudaFree(d_err);
+    cudaFree(d_traces); cudaFree(d_energy);
+    if (st) cudaStreamDestroy(st);
+}
+
+namespace {
+
+// map a reference (grid, field) to the device slot
+int slot_of(const tw_solver *s, int grid, int field)
+{
+    switch (grid) {
+    case TW_NN: return field == 0 && s->elastic ? F_NN : -1;
+    case TW_MN: return field == 0 ? F_MN : -1;
+    case TW_NM: return field == 0 ? F_NM : -1;
+    case TW_MM: return field == 0 ? F_MM0 : (field == 1 && s->elastic ? F_MM1 : -1);
+    }
+    return -1;
+}
+
+template <class S, class C>
+StepArgs<S, C> step_args(const tw_solver *s)
+{
+    StepArgs<S, C> a{};
+    for (int k = 0; k < 5; k++) {
+        a.f[k] = (S *)s->f[k];
+        a.res[k] = (S *)s->res[k];
+        a.coef[k] = (const C *)s->coef[k];
+    }
+    a.pitch = s->pitch;
+    a.Mx = (int)s->d.Mx;
+    a.My = (int)s->d.My;
+    a.op = make_ops<C>((double)s->d.num_dx / (double)s->d.den_dx, s->d.dt, s->periodic && !s->elastic);
+    a.src_inc = s->src_inc;
+    a.src_grid = s->src_grid;
+    a.src_ix = (int)s->src_ix;
+    a.src_iy = (int)s->src_iy;
+    a.max_steps = s->d.max_steps;
+    a.step = s->d_step;
+    a.flags = s->d_flags;
+    return a;
+}
+
+template <class S, class C>
+void energy_phase(const tw_solver *s, int phase, cudaStream_t st)
+{
+    // phase 0: E_p0 (stresses before the step), 1: E_k (velocities), 2: E_p1 (stresses after)
+    EnergyArgs<S, C> e{};
+    e.My = (int)s->d.My;
+    e.pitch = s->pitch;
+    e.max_steps = s->d.max_steps;
+    e.step = s->d_step;
+    e.out = s->d_energy + (long)phase * s->d.max_steps;
+    e.single_core = s->periodic;
+    e.scale = s->periodic ? 1.0 : 0.5;
+    auto term = [&](int a, int b, int wslot, int pslot) {
+        const int t = e.nterms++;
+        e.a[t] = (const S *)s->f[a];
+        e.b[t] = (const S *)s->f[b];
+        e.w[t] = s->w[wslot];
+        e.p[t] = (const C *)s->coef[pslot];
+        e.rows[t] = s->rows[a];
+    };
+    if (phase == 1) {
+        term(F_MN, F_MN, F_MN, F_MN);
+        term(F_NM, F_NM, F_NM, F_NM);
+    } else if (s->elastic) {
+        term(F_MM0, F_MM0, F_MM0, F_MM0);
+        term(F_MM1, F_MM1, F_MM0, F_MM0);
+        term(F_MM0, F_MM1, F_MM1, F_MM0);
+        term(F_NN, F_NN, F_NN, F_NN);
+    } else {
+        term(F_MM0, F_MM0, F_MM0, F_MM0);
+    }
+    launch_energy<S, C>(e, st);
+}
+
+template <class S, class C>
+void enqueue_steps(tw_solver *s, int n, cudaStream_t st)
+{
+    const StepArgs<S, C> a = step_args<S, C>(s);
+    GatherArgs<S> g{};
+    for (int k = 0; k < 5; k++) g.f[k] = (const S *)s->f[k];
+    g.rcv = s->d_rcv;
+    g.n_rcv = (int)(s->rcv_tab.size() / 4);
+    g.pitch = s->pitch;
+    g.traces = s->d_traces;
+    g.max_steps = s->d.max_steps;
+    g.step = s->d_step;
+    g.flags = s->d_flags;
+    const bool en = s->d.energy != 0;
+    for (int k = 0; k < n; k++) {
+        if (en && !s->periodic) energy_phase<S, C>(s, 0, st);
+        launch_half<S, C>(s->elastic ? 0 : 1, s->periodic, s->d.cpst, 0, a, st);
+        if (en) energy_phase<S, C>(s, 1, st);
+        launch_half<S, C>(s->elastic ? 0 : 1, s->periodic, s->d.cpst, 1, a, st);
+        if (en) energy_phase<S, C>(s, 2, st);
+        launch_gather<S>(g, st);
+    }
+}
+
+// launch phase `ph` (0 velocity, 1 stress, 2 energy of the step, 3 gather) of one step
+template <class S, class C>
+void enqueue_phase(tw_solver *s, int ph, cudaStream_t st)
+{
+    const StepArgs<S, C> a = step_args<S, C>(s);
+    if (ph == 0 || ph == 1) {
+        launch_half<S, C>(s->elastic ? 0 : 1, s->periodic, s->d.cpst, ph, a, st);
+    } else if (ph == 2) {
+        if (!s->periodic) energy_phase<S, C>(s, 0, st);
+        energy_phase<S, C>(s, 1, st);
+        energy_phase<S, C>(s, 2, st);
+    } else {
+        GatherArgs<S> g{};
+        for (int k = 0; k < 5; k++) g.f[k] = (const S *)s->f[k];
+        g.rcv = s->d_rcv;
+        g.n_rcv = (int)(s->rcv_tab.size() / 4);
+        g.pitch = s->pitch;
+        g.traces = s->d_traces;
+        g.max_steps = s->d.max_steps;
+        g.step = s->d_step;
+        g.flags = s->d_flags;
+        launch_gather<S>(g, st);
+    }
+}
+
+void enqueue(tw_solver *s, int n, cudaStream_t st)
+{
+    if (s->d.precision == TW_FP64) enqueue_steps<double, double>(s, n, st);
+    else enqueue_steps<float, float>(s, n, st);
+}
+
+// stepping coefficients and energy weights from the FP64 material arrays
+int finalize_material(tw_solver *s)
+{
+    for (int k = 0; k < 5; k++)
+        if (s->has_slot(k) && !s->mat_set[k]) return TW_ERR_STATE;
+    MaterialArgs m{};
+    for (int k = 0; k < 5; k++) {
+        m.mat[k] = s->mat[k];
+        m.coef[k] = s->coef[k];
+        m.w[k] = s->w[k];
+        m.rows[k] = s->rows[k];
+    }
+    m.Mx = (int)s->d.Mx;
+    m.My = (int)s->d.My;
+    m.pitch = s->pitch;
+    m.dx = (double)s->d.num_dx / (double)s->d.den_dx;
+    m.physics = s->elastic ? 0 : 1;
+    m.periodic = s->periodic;
+    const bool f64 = s->d.precision == TW_FP64;
+    for (int i = 0; i < 4; i++) {
+        const double l = SbpTables::A_N_L[i] * m.dx, r = SbpTables::A_N_R[i] * m.dx;
+        m.nxN[i] = f64 ? l : (double)(float)l;
+        m.nxN[4 + i] = f64 ? r : (double)(float)r;
+    }
+    for (int i = 0; i < 3; i++) {
+        const double l = SbpTables::A_M_L[i] * m.dx, r = SbpTables::A_M_R[i] * m.dx;
+        m.nxM[i] = f64 ? l : (double)(float)l;
+        m.nxM[3 + i] = f64 ? r : (double)(float)r;
+    }
+    if (f64) launch_material_finalize<double>(m, s->st);
+    else launch_material_finalize<float>(m, s->st);
+    TW_CUDA(cudaGetLastError());
+    s->mat_dirty = false;
+    s->mat_ready = true;
+    return TW_OK;
+}
+
+int rebuild_source_table(tw_solver *s)
+{
+    std::vector<double> inc(s->d.max_steps, 0.0);
+    if (s->src_grid >= 0) {
+        const double dt = s->d.dt, dx = (double)s->d.num_dx / (double)s->d.den_dx;
+        const bool stress = s->src_grid == TW_NN || s->src_grid == TW_MM;
+        for (int it = 0; it < s->d.max_steps; it++) {
+            // V grids: t = it dt - delay; S grids: t = (it + 1/2) dt - delay (forward_simulation.cpp:63,105);
+            // the single-core tree's P source uses (it + 1 - 1/2) dt, the same value (cpu_acoustic.cpp:309)
+            const double t = stress ? (it + 1. / 2.) * dt - s->d.time_delay : it * dt - s->d.time_delay;
+            double v = ricker(t, s->d.central_f) * dt / (dx * dx);
+            if (s->d.source_scaling != 1.0) v = v / s->d.source_scaling;
+            inc[it] = v;
+        }
+    }
+    TW_CUDA(cudaMemcpyAsync(s->src_inc, inc.data(), sizeof(double) * inc.size(), cudaMemcpyHostToDevice, s->st));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    s->drop_graph();
+    return TW_OK;
+}
+
+int upload_receivers(tw_solver *s)
+{
+    const int n = (int)(s->rcv_tab.size() / 4);
+    if (n > s->rcv_cap) {
+        cudaFree(s->d_rcv);
+        cudaFree(s->d_traces);
+        s->d_rcv = nullptr;
+        s->d_traces = nullptr;
+        int cap = s->rcv_cap ? s->rcv_cap : 16;
+        while (cap < n) cap *= 2;
+        if (s->alloc((void **)&s->d_rcv, sizeof(int) * 4 * cap) != TW_OK) return TW_ERR_NOMEM;
+        if (s->alloc((void **)&s->d_traces, sizeof(double) * 2 * (size_t)cap * s->d.max_steps) != TW_OK) return TW_ERR_NOMEM;
+        TW_CUDA(cudaMemsetAsync(s->d_traces, 0, sizeof(double) * 2 * (size_t)cap * s->d.max_steps, s->st));
+        s->rcv_cap = cap;
+    }
+    if (n > 0)
+        TW_CUDA(cudaMemcpyAsync(s->d_rcv, s->rcv_tab.data(), sizeof(int) * s->rcv_tab.size(), cudaMemcpyHostToDevice, s->st));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    s->drop_graph();
+    return TW_OK;
+}
+
+// host conversion double -> storage bits
+void to_storage(int prec, const double *src, void *dst, long n)
+{
+    if (prec == TW_FP64) memcpy(dst, src, sizeof(double) * n);
+    else if (prec == TW_FP32) for (long i = 0; i < n; i++) ((float *)dst)[i] = (float)src[i];
+    else if (prec == TW_BF16) for (long i = 0; i < n; i++) ((__nv_bfloat16 *)dst)[i] = __float2bfloat16_rn((float)src[i]);
+    else for (long i = 0; i < n; i++) ((__half *)dst)[i] = __float2half_rn((float)src[i]);
+}
+
+double from_storage(int prec, const void *src, long i)
+{
+    if (prec == TW_FP64) return ((const double *)src)[i];
+    if (prec == TW_FP32) return ((const float *)src)[i];
+    if (prec == TW_BF16) return (double)__bfloat162float(((const __nv_bfloat16 *)src)[i]);
+    return (double)__half2float(((const __half *)src)[i]);
+}
+
+// copy a device-layout array (rows x pitch) of `esz`-byte values to the host in the reference
+// layout: an extra periodic duplicate column (N-type y) and row (N-type x with periodic x) repeat
+// column / row 0
+int read_device_array(tw_solver *s, const void *dev, int prec, int esz, int slot, int grid, double *host, long ld)
+{
+    const long R = s->rows[slot], My = s->d.My;
+    std::vector<char> buf((size_t)R * My * esz);
+    TW_CUDA(cudaMemcpy2DAsync(buf.data(), My * esz, dev, s->pitch * esz, My * esz, R, cudaMemcpyDeviceToHost, s->st));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    const long rr = s->ref_rows[grid], rc = s->ref_cols[grid];
+    for (long ix = 0; ix < rr; ix++) {
+        const long sx = ix < R ? ix : ix - R;
+        for (long iy = 0; iy < rc; iy++) {
+            const long sy = iy < My ? iy : iy - My;
+            host[ix * ld + iy] = from_storage(prec, buf.data(), sx * My + sy);
+        }
+    }
+    return TW_OK;
+}
+
+int write_device_array(tw_solver *s, void *dev, int prec, int esz, int slot, const double *host, long ld)
+{
+    const long R = s->rows[slot], My = s->d.My;
+    std::vector<double> tmp((size_t)R * My);
+    for (long ix = 0; ix < R; ix++)
+        for (long iy = 0; iy < My; iy++) tmp[ix * My + iy] = host[ix * ld + iy];
+    std::vector<char> buf((size_t)R * My * esz);
+    to_storage(prec, tmp.data(), buf.data(), R * My);
+    TW_CUDA(cudaMemcpy2DAsync(dev, s->pitch * esz, buf.data(), My * esz, My * esz, R, cudaMemcpyHostToDevice, s->st));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    s->drop_graph();
+    return TW_OK;
+}
+
+int check(tw_solver *s)
+{
+    return s ? TW_OK : TW_ERR_INVALID;
+}
+
+}  // namespace
+
+// ======================================================================== C ABI
+extern "C" {
+
+const char *tw_strerror(int status)
+{
+    switch (status) {
+    case TW_OK: return "ok";
+    case TW_ERR_INVALID: return "invalid argument";
+    case TW_ERR_CUDA: return "CUDA runtime error";
+    case TW_ERR_NOMEM: return "out of memory";
+    case TW_ERR_STATE: return "call out of order (material or set-up missing)";
+    case TW_ERR_LOCATION: return "location is not a grid point";
+    case TW_ERR_OUTSIDE: return "location outside the grid";
+    case TW_ERR_WEAK_BOUNDARY: return "source on a weak boundary or on the periodic seam";
+    case TW_ERR_RECORD_FULL: return "more steps than the records hold";
+    case TW_ERR_NONFINITE: return "non-finite value in a field";
+    case TW_ERR_UNSUPPORTED: return "unsupported configuration";
+    case TW_ERR_MODEL_BOUNDS: return "material interpolation outside the model";
+    }
+    return "unknown status";
+}
+
+const char *tw_last_cuda_error(void) { return g_cuda_error.c_str(); }
+
+int tw_create(tw_solver **out, const tw_grid_desc *desc)
+{
+    if (!out || !desc) return TW_ERR_INVALID;
+    *out = nullptr;
+    const tw_grid_desc &d = *desc;
+    if (d.physics != TW_ELASTIC && d.physics != TW_ACOUSTIC) return TW_ERR_INVALID;
+    if (d.bc_x != TW_BC_SAT_FREE && d.bc_x != TW_BC_PERIODIC) return TW_ERR_INVALID;
+    if (d.physics == TW_ELASTIC && d.bc_x == TW_BC_PERIODIC) return TW_ERR_UNSUPPORTED;
+    if (d.precision != TW_FP64 && d.precision != TW_FP32) return TW_ERR_UNSUPPORTED;
+    if (d.cpst < TW_CPST_00 || d.cpst > TW_CPST_6R) return TW_ERR_INVALID;
+    if (d.bc_x == TW_BC_PERIODIC && d.cpst != TW_CPST_00 && d.cpst != TW_CPST_3R && d.cpst != TW_CPST_6R)
+        return TW_ERR_UNSUPPORTED;   // the single-core tree offers '0', '3', '6' (namespaces.hpp:665-667)
+    if (d.Mx < 8 || d.My < 4 || d.Mx > (1L << 30) / 2 || d.My > (1L << 30) / 2) return TW_ERR_INVALID;
+    if (d.num_dx <= 0 || d.den_dx <= 0 || !(d.dt > 0) || d.max_steps < 1) return TW_ERR_INVALID;
+    if (!(d.source_scaling != 0.0)) return TW_ERR_INVALID;
+
+    tw_solver *s = new (std::nothrow) tw_solver();
+    if (!s) return TW_ERR_NOMEM;
+    s->d = d;
+    s->elastic = d.physics == TW_ELASTIC;
+    s->periodic = d.bc_x == TW_BC_PERIODIC;
+    s->esz = d.precision == TW_FP64 ? 8 : (d.precision == TW_FP32 ? 4 : 2);
+    const int rowsN = s->periodic ? (int)d.Mx : (int)d.Mx + 1;
+    s->rows[F_NN] = s->elastic ? rowsN : 0;
+    s->rows[F_MN] = (int)d.Mx;
+    s->rows[F_NM] = rowsN;
+    s->rows[F_MM0] = (int)d.Mx;
+    s->rows[F_MM1] = s->elastic ? (int)d.Mx : 0;
+    const long Mx = d.Mx, My = d.My;
+    const long rr[4] = {Mx + 1, Mx, Mx + 1, Mx}, rc[4] = {My + 1, My + 1, My, My};
+    for (int g = 0; g < 4; g++) { s->ref_rows[g] = rr[g]; s->ref_cols[g] = rc[g]; }
+    // rows padded to a multiple of 128 bytes so that every row starts aligned
+    const long align = 128 / s->esz;
+    s->pitch = (My + align - 1) / align * align;
+
+    int rc_ = TW_OK;
+    auto fail = [&](int code) { delete s; return code; };
+    cudaError_t e = cudaSetDevice(d.device);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaSetDevice"));
+    e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreate"));
+    const size_t csz = d.precision == TW_FP64 ? 8 : 4;
+    const bool cp = d.cpst != TW_CPST_00;
+    for (int k = 0; k < 5; k++) {
+        if (!s->has_slot(k)) continue;
+        const size_t n = (size_t)s->rows[k] * s->pitch;
+        if ((rc_ = s->alloc(&s->f[k], n * s->esz)) != TW_OK) return fail(rc_);
+        if (cp && (rc_ = s->alloc(&s->res[k], n * s->esz)) != TW_OK) return fail(rc_);
+        if ((rc_ = s->alloc(&s->coef[k], n * csz)) != TW_OK) return fail(rc_);
+        if ((rc_ = s->alloc((void **)&s->w[k], n * sizeof(double))) != TW_OK) return fail(rc_);
+        if ((rc_ = s->alloc((void **)&s->mat[k], (size_t)s->rows[k] * My * sizeof(double))) != TW_OK) return fail(rc_);
+        cudaMemsetAsync(s->f[k], 0, n * s->esz, s->st);
+        if (cp) cudaMemsetAsync(s->res[k], 0, n * s->esz, s->st);
+        cudaMemsetAsync(s->coef[k], 0, n * csz, s->st);
+        cudaMemsetAsync(s->w[k], 0, n * sizeof(double), s->st);
+    }
+    if ((rc_ = s->alloc((void **)&s->src_inc, sizeof(double) * d.max_steps)) != TW_OK) return fail(rc_);
+    if ((rc_ = s->alloc((void **)&s->d_energy, sizeof(double) * 3 * d.max_steps)) != TW_OK) return fail(rc_);
+    if ((rc_ = s->alloc((void **)&s->d_step, sizeof(int))) != TW_OK) return fail(rc_);
+    if ((rc_ = s->alloc((void **)&s->d_flags, sizeof(int))) != TW_OK) return fail(rc_);
+    if ((rc_ = s->alloc((void **)&s->d_err, sizeof(int))) != TW_OK) return fail(rc_);
+    cudaMemsetAsync(s->src_inc, 0, sizeof(double) * d.max_steps, s->st);
+    cudaMemsetAsync(s->d_energy, 0, sizeof(double) * 3 * d.max_steps, s->st);
+    cudaMemsetAsync(s->d_step, 0, sizeof(int), s->st);
+    cudaMemsetAsync(s->d_flags, 0, sizeof(int), s->st);
+    e = cudaStreamSynchronize(s->st);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "tw_create"));
+    if ((rc_ = upload_receivers(s)) != TW_OK) return fail(rc_);
+    *out = s;
+    return TW_OK;
+}
+
+void tw_destroy(tw_solver *s)
+{
+    if (!s) return;
+    cudaSetDevice(s->d.device);
+    if (s->st) cudaStreamSynchronize(s->st);
+    delete s;
+}
+
+int tw_set_material_model(tw_solver *s, const double *rho, const double *vp, const double *vs, long Mx_prmt,
+                          long My_prmt, int num_dxM, int den_dxM)
+{
+    if (check(s) || !rho || !vp || (s->elastic && !vs)) return TW_ERR_INVALID;
+    if (Mx_prmt < 1 || My_prmt < 1 || num_dxM <= 0 || den_dxM <= 0) return TW_ERR_INVALID;
+    // the model must span the simulation region (input_processing.cpp:203-211)
+    for (int dir = 0; dir < 2; dir++) {
+        const long pm = dir == 0 ? Mx_prmt : My_prmt, sm = dir == 0 ? s->d.Mx : s->d.My;
+        if (pm * num_dxM * (long)s->d.den_dx != sm * (long)s->d.num_dx * den_dxM) return TW_ERR_INVALID;
+    }
+    TW_CUDA(cudaSetDevice(s->d.device));
+    const long Nxp = Mx_prmt + 1, Nyp = My_prmt + 1, P = (Nxp + 1) * (Nyp + 1);
+    double *buf = nullptr;   // rho, vp, vs, lambda, 2mu, mu on the padded model
+    TW_CUDA(cudaMalloc((void **)&buf, sizeof(double) * 6 * P));
+    double *drho = buf, *dvp = buf + P, *dvs = buf + 2 * P, *lam = buf + 3 * P, *m2 = buf + 4 * P, *mu = buf + 5 * P;
+    int rc = TW_OK;
+    auto done = [&](int code) { cudaStreamSynchronize(s->st); cudaFree(buf); return code; };
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(drho, rho, sizeof(double) * P, cudaMemcpyHostToDevice, s->st)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(dvp, vp, sizeof(double) * P, cudaMemcpyHostToDevice, s->st)) != cudaSuccess)
+        return done(cuda_fail(e, "model upload"));
+    if (s->elastic) e = cudaMemcpyAsync(dvs, vs, sizeof(double) * P, cudaMemcpyHostToDevice, s->st);
+    else e = cudaMemsetAsync(dvs, 0, sizeof(double) * P, s->st);   // acoustic: vs = 0, lambda = rho vp^2
+    if (e != cudaSuccess) return done(cuda_fail(e, "model upload"));
+    cudaMemsetAsync(s->d_err, 0, sizeof(int), s->st);
+    launch_model_derive(drho, dvp, dvs, P, lam, m2, mu, s->st);
+    const int My = (int)s->d.My;
+    struct { int slot, txN, tyN; const double *src; } jobs[5] = {
+        {F_NN, 1, 1, mu}, {F_MN, 0, 1, drho}, {F_NM, 1, 0, drho}, {F_MM0, 0, 0, lam}, {F_MM1, 0, 0, m2}};
+    for (auto &j : jobs) {
+        if (!s->has_slot(j.slot)) continue;
+        launch_interp(s->rows[j.slot], My, j.txN, j.tyN, s->d.num_dx, s->d.den_dx, num_dxM, den_dxM, Nxp, Nyp, j.src,
+                      s->mat[j.slot], s->d_err, s->st);
+        s->mat_set[j.slot] = true;
+    }
+    int herr = 0;
+    if ((e = cudaMemcpyAsync(&herr, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->st)) != cudaSuccess)
+        return done(cuda_fail(e, "model"));
+    if ((e = cudaStreamSynchronize(s->st)) != cudaSuccess) return done(cuda_fail(e, "model"));
+    if (herr) return done(TW_ERR_MODEL_BOUNDS);
+    rc = finalize_material(s);
+    return done(rc);
+}
+
+int tw_set_material_grid(tw_solver *s, int grid, int idx, const double *coef, long ld)
+{
+    if (check(s) || !coef) return TW_ERR_INVALID;
+    const int slot = slot_of(s, grid, idx);
+    if (slot < 0) return TW_ERR_INVALID;
+    if (ld < s->ref_cols[grid]) return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    const long R = s->rows[slot], My = s->d.My;
+    std::vector<double> tmp((size_t)R * My);
+    for (long ix = 0; ix < R; ix++)
+        for (long iy = 0; iy < My; iy++) tmp[ix * My + iy] = coef[ix * ld + iy];
+    TW_CUDA(cudaMemcpyAsync(s->mat[slot], tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice, s->st));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    s->mat_set[slot] = true;
+    s->mat_dirty = true;
+    bool all = true;
+    for (int k = 0; k < 5; k++) all = all && (!s->has_slot(k) || s->mat_set[k]);
+    if (all) {
+        int rc = finalize_material(s);
+        if (rc != TW_OK) return rc;
+        TW_CUDA(cudaStreamSynchronize(s->st));
+    }
+    return TW_OK;
+}
+
+int tw_set_source(tw_solver *s, int grid, long ix, long iy)
+{
+    if (check(s) || grid < 0 || grid > 3) return TW_ERR_INVALID;
+    if (!s->elastic && grid == TW_NN) return TW_ERR_INVALID;
+    if (ix < 0 || iy < 0 || ix >= s->ref_rows[grid] || iy >= s->ref_cols[grid]) return TW_ERR_OUTSIDE;
+    const bool Nx = grid == TW_NN || grid == TW_NM, Ny = grid == TW_NN || grid == TW_MN;
+    if (!s->periodic && Nx && (ix == 0 || ix == s->d.Mx)) return TW_ERR_WEAK_BOUNDARY;   // forward.cpp:95-96
+    // the reference's duplicate column of an N-type-y grid would stop mirroring column 0
+    // (forward_simulation.cpp:116-135); the same holds for the duplicate row under periodic x
+    if (Ny && (iy == 0 || iy == s->d.My)) return TW_ERR_WEAK_BOUNDARY;
+    if (s->periodic && Nx && (ix == 0 || ix == s->d.Mx)) return TW_ERR_WEAK_BOUNDARY;
+    s->src_grid = grid;
+    s->src_ix = ix;
+    s->src_iy = iy;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    return rebuild_source_table(s);
+}
+
+int tw_set_source_location(tw_solver *s, char tx, char ty, long nx, long dx_, long ny, long dy_)
+{
+    if (check(s)) return TW_ERR_INVALID;
+    long ix, iy;
+    if ((tx != 'N' && tx != 'M') || (ty != 'N' && ty != 'M')) return TW_ERR_INVALID;
+    if (!location_to_index(tx, nx, dx_, s->d.num_dx, s->d.den_dx, &ix)) return TW_ERR_LOCATION;
+    if (!location_to_index(ty, ny, dy_, s->d.num_dx, s->d.den_dx, &iy)) return TW_ERR_LOCATION;
+    const int grid = tx == 'N' ? (ty == 'N' ? TW_NN : TW_NM) : (ty == 'N' ? TW_MN : TW_MM);
+    return tw_set_source(s, grid, ix, iy);
+}
+
+int tw_clear_source(tw_solver *s)
+{
+    if (check(s)) return TW_ERR_INVALID;
+    s->src_grid = -1;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    return rebuild_source_table(s);
+}
+
+int tw_add_receivers(tw_solver *s, int grid, const long *ix, const long *iy, int n)
+{
+    if (check(s) || grid < 0 || grid > 3 || n < 0 || (n > 0 && (!ix || !iy))) return TW_ERR_INVALID;
+    if (!s->elastic && grid == TW_NN) return TW_ERR_INVALID;
+    const int s0 = slot_of(s, grid, 0), s1 = slot_of(s, grid, 1);
+    std::vector<int> add;
+    for (int k = 0; k < n; k++) {
+        // the reference accepts indices up to and including the grid size (forward.cpp:154-155);
+        // only points of the grid are accepted here
+        if (ix[k] < 0 || iy[k] < 0 || ix[k] >= s->ref_rows[grid] || iy[k] >= s->ref_cols[grid]) return TW_ERR_OUTSIDE;
+        const long row = ix[k] < s->rows[s0] ? ix[k] : ix[k] - s->rows[s0];   // periodic duplicate row
+        const long col = iy[k] < s->d.My ? iy[k] : iy[k] - s->d.My;            // periodic duplicate column
+        add.insert(add.end(), {s0, s1, (int)row, (int)col});
+    }
+    s->rcv_tab.insert(s->rcv_tab.end(), add.begin(), add.end());
+    TW_CUDA(cudaSetDevice(s->d.device));
+    return upload_receivers(s);
+}
+
+int tw_add_receiver_location(tw_solver *s, char tx, char ty, long nx, long dx_, long ny, long dy_)
+{
+    if (check(s)) return TW_ERR_INVALID;
+    long ix, iy;
+    if ((tx != 'N' && tx != 'M') || (ty != 'N' && ty != 'M')) return TW_ERR_INVALID;
+    if (!location_to_index(tx, nx, dx_, s->d.num_dx, s->d.den_dx, &ix)) return TW_ERR_LOCATION;
+    if (!location_to_index(ty, ny, dy_, s->d.num_dx, s->d.den_dx, &iy)) return TW_ERR_LOCATION;
+    const int grid = tx == 'N' ? (ty == 'N' ? TW_NN : TW_NM) : (ty == 'N' ? TW_MN : TW_MM);
+    return tw_add_receivers(s, grid, &ix, &iy, 1);
+}
+
+int tw_reset(tw_solver *s)
+{
+    if (check(s)) return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    for (int k = 0; k < 5; k++) {
+        if (!s->has_slot(k)) continue;
+        const size_t n = (size_t)s->rows[k] * s->pitch * s->esz;
+        TW_CUDA(cudaMemsetAsync(s->f[k], 0, n, s->st));
+        if (s->res[k]) TW_CUDA(cudaMemsetAsync(s->res[k], 0, n, s->st));
+    }
+    TW_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * 3 * s->d.max_steps, s->st));
+    if (s->d_traces) TW_CUDA(cudaMemsetAsync(s->d_traces, 0, sizeof(double) * 2 * (size_t)s->rcv_cap * s->d.max_steps, s->st));
+    TW_CUDA(cudaMemsetAsync(s->d_step, 0, sizeof(int), s->st));
+    TW_CUDA(cudaMemsetAsync(s->d_flags, 0, sizeof(int), s->st));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    s->steps_done = 0;
+    s->sticky = TW_OK;
+    return TW_OK;
+}
+
+int tw_step(tw_solver *s, int n)
+{
+    if (check(s) || n < 0) return TW_ERR_INVALID;
+    if (!s->mat_ready) return TW_ERR_STATE;
+    if (s->steps_done + (long)n > s->d.max_steps) return TW_ERR_RECORD_FULL;
+    if (n == 0) return TW_OK;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    // a graph of G steps captured once and replayed; leftover steps are launched directly
+    const int G = 16;
+    int left = n;
+    if (n >= G) {
+        if (!s->gexec || s->graph_steps != G) {
+            s->drop_graph();
+            cudaGraph_t graph;
+            TW_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+            enqueue(s, G, s->st);
+            TW_CUDA(cudaStreamEndCapture(s->st, &graph));
+            cudaError_t e = cudaGraphInstantiate(&s->gexec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+            s->graph_steps = G;
+        }
+        while (left >= G) {
+            TW_CUDA(cudaGraphLaunch(s->gexec, s->st));
+            left -= G;
+        }
+    }
+    if (left > 0) enqueue(s, left, s->st);
+    TW_CUDA(cudaGetLastError());
+    s->steps_done += n;
+    return TW_OK;
+}
+
+int tw_sync(tw_solver *s)
+{
+    if (check(s)) return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    int flags = 0;
+    TW_CUDA(cudaMemcpyAsync(&flags, s->d_flags, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    if (flags & FLAG_NONFINITE) s->sticky = TW_ERR_NONFINITE;
+    else if (flags & FLAG_RECORD_FULL) s->sticky = TW_ERR_RECORD_FULL;
+    return s->sticky;
+}
+
+int tw_read_field(tw_solver *s, int grid, int field, double *host, long ld)
+{
+    if (check(s) || !host || grid < 0 || grid > 3) return TW_ERR_INVALID;
+    const int slot = slot_of(s, grid, field);
+    if (slot < 0 || ld < s->ref_cols[grid]) return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    return read_device_array(s, s->f[slot], s->d.precision, s->esz, slot, grid, host, ld);
+}
+
+int tw_write_field(tw_solver *s, int grid, int field, const double *host, long ld)
+{
+    if (check(s) || !host || grid < 0 || grid > 3) return TW_ERR_INVALID;
+    const int slot = slot_of(s, grid, field);
+    if (slot < 0 || ld < s->ref_cols[grid]) return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    return write_device_array(s, s->f[slot], s->d.precision, s->esz, slot, host, ld);
+}
+
+int tw_read_resid(tw_solver *s, int grid, int field, double *host, long ld)
+{
+    if (check(s) || !host || grid < 0 || grid > 3) return TW_ERR_INVALID;
+    const int slot = slot_of(s, grid, field);
+    if (slot < 0 || ld < s->ref_cols[grid] || !s->res[slot]) return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    return read_device_array(s, s->res[slot], s->d.precision, s->esz, slot, grid, host, ld);
+}
+
+int tw_write_resid(tw_solver *s, int grid, int field, const double *host, long ld)
+{
+    if (check(s) || !host || grid < 0 || grid > 3) return TW_ERR_INVALID;
+    const int slot = slot_of(s, grid, field);
+    if (slot < 0 || ld < s->ref_cols[grid] || !s->res[slot]) return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    return write_device_array(s, s->res[slot], s->d.precision, s->esz, slot, host, ld);
+}
+
+int tw_read_receivers(tw_solver *s, double *host)
+{
+    if (check(s) || !host) return TW_ERR_INVALID;
+    const int n = (int)(s->rcv_tab.size() / 4);
+    if (n == 0 || s->steps_done == 0) return TW_OK;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    TW_CUDA(cudaMemcpy2DAsync(host, sizeof(double) * s->steps_done, s->d_traces, sizeof(double) * s->d.max_steps,
+                              sizeof(double) * s->steps_done, 2 * (size_t)n, cudaMemcpyDeviceToHost, s->st));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    return TW_OK;
+}
+
+int tw_read_energy(tw_solver *s, double *E_k, double *E_p0, double *E_p1)
+{
+    if (check(s)) return TW_ERR_INVALID;
+    if (!s->d.energy) return TW_ERR_STATE;
+    const int n = s->steps_done;
+    if (n == 0) return TW_OK;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    std::vector<double> e(3 * (size_t)s->d.max_steps);
+    TW_CUDA(cudaMemcpyAsync(e.data(), s->d_energy, sizeof(double) * e.size(), cudaMemcpyDeviceToHost, s->st));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    const double *p0 = e.data(), *k = e.data() + s->d.max_steps, *p1 = e.data() + 2 * s->d.max_steps;
+    for (int it = 0; it < n; it++) {
+        if (E_k) E_k[it] = k[it];
+        if (E_p1) E_p1[it] = p1[it];
+        if (E_p0) E_p0[it] = s->periodic ? (it > 0 ? p1[it - 1] : 0.) : p0[it];
+    }
+    return TW_OK;
+}
+
+int tw_get_info(tw_solver *s, tw_info *info)
+{
+    if (check(s) || !info) return TW_ERR_INVALID;
+    for (int g = 0; g < 4; g++) { info->rows[g] = s->ref_rows[g]; info->cols[g] = s->ref_cols[g]; }
+    info->pitch = s->pitch;
+    info->steps_done = s->steps_done;
+    info->n_rcv = (int)(s->rcv_tab.size() / 4);
+    const int nf = s->elastic ? 5 : 3;
+    const double csz = s->d.precision == TW_FP64 ? 8 : 4;
+    info->bytes_per_update = nf * (2.0 * s->esz + (s->d.cpst != TW_CPST_00 ? 2.0 * s->esz : 0.0)) + nf * csz;
+    info->device_bytes = s->dev_bytes;
+    return TW_OK;
+}
+
+int tw_profile(tw_solver *s, int n, double *ms)
+{
+    if (check(s) || n < 1 || !ms) return TW_ERR_INVALID;
+    if (!s->mat_ready) return TW_ERR_STATE;
+    if (s->steps_done + (long)n > s->d.max_steps) return TW_ERR_RECORD_FULL;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    std::vector<cudaEvent_t> ev((size_t)8 * n);
+    for (auto &e : ev) TW_CUDA(cudaEventCreate(&e));
+    const bool f64 = s->d.precision == TW_FP64;
+    for (int k = 0; k < n; k++)
+        for (int ph = 0; ph < 4; ph++) {
+            cudaEventRecord(ev[(size_t)8 * k + 2 * ph], s->st);
+            if (ph != 2 || s->d.energy) {
+                if (f64) enqueue_phase<double, double>(s, ph, s->st);
+                else enqueue_phase<float, float>(s, ph, s->st);
+            }
+            cudaEventRecord(ev[(size_t)8 * k + 2 * ph + 1], s->st);
+        }
+    cudaError_t e = cudaStreamSynchronize(s->st);
+    double acc[4] = {0, 0, 0, 0};
+    for (int k = 0; k < n && e == cudaSuccess; k++)
+        for (int ph = 0; ph < 4; ph++) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, ev[(size_t)8 * k + 2 * ph], ev[(size_t)8 * k + 2 * ph + 1]);
+            acc[ph] += t;
+        }
+    for (auto &x : ev) cudaEventDestroy(x);
+    if (e != cudaSuccess) return cuda_fail(e, "tw_profile");
+    for (int ph = 0; ph < 4; ph++) ms[ph] = acc[ph] / n;
+    s->steps_done += n;
+    return TW_OK;
+}
+
+int tw_location_to_index(char type, long num, long den, int num_dx, int den_dx, long *index)
+{
+    if (!index || num_dx <= 0 || den_dx <= 0) return TW_ERR_INVALID;
+    if (type != 'N' && type != 'M') return TW_ERR_INVALID;
+    return location_to_index(type, num, den, num_dx, den_dx, index) ? TW_OK : TW_ERR_LOCATION;
+}
+
+int tw_get_stream(tw_solver *s, void **stream)
+{
+    if (check(s) || !stream) return TW_ERR_INVALID;
+    *stream = (void *)s->st;
+    return TW_OK;
+}
+
+}  // extern "C"

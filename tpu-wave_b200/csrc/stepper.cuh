@@ -1,0 +1,145 @@
+// Kernel arguments and per-point operators of the staggered SBP-SAT stepper.
+//
+// Device layout (all grids): row-major, `pitch` elements per row, x = row. Data-y is periodic
+// with period My for every grid, so the N-type-y grids (NN, MN) keep only columns 0..My-1:
+// the reference's extra column My duplicates column 0 bit for bit (it is computed by the same
+// arithmetic from wrapped reads, grid_drvt.tpp:259-284) and is rebuilt on readback. Rows: N-type
+// x grids have Mx+1 rows with free-surface (SAT) ends, Mx rows when x is periodic.
+#pragma once
+#include "device_math.cuh"
+#include "sbp.hpp"
+
+namespace tw {
+
+enum { G_NN = 0, G_MN = 1, G_NM = 2, G_MM = 3 };
+enum { F_NN = 0, F_MN = 1, F_NM = 2, F_MM0 = 3, F_MM1 = 4 };
+enum { FLAG_NONFINITE = 1, FLAG_RECORD_FULL = 2 };
+
+template <class S, class C>
+struct StepArgs {
+    S *f[5];              // fields NN, MN, NM, MM0 (sxx / p), MM1 (syy)
+    S *res[5];            // compensation arrays (R or C), null without compensation
+    const C *coef[5];     // NN mu, MN 1/rho, NM 1/rho, MM lambda (kappa), MM 2mu
+    long pitch;
+    int Mx, My;
+    Ops<C> op;
+    const double *src_inc;    // per-step source increment A(t) dt / dx^2 / scaling
+    int src_grid, src_ix, src_iy;
+    int max_steps;
+    const int *step;          // device step counter (read by every kernel of a step)
+    int *flags;               // sticky error flags
+};
+
+__device__ __forceinline__ int wrap(int j, int n) { return j < 0 ? j + n : (j >= n ? j - n : j); }
+
+template <class C, class S>
+__device__ __forceinline__ C ld(const S *p, long i) { return to_c<C>(__ldg(p + i)); }
+template <class C>
+__device__ __forceinline__ C ld(const __nv_bfloat16 *p, long i) { return to_c<C>(p[i]); }
+template <class C>
+__device__ __forceinline__ C ld(const __half *p, long i) { return to_c<C>(p[i]); }
+
+// derivative along x of an M-type-x grid (rows 0..Mx-1) from its N-type neighbour with rows
+// 0..Mx: DN closures on 3 rows at each end, interior shifts {-1,0,1,2} (grid_drvt.tpp:312-466,
+// grid.hpp:361-362).
+template <class C, class S>
+__device__ __forceinline__ C dx_from_N(const Ops<C> &o, const S *nb, long pitch, int Mx, int ix, int iy)
+{
+    C v = C(0);
+    if (ix < 3) {
+#pragma unroll
+        for (int w = 0; w < 5; w++) v = add(v, mul(ld<C>(nb, (long)w * pitch + iy), o.dnL[ix][w]));
+    } else if (ix >= Mx - 3) {
+        const int r = ix - (Mx - 3);
+#pragma unroll
+        for (int w = 0; w < 5; w++) v = add(v, mul(ld<C>(nb, (long)(Mx - 4 + w) * pitch + iy), o.dnR[r][w]));
+    } else {
+#pragma unroll
+        for (int w = 0; w < 4; w++) v = add(v, mul(ld<C>(nb, (long)(ix - 1 + w) * pitch + iy), o.st[w]));
+    }
+    return v;
+}
+
+// derivative along x of an N-type-x grid (rows 0..Mx) from its M-type neighbour with rows
+// 0..Mx-1: DM closures on 4 rows at each end, interior shifts {-2,-1,0,1}.
+template <class C, class S>
+__device__ __forceinline__ C dx_from_M(const Ops<C> &o, const S *nb, long pitch, int Mx, int ix, int iy)
+{
+    C v = C(0);
+    if (ix < 4) {
+#pragma unroll
+        for (int w = 0; w < 5; w++) v = add(v, mul(ld<C>(nb, (long)w * pitch + iy), o.dmL[ix][w]));
+    } else if (ix >= Mx - 3) {
+        const int r = ix - (Mx - 3);
+#pragma unroll
+        for (int w = 0; w < 5; w++) v = add(v, mul(ld<C>(nb, (long)(Mx - 5 + w) * pitch + iy), o.dmR[r][w]));
+    } else {
+#pragma unroll
+        for (int w = 0; w < 4; w++) v = add(v, mul(ld<C>(nb, (long)(ix - 2 + w) * pitch + iy), o.st[w]));
+    }
+    return v;
+}
+
+// periodic x derivative (single-core acoustic tree): first index offset lo = -2 for N-type
+// rows reading M-type rows, -1 for M-type rows reading N-type rows
+template <class C, class S>
+__device__ __forceinline__ C dx_periodic(const Ops<C> &o, const S *nb, long pitch, int Mx, int ix, int iy, int lo)
+{
+    C v = C(0);
+#pragma unroll
+    for (int w = 0; w < 4; w++) v = add(v, mul(ld<C>(nb, (long)wrap(ix + lo + w, Mx) * pitch + iy), o.st[w]));
+    return v;
+}
+
+// periodic y derivative: lo = -2 on N-type-y grids (reading M-type columns), -1 on M-type-y
+// grids (grid.hpp:361-362, grid_drvt.tpp:45-167 with N_modulo = My)
+template <class C, class S>
+__device__ __forceinline__ C dy_periodic(const Ops<C> &o, const S *row, int My, int iy, int lo)
+{
+    C v = C(0);
+#pragma unroll
+    for (int w = 0; w < 4; w++) v = add(v, mul(ld<C>(row, (long)wrap(iy + lo + w, My)), o.st[w]));
+    return v;
+}
+
+// SAT penalty of the M-type-x velocity grid MN (rows 0..2 and Mx-3..Mx-1): the boundary value
+// of the NN neighbour (projection {1}) times eta*A_inv_projection (grid_drvt.tpp:563-693)
+template <class C, class S>
+__device__ __forceinline__ bool sat_MN(const Ops<C> &o, const S *nn, long pitch, int Mx, int ix, int iy, C &v)
+{
+    if (ix < 3) {
+        const C send = add(C(0), mul(o.pN, ld<C>(nn, iy)));
+        v = mul(o.satML[ix], sub(send, C(0)));
+        return true;
+    }
+    if (ix >= Mx - 3) {
+        const C send = add(C(0), mul(o.pN, ld<C>(nn, (long)Mx * pitch + iy)));
+        v = mul(o.satMR[ix - (Mx - 3)], sub(send, C(0)));
+        return true;
+    }
+    return false;
+}
+
+// SAT penalty of the N-type-x velocity grid NM (rows 0 and Mx): sxx extrapolated to the
+// boundary with {15/8, -5/4, 3/8} over three MM rows
+template <class C, class S>
+__device__ __forceinline__ bool sat_NM(const Ops<C> &o, const S *mm, long pitch, int Mx, int ix, int iy, C &v)
+{
+    if (ix == 0) {
+        C send = C(0);
+#pragma unroll
+        for (int w = 0; w < 3; w++) send = add(send, mul(o.pML[w], ld<C>(mm, (long)w * pitch + iy)));
+        v = mul(o.satNL, sub(send, C(0)));
+        return true;
+    }
+    if (ix == Mx) {
+        C send = C(0);
+#pragma unroll
+        for (int w = 0; w < 3; w++) send = add(send, mul(o.pMR[w], ld<C>(mm, (long)(Mx - 3 + w) * pitch + iy)));
+        v = mul(o.satNR, sub(send, C(0)));
+        return true;
+    }
+    return false;
+}
+
+}  // namespace tw
