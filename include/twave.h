@@ -38,8 +38,7 @@ enum {
     TW_ERR_STATE = -4,          /* call out of order (e.g. stepping before the material is set) */
     TW_ERR_LOCATION = -5,       /* location is not a grid point (forward.cpp:38-39,48-49) */
     TW_ERR_OUTSIDE = -6,        /* location outside the grid (forward.cpp:91) */
-    TW_ERR_WEAK_BOUNDARY = -7,  /* source on an SAT boundary node (forward.cpp:95-96) or on the
-                                   periodic seam of an N-type-y grid (forward_simulation.cpp:116-135) */
+    TW_ERR_WEAK_BOUNDARY = -7,  /* source on an SAT free-surface node row (forward.cpp:95-96) */
     TW_ERR_RECORD_FULL = -8,    /* more steps than the trace/energy records hold */
     TW_ERR_NONFINITE = -9,      /* a NaN/Inf appeared in a field (sticky, reported by tw_sync) */
     TW_ERR_UNSUPPORTED = -10,   /* combination not implemented (e.g. elastic with periodic x) */
@@ -133,7 +132,7 @@ TW_API int tw_sync(tw_solver *s);
 /* Field readback in the reference layout (copy_field_pitched dev_to_hst, grid.cuh:463-469):
  * rows x cols of the grid, row stride ld >= cols, converted to double. field: 0, or 1 for syy on MM. */
 TW_API int tw_read_field(tw_solver *s, int grid, int field, double *host, long ld);
-/* Set a field from the host (reference layout); the periodic duplicate column (and row) is ignored. */
+/* Set a field from the host (reference layout). */
 TW_API int tw_write_field(tw_solver *s, int grid, int field, const double *host, long ld);
 /* Compensation arrays (Vec_rths for 'R' codes, Vec_cpst for 'C' codes), same layout. */
 TW_API int tw_read_resid(tw_solver *s, int grid, int field, double *host, long ld);

@@ -27,12 +27,12 @@ void launch_model_derive(const double *rho, const double *vp, const double *vs, 
 // interpolate_forward_parameter (grid_parameter.cpp:13-57): the location of grid point (ix, iy)
 // in units of the model spacing is num/den; its integer part indexes the padded model, the
 // remainder (computed in double) weights the four corners.
-__global__ void k_interp(int rows, int My, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
+__global__ void k_interp(int rows, int cols, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
                          long Nxp, long Nyp, const double *in, double *out, int *err)
 {
     const int iy = blockIdx.x * blockDim.x + threadIdx.x;
     const int ix = blockIdx.y * blockDim.y + threadIdx.y;
-    if (iy >= My || ix >= rows) return;
+    if (iy >= cols || ix >= rows) return;
     long nx, dxl, ny, dyl;
     if (txN) { nx = (long)ix * num_dx; dxl = den_dx; } else { nx = (2L * ix + 1) * num_dx; dxl = 2L * den_dx; }
     if (tyN) { ny = (long)iy * num_dx; dyl = den_dx; } else { ny = (2L * iy + 1) * num_dx; dyl = 2L * den_dx; }
@@ -47,14 +47,14 @@ __global__ void k_interp(int rows, int My, int txN, int tyN, int num_dx, int den
     v = add(v, mul(mul(a, eta), in[ixM * PS + iyM + 1]));
     v = add(v, mul(mul(xi, b), in[(ixM + 1) * PS + iyM]));
     v = add(v, mul(mul(xi, eta), in[(ixM + 1) * PS + iyM + 1]));
-    out[(long)ix * My + iy] = v;
+    out[(long)ix * cols + iy] = v;
 }
 
-void launch_interp(int rows, int My, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
+void launch_interp(int rows, int cols, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
                    long Nx_prmt, long Ny_prmt, const double *in, double *out, int *err, cudaStream_t st)
 {
-    const dim3 b(32, 8), g((My + 31) / 32, (rows + 7) / 8);
-    k_interp<<<g, b, 0, st>>>(rows, My, txN, tyN, num_dx, den_dx, num_dxM, den_dxM, Nx_prmt, Ny_prmt, in, out, err);
+    const dim3 b(32, 8), g((cols + 31) / 32, (rows + 7) / 8);
+    k_interp<<<g, b, 0, st>>>(rows, cols, txN, tyN, num_dx, den_dx, num_dxM, den_dxM, Nx_prmt, Ny_prmt, in, out, err);
 }
 
 // x factor of the energy norm for row ix of a grid with `rows` rows (adjust_parameters_energy_periodic,
@@ -77,52 +77,65 @@ __global__ void k_material_finalize(MaterialArgs m)
 {
     const int iy = blockIdx.x * blockDim.x + threadIdx.x;
     const int ix = blockIdx.y * blockDim.y + threadIdx.y;
-    if (iy >= m.My) return;
-    const long i = (long)ix * m.My + iy;       // compact FP64 input
-    const long o = (long)ix * m.pitch + iy;    // device layout
     const double dx = m.dx;
-    const double w_sc = mul(dx, dx) / 2.;      // single-core weight dx*dx/2 (namespaces.hpp:754)
     const bool elastic = m.physics == 0;
     C **coef = (C **)m.coef;
+    // y factor of the norm (grid_energy.cpp:123-152): dx everywhere, then 1 on the first and 0 on
+    // the last (duplicate) point of an N-type-y grid
+    auto y_factor = [&](int g, double w) {
+        w = mul(w, dx);
+        if (m.cols[g] == m.My + 1 && iy == m.My) w = mul(w, 0.);
+        return w;
+    };
+    // single-core weights (namespaces.hpp:734-776): dx*dx/2, halved on the end points of an N direction
+    auto sc_weight = [&](int g) {
+        double w = mul(dx, dx) / 2.;
+        if (m.cols[g] == m.My + 1 && (iy == 0 || iy == m.My)) w = w / 2.;
+        if (m.rows[g] == m.Mx + 1 && (ix == 0 || ix == m.Mx)) w = w / 2.;
+        return w;
+    };
     // NN (elastic only): mu, weight 1/mu
-    if (elastic && ix < m.rows[F_NN]) {
+    if (elastic && ix < m.rows[F_NN] && iy < m.cols[F_NN]) {
+        const long i = (long)ix * m.cols[F_NN] + iy, o = (long)ix * m.pitch + iy;
         const C mu = (C)m.mat[F_NN][i];
         coef[F_NN][o] = mu;
         double w = __ddiv_rn(1., (double)mu);
         w = mul(w, norm_x(m, 1, m.rows[F_NN], ix));
-        m.w[F_NN][o] = mul(w, dx);
+        m.w[F_NN][o] = y_factor(F_NN, w);
     }
     // velocity grids: 1/rho from the FP64 density (make_density_reciprocal), weight rho
     for (int g = F_MN; g <= F_NM; g++) {
-        if (ix >= m.rows[g]) continue;
+        if (ix >= m.rows[g] || iy >= m.cols[g]) continue;
+        const long i = (long)ix * m.cols[g] + iy, o = (long)ix * m.pitch + iy;
         const double rho = m.mat[g][i];
         coef[g][o] = (C)__ddiv_rn(1., rho);
         if (m.periodic) {
-            m.w[g][o] = w_sc;
+            m.w[g][o] = sc_weight(g);
         } else {
             double w = (double)(C)rho;
             w = mul(w, norm_x(m, g == F_NM, m.rows[g], ix));
-            m.w[g][o] = mul(w, dx);
+            m.w[g][o] = y_factor(g, w);
         }
     }
-    if (ix < m.rows[F_MM0]) {
+    if (ix < m.rows[F_MM0] && iy < m.cols[F_MM0]) {
+        const long i = (long)ix * m.cols[F_MM0] + iy, o = (long)ix * m.pitch + iy;
         const C lam = (C)m.mat[F_MM0][i];
         coef[F_MM0][o] = lam;
-        const double fx = norm_x(m, 0, m.rows[F_MM0], ix);
+        const double fx = m.periodic ? 0. : norm_x(m, 0, m.rows[F_MM0], ix);
         if (elastic) {
             const C m2 = (C)m.mat[F_MM1][i];
             coef[F_MM1][o] = m2;
             const double l = (double)lam, t = (double)m2;
             const double den = mul(t, add(mul(2., l), t));
-            double w1 = __ddiv_rn(add(l, t), den);
-            double w2 = -__ddiv_rn(mul(l, 2.), den);
-            m.w[F_MM0][o] = mul(mul(w1, fx), dx);
-            m.w[F_MM1][o] = mul(mul(w2, fx), dx);
+            const double w1 = __ddiv_rn(add(l, t), den);
+            const double w2 = -__ddiv_rn(mul(l, 2.), den);
+            m.w[F_MM0][o] = y_factor(F_MM0, mul(w1, fx));
+            m.w[F_MM1][o] = y_factor(F_MM1, mul(w2, fx));
         } else if (m.periodic) {
-            m.w[F_MM0][o] = w_sc;
+            m.w[F_MM0][o] = sc_weight(F_MM0);
         } else {
             // acoustic free surface: the mu -> 0 limit of the elastic weights, (2 P1 + P2) -> 1/kappa
-            m.w[F_MM0][o] = mul(mul(__ddiv_rn(1., (double)lam), fx), dx);
+            m.w[F_MM0][o] = y_factor(F_MM0, mul(__ddiv_rn(1., (double)lam), fx));
         }
     }
 }
@@ -130,9 +143,7 @@ __global__ void k_material_finalize(MaterialArgs m)
 template <class C>
 void launch_material_finalize(const MaterialArgs &m, cudaStream_t st)
 {
-    const int rows = m.rows[F_NM] > m.rows[F_MM0] ? m.rows[F_NM] : m.rows[F_MM0];
-    const int rmax = m.rows[F_NN] > rows ? m.rows[F_NN] : rows;
-    const dim3 b(32, 8), g((m.My + 31) / 32, (rmax + 7) / 8);
+    const dim3 b(32, 8), g((m.My + 1 + 31) / 32, (m.Mx + 1 + 7) / 8);
     k_material_finalize<C><<<g, b, 0, st>>>(m);
 }
 template void launch_material_finalize<double>(const MaterialArgs &, cudaStream_t);
@@ -151,15 +162,18 @@ __global__ void __launch_bounds__(256) k_energy(EnergyArgs<S, C> e)
 {
     const int it = *e.step;
     if (it >= e.max_steps) return;
-    int rmax = 0;
-    for (int t = 0; t < e.nterms; t++) rmax = e.rows[t] > rmax ? e.rows[t] : rmax;
-    const long n = (long)rmax * e.My;
+    int rmax = 0, cmax = 0;
+    for (int t = 0; t < e.nterms; t++) {
+        rmax = e.rows[t] > rmax ? e.rows[t] : rmax;
+        cmax = e.cols[t] > cmax ? e.cols[t] : cmax;
+    }
+    const long n = (long)rmax * cmax;
     double acc = 0.;
     for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < n; k += (long)gridDim.x * blockDim.x) {
-        const int ix = (int)(k / e.My), iy = (int)(k - (long)ix * e.My);
+        const int ix = (int)(k / cmax), iy = (int)(k - (long)ix * cmax);
         const long o = (long)ix * e.pitch + iy;
         for (int t = 0; t < e.nterms; t++) {
-            if (ix >= e.rows[t]) continue;
+            if (ix >= e.rows[t] || iy >= e.cols[t]) continue;
             if (e.single_core) {   // soln * prmt * soln * weight (cpu_acoustic.cpp:341)
                 const C s = to_c<C>(e.a[t][o]);
                 acc = add(acc, mul((double)mul(mul(s, e.p[t][o]), s), e.w[t][o]));

@@ -14,17 +14,16 @@ void launch_half(int physics, int periodic, int cpst, int half, const StepArgs<S
 void launch_model_derive(const double *rho, const double *vp, const double *vs, long n, double *lam,
                          double *m2, double *mu, cudaStream_t st);
 
-// bilinear interpolation onto one grid (grid_parameter.cpp:7-60); out: rows x My, row pitch My
-// (the periodic duplicate column of N-type-y grids is not produced). err: set to 1 on an
-// out-of-bounds model access.
-void launch_interp(int rows, int My, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
+// bilinear interpolation onto one grid (grid_parameter.cpp:7-60); out: rows x cols, compact.
+// err: set to 1 on an out-of-bounds model access.
+void launch_interp(int rows, int cols, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
                    long Nx_prmt, long Ny_prmt, const double *in, double *out, int *err, cudaStream_t st);
 
 struct MaterialArgs {
-    const double *mat[5];     // FP64 NN mu, MN rho, NM rho, MM lambda (kappa), MM 2mu; rows x My
+    const double *mat[5];     // FP64 NN mu, MN rho, NM rho, MM lambda (kappa), MM 2mu; rows x cols
     void *coef[5];            // stored stepping coefficients (compute type), rows x pitch
     double *w[5];             // energy weights, rows x pitch (w[4] = P2 on MM)
-    int rows[5];
+    int rows[5], cols[5];
     int Mx, My;
     long pitch;
     double dx;
@@ -42,9 +41,8 @@ struct EnergyArgs {
     const S *b[4];
     const double *w[4];
     const C *p[4];            // single-core form ((s p) s) w uses the stepping coefficient
-    int rows[4];
+    int rows[4], cols[4];
     int nterms;
-    int My;
     long pitch;
     double scale;             // 1/2 for the SBP energy (grid_energy.cpp:215), 1 for the single-core sums
     int single_core;

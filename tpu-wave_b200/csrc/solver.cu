@@ -61,7 +61,8 @@ struct tw_solver {
     int elastic = 1, periodic = 0;
     int esz = 4;                      // bytes per stored field value
     long pitch = 0;
-    int rows[5] = {0, 0, 0, 0, 0};    // device rows per field slot (0: slot unused)
+    int rows[5] = {0, 0, 0, 0, 0};    // rows per field slot (0: slot unused)
+    int cols[5] = {0, 0, 0, 0, 0};    // columns per field slot
     long ref_rows[4], ref_cols[4];    // reference sizes per grid
     cudaStream_t st = nullptr;
     void *f[5] = {}, *res[5] = {}, *coef[5] = {};
@@ -151,7 +152,6 @@ void energy_phase(const tw_solver *s, int phase, cudaStream_t st)
 {
     // phase 0: E_p0 (stresses before the step), 1: E_k (velocities), 2: E_p1 (stresses after)
     EnergyArgs<S, C> e{};
-    e.My = (int)s->d.My;
     e.pitch = s->pitch;
     e.max_steps = s->d.max_steps;
     e.step = s->d_step;
@@ -165,6 +165,7 @@ void energy_phase(const tw_solver *s, int phase, cudaStream_t st)
         e.w[t] = s->w[wslot];
         e.p[t] = (const C *)s->coef[pslot];
         e.rows[t] = s->rows[a];
+        e.cols[t] = s->cols[a];
     };
     if (phase == 1) {
         term(F_MN, F_MN, F_MN, F_MN);
@@ -246,6 +247,7 @@ int finalize_material(tw_solver *s)
         m.coef[k] = s->coef[k];
         m.w[k] = s->w[k];
         m.rows[k] = s->rows[k];
+        m.cols[k] = s->cols[k];
     }
     m.Mx = (int)s->d.Mx;
     m.My = (int)s->d.My;
@@ -332,35 +334,27 @@ double from_storage(int prec, const void *src, long i)
     return (double)__half2float(((const __half *)src)[i]);
 }
 
-// copy a device-layout array (rows x pitch) of `esz`-byte values to the host in the reference
-// layout: an extra periodic duplicate column (N-type y) and row (N-type x with periodic x) repeat
-// column / row 0
-int read_device_array(tw_solver *s, const void *dev, int prec, int esz, int slot, int grid, double *host, long ld)
+// copy a device array (rows x pitch) of `esz`-byte values to the host in the reference layout
+int read_device_array(tw_solver *s, const void *dev, int prec, int esz, int slot, double *host, long ld)
 {
-    const long R = s->rows[slot], My = s->d.My;
-    std::vector<char> buf((size_t)R * My * esz);
-    TW_CUDA(cudaMemcpy2DAsync(buf.data(), My * esz, dev, s->pitch * esz, My * esz, R, cudaMemcpyDeviceToHost, s->st));
+    const long R = s->rows[slot], Cn = s->cols[slot];
+    std::vector<char> buf((size_t)R * Cn * esz);
+    TW_CUDA(cudaMemcpy2DAsync(buf.data(), Cn * esz, dev, s->pitch * esz, Cn * esz, R, cudaMemcpyDeviceToHost, s->st));
     TW_CUDA(cudaStreamSynchronize(s->st));
-    const long rr = s->ref_rows[grid], rc = s->ref_cols[grid];
-    for (long ix = 0; ix < rr; ix++) {
-        const long sx = ix < R ? ix : ix - R;
-        for (long iy = 0; iy < rc; iy++) {
-            const long sy = iy < My ? iy : iy - My;
-            host[ix * ld + iy] = from_storage(prec, buf.data(), sx * My + sy);
-        }
-    }
+    for (long ix = 0; ix < R; ix++)
+        for (long iy = 0; iy < Cn; iy++) host[ix * ld + iy] = from_storage(prec, buf.data(), ix * Cn + iy);
     return TW_OK;
 }
 
 int write_device_array(tw_solver *s, void *dev, int prec, int esz, int slot, const double *host, long ld)
 {
-    const long R = s->rows[slot], My = s->d.My;
-    std::vector<double> tmp((size_t)R * My);
+    const long R = s->rows[slot], Cn = s->cols[slot];
+    std::vector<double> tmp((size_t)R * Cn);
     for (long ix = 0; ix < R; ix++)
-        for (long iy = 0; iy < My; iy++) tmp[ix * My + iy] = host[ix * ld + iy];
-    std::vector<char> buf((size_t)R * My * esz);
-    to_storage(prec, tmp.data(), buf.data(), R * My);
-    TW_CUDA(cudaMemcpy2DAsync(dev, s->pitch * esz, buf.data(), My * esz, My * esz, R, cudaMemcpyHostToDevice, s->st));
+        for (long iy = 0; iy < Cn; iy++) tmp[ix * Cn + iy] = host[ix * ld + iy];
+    std::vector<char> buf((size_t)R * Cn * esz);
+    to_storage(prec, tmp.data(), buf.data(), R * Cn);
+    TW_CUDA(cudaMemcpy2DAsync(dev, s->pitch * esz, buf.data(), Cn * esz, Cn * esz, R, cudaMemcpyHostToDevice, s->st));
     TW_CUDA(cudaStreamSynchronize(s->st));
     s->drop_graph();
     return TW_OK;
@@ -419,18 +413,19 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
     s->elastic = d.physics == TW_ELASTIC;
     s->periodic = d.bc_x == TW_BC_PERIODIC;
     s->esz = d.precision == TW_FP64 ? 8 : (d.precision == TW_FP32 ? 4 : 2);
-    const int rowsN = s->periodic ? (int)d.Mx : (int)d.Mx + 1;
-    s->rows[F_NN] = s->elastic ? rowsN : 0;
-    s->rows[F_MN] = (int)d.Mx;
-    s->rows[F_NM] = rowsN;
-    s->rows[F_MM0] = (int)d.Mx;
-    s->rows[F_MM1] = s->elastic ? (int)d.Mx : 0;
+    const int Mx_ = (int)d.Mx, My_ = (int)d.My;
+    const int rws[5] = {Mx_ + 1, Mx_, Mx_ + 1, Mx_, Mx_}, cls[5] = {My_ + 1, My_ + 1, My_, My_, My_};
+    for (int k = 0; k < 5; k++) {
+        const bool used = s->elastic || (k != F_NN && k != F_MM1);
+        s->rows[k] = used ? rws[k] : 0;
+        s->cols[k] = used ? cls[k] : 0;
+    }
     const long Mx = d.Mx, My = d.My;
     const long rr[4] = {Mx + 1, Mx, Mx + 1, Mx}, rc[4] = {My + 1, My + 1, My, My};
     for (int g = 0; g < 4; g++) { s->ref_rows[g] = rr[g]; s->ref_cols[g] = rc[g]; }
     // rows padded to a multiple of 128 bytes so that every row starts aligned
     const long align = 128 / s->esz;
-    s->pitch = (My + align - 1) / align * align;
+    s->pitch = (My + 1 + align - 1) / align * align;
 
     int rc_ = TW_OK;
     auto fail = [&](int code) { delete s; return code; };
@@ -447,7 +442,7 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
         if (cp && (rc_ = s->alloc(&s->res[k], n * s->esz)) != TW_OK) return fail(rc_);
         if ((rc_ = s->alloc(&s->coef[k], n * csz)) != TW_OK) return fail(rc_);
         if ((rc_ = s->alloc((void **)&s->w[k], n * sizeof(double))) != TW_OK) return fail(rc_);
-        if ((rc_ = s->alloc((void **)&s->mat[k], (size_t)s->rows[k] * My * sizeof(double))) != TW_OK) return fail(rc_);
+        if ((rc_ = s->alloc((void **)&s->mat[k], (size_t)s->rows[k] * s->cols[k] * sizeof(double))) != TW_OK) return fail(rc_);
         cudaMemsetAsync(s->f[k], 0, n * s->esz, s->st);
         if (cp) cudaMemsetAsync(s->res[k], 0, n * s->esz, s->st);
         cudaMemsetAsync(s->coef[k], 0, n * csz, s->st);
@@ -503,12 +498,11 @@ int tw_set_material_model(tw_solver *s, const double *rho, const double *vp, con
     if (e != cudaSuccess) return done(cuda_fail(e, "model upload"));
     cudaMemsetAsync(s->d_err, 0, sizeof(int), s->st);
     launch_model_derive(drho, dvp, dvs, P, lam, m2, mu, s->st);
-    const int My = (int)s->d.My;
     struct { int slot, txN, tyN; const double *src; } jobs[5] = {
         {F_NN, 1, 1, mu}, {F_MN, 0, 1, drho}, {F_NM, 1, 0, drho}, {F_MM0, 0, 0, lam}, {F_MM1, 0, 0, m2}};
     for (auto &j : jobs) {
         if (!s->has_slot(j.slot)) continue;
-        launch_interp(s->rows[j.slot], My, j.txN, j.tyN, s->d.num_dx, s->d.den_dx, num_dxM, den_dxM, Nxp, Nyp, j.src,
+        launch_interp(s->rows[j.slot], s->cols[j.slot], j.txN, j.tyN, s->d.num_dx, s->d.den_dx, num_dxM, den_dxM, Nxp, Nyp, j.src,
                       s->mat[j.slot], s->d_err, s->st);
         s->mat_set[j.slot] = true;
     }
@@ -528,10 +522,10 @@ int tw_set_material_grid(tw_solver *s, int grid, int idx, const double *coef, lo
     if (slot < 0) return TW_ERR_INVALID;
     if (ld < s->ref_cols[grid]) return TW_ERR_INVALID;
     TW_CUDA(cudaSetDevice(s->d.device));
-    const long R = s->rows[slot], My = s->d.My;
-    std::vector<double> tmp((size_t)R * My);
+    const long R = s->rows[slot], Cn = s->cols[slot];
+    std::vector<double> tmp((size_t)R * Cn);
     for (long ix = 0; ix < R; ix++)
-        for (long iy = 0; iy < My; iy++) tmp[ix * My + iy] = coef[ix * ld + iy];
+        for (long iy = 0; iy < Cn; iy++) tmp[ix * Cn + iy] = coef[ix * ld + iy];
     TW_CUDA(cudaMemcpyAsync(s->mat[slot], tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice, s->st));
     TW_CUDA(cudaStreamSynchronize(s->st));
     s->mat_set[slot] = true;
@@ -551,12 +545,10 @@ int tw_set_source(tw_solver *s, int grid, long ix, long iy)
     if (check(s) || grid < 0 || grid > 3) return TW_ERR_INVALID;
     if (!s->elastic && grid == TW_NN) return TW_ERR_INVALID;
     if (ix < 0 || iy < 0 || ix >= s->ref_rows[grid] || iy >= s->ref_cols[grid]) return TW_ERR_OUTSIDE;
-    const bool Nx = grid == TW_NN || grid == TW_NM, Ny = grid == TW_NN || grid == TW_MN;
-    if (!s->periodic && Nx && (ix == 0 || ix == s->d.Mx)) return TW_ERR_WEAK_BOUNDARY;   // forward.cpp:95-96
-    // the reference's duplicate column of an N-type-y grid would stop mirroring column 0
-    // (forward_simulation.cpp:116-135); the same holds for the duplicate row under periodic x
-    if (Ny && (iy == 0 || iy == s->d.My)) return TW_ERR_WEAK_BOUNDARY;
-    if (s->periodic && Nx && (ix == 0 || ix == s->d.Mx)) return TW_ERR_WEAK_BOUNDARY;
+    const bool Nx = grid == TW_NN || grid == TW_NM;
+    // the reference stops on a source on the free-surface node rows (forward.cpp:95-96); on the
+    // periodic seam it only warns (:97-98) and so does nothing here
+    if (!s->periodic && Nx && (ix == 0 || ix == s->d.Mx)) return TW_ERR_WEAK_BOUNDARY;
     s->src_grid = grid;
     s->src_ix = ix;
     s->src_iy = iy;
@@ -593,9 +585,7 @@ int tw_add_receivers(tw_solver *s, int grid, const long *ix, const long *iy, int
         // the reference accepts indices up to and including the grid size (forward.cpp:154-155);
         // only points of the grid are accepted here
         if (ix[k] < 0 || iy[k] < 0 || ix[k] >= s->ref_rows[grid] || iy[k] >= s->ref_cols[grid]) return TW_ERR_OUTSIDE;
-        const long row = ix[k] < s->rows[s0] ? ix[k] : ix[k] - s->rows[s0];   // periodic duplicate row
-        const long col = iy[k] < s->d.My ? iy[k] : iy[k] - s->d.My;            // periodic duplicate column
-        add.insert(add.end(), {s0, s1, (int)row, (int)col});
+        add.insert(add.end(), {s0, s1, (int)ix[k], (int)iy[k]});
     }
     s->rcv_tab.insert(s->rcv_tab.end(), add.begin(), add.end());
     TW_CUDA(cudaSetDevice(s->d.device));
@@ -684,7 +674,7 @@ int tw_read_field(tw_solver *s, int grid, int field, double *host, long ld)
     const int slot = slot_of(s, grid, field);
     if (slot < 0 || ld < s->ref_cols[grid]) return TW_ERR_INVALID;
     TW_CUDA(cudaSetDevice(s->d.device));
-    return read_device_array(s, s->f[slot], s->d.precision, s->esz, slot, grid, host, ld);
+    return read_device_array(s, s->f[slot], s->d.precision, s->esz, slot, host, ld);
 }
 
 int tw_write_field(tw_solver *s, int grid, int field, const double *host, long ld)
@@ -702,7 +692,7 @@ int tw_read_resid(tw_solver *s, int grid, int field, double *host, long ld)
     const int slot = slot_of(s, grid, field);
     if (slot < 0 || ld < s->ref_cols[grid] || !s->res[slot]) return TW_ERR_INVALID;
     TW_CUDA(cudaSetDevice(s->d.device));
-    return read_device_array(s, s->res[slot], s->d.precision, s->esz, slot, grid, host, ld);
+    return read_device_array(s, s->res[slot], s->d.precision, s->esz, slot, host, ld);
 }
 
 int tw_write_resid(tw_solver *s, int grid, int field, const double *host, long ld)

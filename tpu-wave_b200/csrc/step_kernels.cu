@@ -38,34 +38,34 @@ __global__ void __launch_bounds__(256) k_elastic_velocity(StepArgs<S, C> a)
 {
     const int iy = blockIdx.x * blockDim.x + threadIdx.x;
     const int ix = blockIdx.y * blockDim.y + threadIdx.y;
-    if (iy >= a.My || ix > a.Mx) return;
+    if (iy > a.My || ix > a.Mx) return;
     const int it = *a.step;
     const long pitch = a.pitch;
     const long i = (long)ix * pitch + iy;
     constexpr bool kr = Cpst<CPST>::keep_r, kc = Cpst<CPST>::keep_c;
 
-    if (ix < a.Mx) {   // MN: velocity along y; x from NN, y from MM syy
+    if (ix < a.Mx) {   // MN (Mx x My+1): velocity along y; x from NN, y from MM syy
         C r, c;
         load_rc<S, C, CPST>(a.res[F_MN], i, r, c);
         const C P = __ldg(a.coef[F_MN] + i);
         C v = dx_from_N<C>(a.op, a.f[F_NN], pitch, a.Mx, ix, iy);
         r = add(r, mul(v, P));
         if (sat_MN<C>(a.op, a.f[F_NN], pitch, a.Mx, ix, iy, v)) r = add(r, mul(v, P));
-        v = dy_periodic<C>(a.op, a.f[F_MM1] + (long)ix * pitch, a.My, iy, -2);
+        v = dy_periodic<false, C>(a.op, a.f[F_MM1] + (long)ix * pitch, a.My, iy);
         r = add(r, mul(v, P));
         C s = to_c<C>(a.f[F_MN][i]);
         time_update<CPST>(s, r, c);
         finish_point(a.f[F_MN], a.res[F_MN], i, s, r, c, kr, kc,
                      a.src_grid == G_MN && ix == a.src_ix && iy == a.src_iy, a.src_inc, it, a.flags);
     }
-    {   // NM: velocity along x; x from MM sxx, y from NN
+    if (iy < a.My) {   // NM (Mx+1 x My): velocity along x; x from MM sxx, y from NN
         C r, c;
         load_rc<S, C, CPST>(a.res[F_NM], i, r, c);
         const C P = __ldg(a.coef[F_NM] + i);
         C v = dx_from_M<C>(a.op, a.f[F_MM0], pitch, a.Mx, ix, iy);
         r = add(r, mul(v, P));
         if (sat_NM<C>(a.op, a.f[F_MM0], pitch, a.Mx, ix, iy, v)) r = add(r, mul(v, P));
-        v = dy_periodic<C>(a.op, a.f[F_NN] + (long)ix * pitch, a.My, iy, -1);
+        v = dy_periodic<true, C>(a.op, a.f[F_NN] + (long)ix * pitch, a.My, iy);
         r = add(r, mul(v, P));
         C s = to_c<C>(a.f[F_NM][i]);
         time_update<CPST>(s, r, c);
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(256) k_elastic_stress(StepArgs<S, C> a)
 {
     const int iy = blockIdx.x * blockDim.x + threadIdx.x;
     const int ix = blockIdx.y * blockDim.y + threadIdx.y;
-    if (iy >= a.My || ix > a.Mx) return;
+    if (iy > a.My || ix > a.Mx) return;
     const int it = *a.step;
     const long pitch = a.pitch;
     const long i = (long)ix * pitch + iy;
@@ -87,19 +87,19 @@ __global__ void __launch_bounds__(256) k_elastic_stress(StepArgs<S, C> a)
     const double *si = a.src_inc + 0;
     const bool src_here = ix == a.src_ix && iy == a.src_iy;
 
-    {   // NN: shear stress; x from MN, y from NM
+    {   // NN (Mx+1 x My+1): shear stress; x from MN, y from NM
         C r, c;
         load_rc<S, C, CPST>(a.res[F_NN], i, r, c);
         const C P = __ldg(a.coef[F_NN] + i);
         C v = dx_from_M<C>(a.op, a.f[F_MN], pitch, a.Mx, ix, iy);
         r = add(r, mul(v, P));
-        v = dy_periodic<C>(a.op, a.f[F_NM] + (long)ix * pitch, a.My, iy, -2);
+        v = dy_periodic<false, C>(a.op, a.f[F_NM] + (long)ix * pitch, a.My, iy);
         r = add(r, mul(v, P));
         C s = to_c<C>(a.f[F_NN][i]);
         time_update<CPST>(s, r, c);
         finish_point(a.f[F_NN], a.res[F_NN], i, s, r, c, kr, kc, a.src_grid == G_NN && src_here, si, it, a.flags);
     }
-    if (ix < a.Mx) {   // MM: normal stresses; x from NM, y from MN
+    if (ix < a.Mx && iy < a.My) {   // MM (Mx x My): normal stresses; x from NM, y from MN
         C r0, c0, r1, c1;
         load_rc<S, C, CPST>(a.res[F_MM0], i, r0, c0);
         load_rc<S, C, CPST>(a.res[F_MM1], i, r1, c1);
@@ -109,7 +109,7 @@ __global__ void __launch_bounds__(256) k_elastic_stress(StepArgs<S, C> a)
         r0 = add(r0, mul(v, L));
         r1 = add(r1, mul(v, L));
         r0 = add(r0, mul(v, M2));
-        v = dy_periodic<C>(a.op, a.f[F_MN] + (long)ix * pitch, a.My, iy, -1);
+        v = dy_periodic<true, C>(a.op, a.f[F_MN] + (long)ix * pitch, a.My, iy);
         r0 = add(r0, mul(v, L));
         r1 = add(r1, mul(v, L));
         r1 = add(r1, mul(v, M2));
@@ -131,32 +131,31 @@ __global__ void __launch_bounds__(256) k_acoustic_velocity(StepArgs<S, C> a)
 {
     const int iy = blockIdx.x * blockDim.x + threadIdx.x;
     const int ix = blockIdx.y * blockDim.y + threadIdx.y;
-    const int rows_N = PERIODIC ? a.Mx : a.Mx + 1;
-    if (iy >= a.My || ix >= rows_N) return;
+    if (iy > a.My || ix > a.Mx) return;
     const int it = *a.step;
     const long pitch = a.pitch;
     const long i = (long)ix * pitch + iy;
     constexpr bool kr = Cpst<CPST>::keep_r, kc = Cpst<CPST>::keep_c;
     const S *p = a.f[F_MM0];
 
-    if (ix < a.Mx) {   // MN: velocity along y, y derivative of p only
+    if (ix < a.Mx) {   // MN (Mx x My+1): velocity along y, y derivative of p only
         C r, c;
         load_rc<S, C, CPST>(a.res[F_MN], i, r, c);
         const C P = __ldg(a.coef[F_MN] + i);
-        const C v = dy_periodic<C>(a.op, p + (long)ix * pitch, a.My, iy, -2);
+        const C v = dy_periodic<false, C>(a.op, p + (long)ix * pitch, a.My, iy);
         r = add(r, mul(v, P));
         C s = to_c<C>(a.f[F_MN][i]);
         time_update<CPST>(s, r, c);
         finish_point(a.f[F_MN], a.res[F_MN], i, s, r, c, kr, kc,
                      a.src_grid == G_MN && ix == a.src_ix && iy == a.src_iy, a.src_inc, it, a.flags);
     }
-    {   // NM: velocity along x, x derivative of p (+ SAT on the free-surface rows)
+    if (iy < a.My) {   // NM (Mx+1 x My): velocity along x, x derivative of p (+ SAT on the free surfaces)
         C r, c;
         load_rc<S, C, CPST>(a.res[F_NM], i, r, c);
         const C P = __ldg(a.coef[F_NM] + i);
         C v;
         if constexpr (PERIODIC) {
-            v = dx_periodic<C>(a.op, p, pitch, a.Mx, ix, iy, -2);
+            v = dx_periodic<false, C>(a.op, p, pitch, a.Mx, ix, iy);
             r = add(r, mul(v, P));
         } else {
             v = dx_from_M<C>(a.op, p, pitch, a.Mx, ix, iy);
@@ -183,10 +182,10 @@ __global__ void __launch_bounds__(256) k_acoustic_pressure(StepArgs<S, C> a)
     C r, c;
     load_rc<S, C, CPST>(a.res[F_MM0], i, r, c);
     const C K = __ldg(a.coef[F_MM0] + i);
-    C v = PERIODIC ? dx_periodic<C>(a.op, a.f[F_NM], pitch, a.Mx, ix, iy, -1)
+    C v = PERIODIC ? dx_periodic<true, C>(a.op, a.f[F_NM], pitch, a.Mx, ix, iy)
                    : dx_from_N<C>(a.op, a.f[F_NM], pitch, a.Mx, ix, iy);
     r = add(r, mul(v, K));
-    v = dy_periodic<C>(a.op, a.f[F_MN] + (long)ix * pitch, a.My, iy, -1);
+    v = dy_periodic<true, C>(a.op, a.f[F_MN] + (long)ix * pitch, a.My, iy);
     r = add(r, mul(v, K));
     C s = to_c<C>(a.f[F_MM0][i]);
     time_update<CPST>(s, r, c);
@@ -202,15 +201,16 @@ template <class S, class C, int CPST>
 void launch_cpst(int physics, int periodic, int half, const StepArgs<S, C> &a, cudaStream_t st)
 {
     const dim3 b(32, 8);
+    const dim3 gN = grid_for(a.Mx + 1, a.My + 1, b), gM = grid_for(a.Mx, a.My, b);
     if (physics == 0) {
-        if (half == 0) k_elastic_velocity<S, C, CPST><<<grid_for(a.Mx + 1, a.My, b), b, 0, st>>>(a);
-        else k_elastic_stress<S, C, CPST><<<grid_for(a.Mx + 1, a.My, b), b, 0, st>>>(a);
+        if (half == 0) k_elastic_velocity<S, C, CPST><<<gN, b, 0, st>>>(a);
+        else k_elastic_stress<S, C, CPST><<<gN, b, 0, st>>>(a);
     } else if (periodic) {
-        if (half == 0) k_acoustic_velocity<S, C, CPST, true><<<grid_for(a.Mx, a.My, b), b, 0, st>>>(a);
-        else k_acoustic_pressure<S, C, CPST, true><<<grid_for(a.Mx, a.My, b), b, 0, st>>>(a);
+        if (half == 0) k_acoustic_velocity<S, C, CPST, true><<<gN, b, 0, st>>>(a);
+        else k_acoustic_pressure<S, C, CPST, true><<<gM, b, 0, st>>>(a);
     } else {
-        if (half == 0) k_acoustic_velocity<S, C, CPST, false><<<grid_for(a.Mx + 1, a.My, b), b, 0, st>>>(a);
-        else k_acoustic_pressure<S, C, CPST, false><<<grid_for(a.Mx, a.My, b), b, 0, st>>>(a);
+        if (half == 0) k_acoustic_velocity<S, C, CPST, false><<<gN, b, 0, st>>>(a);
+        else k_acoustic_pressure<S, C, CPST, false><<<gM, b, 0, st>>>(a);
     }
 }
 }  // namespace

@@ -1,10 +1,12 @@
 // Kernel arguments and per-point operators of the staggered SBP-SAT stepper.
 //
-// Device layout (all grids): row-major, `pitch` elements per row, x = row. Data-y is periodic
-// with period My for every grid, so the N-type-y grids (NN, MN) keep only columns 0..My-1:
-// the reference's extra column My duplicates column 0 bit for bit (it is computed by the same
-// arithmetic from wrapped reads, grid_drvt.tpp:259-284) and is rebuilt on readback. Rows: N-type
-// x grids have Mx+1 rows with free-surface (SAT) ends, Mx rows when x is periodic.
+// Device layout: every grid keeps the reference's sizes (grid.hpp:168-169), row-major with
+// `pitch` elements per row (x = row): N-type directions have M+1 points, M-type ones M. Along a
+// periodic direction the last N point is the reference's "duplicate" of point 0: it has its own
+// material and is updated like any other point, its y derivative reads the M neighbour with the
+// wrap modulo M, and the M-type grids read it directly at their last point; only beyond it do
+// their reads wrap (grid_drvt.tpp:45-167 with N_modulo = M; singlecore copy_to_halo,
+// namespaces.hpp:566-590). With a medium that repeats at the seam the two columns stay equal.
 #pragma once
 #include "device_math.cuh"
 #include "sbp.hpp"
@@ -30,7 +32,11 @@ struct StepArgs {
     int *flags;               // sticky error flags
 };
 
+// read index of an M-type periodic neighbour (n points): wrap modulo n
 __device__ __forceinline__ int wrap(int j, int n) { return j < 0 ? j + n : (j >= n ? j - n : j); }
+// read index of an N-type periodic neighbour (n + 1 points, the last one the seam duplicate):
+// read directly up to n, wrap beyond
+__device__ __forceinline__ int nread(int j, int n) { return j < 0 ? j + n : (j > n ? j - n : j); }
 
 template <class C, class S>
 __device__ __forceinline__ C ld(const S *p, long i) { return to_c<C>(__ldg(p + i)); }
@@ -80,25 +86,31 @@ __device__ __forceinline__ C dx_from_M(const Ops<C> &o, const S *nb, long pitch,
     return v;
 }
 
-// periodic x derivative (single-core acoustic tree): first index offset lo = -2 for N-type
-// rows reading M-type rows, -1 for M-type rows reading N-type rows
-template <class C, class S>
-__device__ __forceinline__ C dx_periodic(const Ops<C> &o, const S *nb, long pitch, int Mx, int ix, int iy, int lo)
+// periodic x derivative (single-core acoustic tree): an N-type row reads M-type rows ix-2..ix+1
+// (wrapped), an M-type row reads N-type rows ix-1..ix+2 (seam row read directly)
+template <bool FROM_N, class C, class S>
+__device__ __forceinline__ C dx_periodic(const Ops<C> &o, const S *nb, long pitch, int Mx, int ix, int iy)
 {
     C v = C(0);
 #pragma unroll
-    for (int w = 0; w < 4; w++) v = add(v, mul(ld<C>(nb, (long)wrap(ix + lo + w, Mx) * pitch + iy), o.st[w]));
+    for (int w = 0; w < 4; w++) {
+        const int r = FROM_N ? nread(ix - 1 + w, Mx) : wrap(ix - 2 + w, Mx);
+        v = add(v, mul(ld<C>(nb, (long)r * pitch + iy), o.st[w]));
+    }
     return v;
 }
 
-// periodic y derivative: lo = -2 on N-type-y grids (reading M-type columns), -1 on M-type-y
-// grids (grid.hpp:361-362, grid_drvt.tpp:45-167 with N_modulo = My)
-template <class C, class S>
-__device__ __forceinline__ C dy_periodic(const Ops<C> &o, const S *row, int My, int iy, int lo)
+// periodic y derivative (grid.hpp:361-362, grid_drvt.tpp:45-167): an N-type-y point reads
+// M-type columns iy-2..iy+1 (wrapped), an M-type-y point reads N-type columns iy-1..iy+2
+template <bool FROM_N, class C, class S>
+__device__ __forceinline__ C dy_periodic(const Ops<C> &o, const S *row, int My, int iy)
 {
     C v = C(0);
 #pragma unroll
-    for (int w = 0; w < 4; w++) v = add(v, mul(ld<C>(row, (long)wrap(iy + lo + w, My)), o.st[w]));
+    for (int w = 0; w < 4; w++) {
+        const int c = FROM_N ? nread(iy - 1 + w, My) : wrap(iy - 2 + w, My);
+        v = add(v, mul(ld<C>(row, (long)c), o.st[w]));
+    }
     return v;
 }
 
