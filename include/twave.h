@@ -42,7 +42,8 @@ enum {
     TW_ERR_RECORD_FULL = -8,    /* more steps than the trace/energy records hold */
     TW_ERR_NONFINITE = -9,      /* a NaN/Inf appeared in a field (sticky, reported by tw_sync) */
     TW_ERR_UNSUPPORTED = -10,   /* combination not implemented (e.g. elastic with periodic x) */
-    TW_ERR_MODEL_BOUNDS = -11   /* interpolation stepped out of the model (grid_parameter.cpp:54-56) */
+    TW_ERR_MODEL_BOUNDS = -11,  /* interpolation stepped out of the model (grid_parameter.cpp:54-56) */
+    TW_ERR_TOO_LARGE = -12      /* model larger than the no-allocation scratch (TW_NOALLOC_MAX_MODEL_POINTS) */
 };
 
 /* ---- enums ------------------------------------------------------------------------------ */
@@ -158,6 +159,27 @@ TW_API int tw_profile(tw_solver *s, int n, double *ms);
 TW_API int tw_location_to_index(char type, long num, long den, int num_dx, int den_dx, long *index);
 /* The handle's cudaStream_t, for callers that order their own work after tw_step. */
 TW_API int tw_get_stream(tw_solver *s, void **stream);
+/* No counterpart in the reference: the material interpolation of tw_set_material_model without
+ * any device allocation, for callers that cannot allocate device memory - a process whose GPU
+ * memory is already reserved by another allocator (for example PyTorch's caching allocator) or
+ * that fixes its memory budget at start-up, and that re-maps the medium repeatedly, as an
+ * inversion loop does every iteration. tw_set_material_model allocates a temporary buffer per
+ * call; this entry point uses a static device scratch of TW_NOALLOC_MAX_MODEL_POINTS doubles for
+ * each of lambda, 2mu and mu on the padded model (12 MiB held by every GPU that loads the
+ * library, until the process exits) and returns TW_ERR_TOO_LARGE for a larger padded model
+ * (Mx_prmt+2)*(My_prmt+2). All pointers are caller-owned device memory: d_rho/d_vp/d_vs the padded
+ * model (row stride My_prmt+2, d_vs zeros for acoustic media); outputs at the reference grid sizes,
+ * compact: NN mu (Mx+1)x(My+1), MN rho Mx x(My+1), NM rho (Mx+1)x My, MM lambda and 2mu Mx x My -
+ * the values tw_set_material_grid accepts. Runs on `stream` (a cudaStream_t, 0 for the legacy
+ * default stream) and waits for it before returning. The first call on a device looks up the
+ * scratch's device address (cudaGetSymbolAddress) with that device current; make that first call
+ * before any stream capture. Every call shares the scratch, so calls that overlap on the GPU race. */
+#define TW_NOALLOC_MAX_MODEL_POINTS (1L << 19)
+TW_API int tw_material_map_noalloc(const double *d_rho, const double *d_vp, const double *d_vs, long Mx_prmt,
+                                   long My_prmt, int num_dxM, int den_dxM, long Mx, long My, int num_dx,
+                                   int den_dx, double *d_NN_mu, double *d_MN_rho, double *d_NM_rho,
+                                   double *d_MM_lambda, double *d_MM_2mu, void *stream);
+
 TW_API const char *tw_strerror(int status);
 TW_API const char *tw_last_cuda_error(void);
 

@@ -30,7 +30,7 @@ PRECISION = {"f64": FP64, "f32": FP32, "bf16": BF16, "fp16": FP16}
 
 ERRORS = {0: "TW_OK", -1: "TW_ERR_INVALID", -2: "TW_ERR_CUDA", -3: "TW_ERR_NOMEM", -4: "TW_ERR_STATE",
           -5: "TW_ERR_LOCATION", -6: "TW_ERR_OUTSIDE", -7: "TW_ERR_WEAK_BOUNDARY", -8: "TW_ERR_RECORD_FULL",
-          -9: "TW_ERR_NONFINITE", -10: "TW_ERR_UNSUPPORTED", -11: "TW_ERR_MODEL_BOUNDS"}
+          -9: "TW_ERR_NONFINITE", -10: "TW_ERR_UNSUPPORTED", -11: "TW_ERR_MODEL_BOUNDS", -12: "TW_ERR_TOO_LARGE"}
 
 
 class TwError(RuntimeError):
@@ -87,6 +87,8 @@ def lib() -> C.CDLL:
         L.tw_get_info.argtypes = [vp, C.POINTER(Info)]
         L.tw_get_stream.argtypes = [vp, C.POINTER(vp)]
         L.tw_profile.argtypes = [vp, C.c_int, dp]
+        L.tw_material_map_noalloc.argtypes = [vp, vp, vp, C.c_long, C.c_long, C.c_int, C.c_int, C.c_long, C.c_long,
+                                              C.c_int, C.c_int, vp, vp, vp, vp, vp, vp]
         L.tw_location_to_index.argtypes = [C.c_char, C.c_long, C.c_long, C.c_int, C.c_int, lp]
         L.tw_strerror.restype = C.c_char_p
         L.tw_strerror.argtypes = [C.c_int]

@@ -385,6 +385,7 @@ const char *tw_strerror(int status)
     case TW_ERR_NONFINITE: return "non-finite value in a field";
     case TW_ERR_UNSUPPORTED: return "unsupported configuration";
     case TW_ERR_MODEL_BOUNDS: return "material interpolation outside the model";
+    case TW_ERR_TOO_LARGE: return "model larger than the no-allocation scratch (TW_NOALLOC_MAX_MODEL_POINTS)";
     }
     return "unknown status";
 }
