@@ -182,3 +182,27 @@ def test_nonfinite_value_is_reported_not_faulted(tw):
         assert np.isfinite(s.read_field(tw.MM)).all()
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("cpst", ["00", "6R", "3C"])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_many_strips_and_segments_match_oracle(cpst, prec):
+    """A grid wide and tall enough for several column strips and row segments of the one-launch
+    step; receivers sit on strip and segment edges and on the periodic seam."""
+    Mx, My = 70, 500
+    den = 500
+    rcvs = [("N", "M", 15, den, 2 * 247 + 1, 2 * den), ("N", "M", 16, den, 2 * 248 + 1, 2 * den),
+            ("M", "M", 2 * 47 + 1, 2 * den, 2 * 495 + 1, 2 * den), ("N", "N", 48, den, My, den),
+            ("M", "N", 2 * 69 + 1, 2 * den, 0, 1), ("N", "N", Mx, den, 248, den), ("N", "M", Mx, den, 2 * 499 + 1, 2 * den)]
+    case = elastic_case(Mx, My, seed=77, cpst=cpst, Nt=6, den_dx=den, rcvs=rcvs,
+                        src=("N", "M", 16, den, 2 * 248 + 1, 2 * den))
+    T = np.float64 if prec == "f64" else np.float32
+    f0 = [a.astype(T).astype(np.float64) for a in _random_state(Mx, My, 5)]
+    r0 = None if cpst == "00" else [a.astype(T).astype(np.float64) for a in _random_state(Mx, My, 6, scale=1e-8)]
+    want = orc.elastic_run(case, prec, fields0=f0, resid0=r0)
+    got = product_elastic(case, prec, fields0=f0, resid0=r0)
+    for k, v in got["fields"].items():
+        assert np.array_equal(v, want.fields[k]), k
+    assert np.array_equal(got["traces"], want.traces)
+    for k in ("E_k", "E_p0", "E_p1"):
+        assert energy_close(got[k], getattr(want, k)), k

@@ -53,6 +53,39 @@ struct EnergyArgs {
 template <class S, class C>
 void launch_energy(const EnergyArgs<S, C> &e, cudaStream_t st);
 
+// fused elastic step (fused_step.cu): one CTA per strip of FS_TY columns x segment of rows
+constexpr int FS_THREADS = 256;
+constexpr int FS_HALO = 4;
+constexpr int FS_TY = FS_THREADS - 2 * FS_HALO;
+
+template <class S, class C>
+struct FusedArgs {
+    const S *in[5];           // state before the step
+    S *out[5];                // state after the step
+    const S *rin[5];          // compensation arrays before / after
+    S *rout[5];
+    const C *coef[5];
+    long pitch;
+    int Mx, My;
+    Ops<C> op;
+    int seg_rows, n_seg, n_strip;
+    const double *src_inc;
+    int src_grid, src_ix, src_iy;
+    int *step;                // read by every CTA; the last CTA to finish advances it
+    int *done;                // CTA completion counter (zero between steps)
+    int *flags;
+    int max_steps;
+    const double *w[5];       // energy weights (ENERGY only)
+    double *energy;           // [3][max_steps]: E_p0, E_k, E_p1
+    const int *rcv_off;       // receivers owned by each CTA (CSR over blockIdx.y * n_strip + blockIdx.x)
+    const int *rcv;           // [n][4]: field slot, row, column, trace row (2 * receiver + field)
+    double *traces;
+};
+template <class S, class C>
+void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, cudaStream_t st);
+template <class S, class C>
+cudaError_t prepare_fused();
+
 template <class S>
 struct GatherArgs {
     const S *f[5];

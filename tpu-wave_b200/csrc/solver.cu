@@ -11,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <algorithm>
 #include <new>
 #include <string>
 #include <vector>
@@ -66,6 +67,13 @@ struct tw_solver {
     long ref_rows[4], ref_cols[4];    // reference sizes per grid
     cudaStream_t st = nullptr;
     void *f[5] = {}, *res[5] = {}, *coef[5] = {};
+    // fused elastic path: double-buffered state, strip x segment geometry, per-CTA receivers
+    bool fused = false;
+    void *f2[5] = {}, *res2[5] = {};
+    int parity = 0;                   // which buffer holds the current state (0: f/res, 1: f2/res2)
+    int seg_rows = 0, n_seg = 1, n_strip = 1;
+    int *d_done = nullptr, *d_rcv_off = nullptr, *d_rcv_list = nullptr;
+    int rcv_list_cap = 0;
     double *w[5] = {}, *mat[5] = {};
     bool mat_set[5] = {};
     bool mat_dirty = true, mat_ready = false;
@@ -105,6 +113,8 @@ tw_solver::~tw_solver()
     for (int k = 0; k < 5; k++) {
         cudaFree(f[k]); cudaFree(res[k]); cudaFree(coef[k]); cudaFree(w[k]); cudaFree(mat[k]);
     }
+    for (int k = 0; k < 5; k++) { cudaFree(f2[k]); cudaFree(res2[k]); }
+    cudaFree(d_done); cudaFree(d_rcv_off); cudaFree(d_rcv_list);
     cudaFree(src_inc); cudaFree(d_step); cudaFree(d_flags); cudaFree(d_rcv); cudaFree(d_err);
     cudaFree(d_traces); cudaFree(d_energy);
     if (st) cudaStreamDestroy(st);
@@ -205,6 +215,47 @@ void enqueue_steps(tw_solver *s, int n, cudaStream_t st)
     }
 }
 
+void *cur_f(const tw_solver *s, int k) { return s->parity ? s->f2[k] : s->f[k]; }
+void *cur_res(const tw_solver *s, int k) { return s->parity ? s->res2[k] : s->res[k]; }
+
+// one fused elastic step from the current buffers into the other ones
+template <class S, class C>
+void enqueue_fused_step(tw_solver *s, cudaStream_t st)
+{
+    FusedArgs<S, C> a{};
+    void **fin = s->parity ? s->f2 : s->f, **fout = s->parity ? s->f : s->f2;
+    void **rin = s->parity ? s->res2 : s->res, **rout = s->parity ? s->res : s->res2;
+    for (int k = 0; k < 5; k++) {
+        a.in[k] = (const S *)fin[k];
+        a.out[k] = (S *)fout[k];
+        a.rin[k] = (const S *)rin[k];
+        a.rout[k] = (S *)rout[k];
+        a.coef[k] = (const C *)s->coef[k];
+        a.w[k] = s->w[k];
+    }
+    a.pitch = s->pitch;
+    a.Mx = (int)s->d.Mx;
+    a.My = (int)s->d.My;
+    a.op = make_ops<C>((double)s->d.num_dx / (double)s->d.den_dx, s->d.dt, false);
+    a.seg_rows = s->seg_rows;
+    a.n_seg = s->n_seg;
+    a.n_strip = s->n_strip;
+    a.src_inc = s->src_inc;
+    a.src_grid = s->src_grid;
+    a.src_ix = (int)s->src_ix;
+    a.src_iy = (int)s->src_iy;
+    a.step = s->d_step;
+    a.done = s->d_done;
+    a.flags = s->d_flags;
+    a.max_steps = s->d.max_steps;
+    a.energy = s->d_energy;
+    a.rcv_off = s->d_rcv_off;
+    a.rcv = s->d_rcv_list;
+    a.traces = s->d_traces;
+    launch_fused<S, C>(a, s->d.cpst, s->d.energy != 0, st);
+    s->parity ^= 1;
+}
+
 // launch phase `ph` (0 velocity, 1 stress, 2 energy of the step, 3 gather) of one step
 template <class S, class C>
 void enqueue_phase(tw_solver *s, int ph, cudaStream_t st)
@@ -232,6 +283,13 @@ void enqueue_phase(tw_solver *s, int ph, cudaStream_t st)
 
 void enqueue(tw_solver *s, int n, cudaStream_t st)
 {
+    if (s->fused) {
+        for (int k = 0; k < n; k++) {
+            if (s->d.precision == TW_FP64) enqueue_fused_step<double, double>(s, st);
+            else enqueue_fused_step<float, float>(s, st);
+        }
+        return;
+    }
     if (s->d.precision == TW_FP64) enqueue_steps<double, double>(s, n, st);
     else enqueue_steps<float, float>(s, n, st);
 }
@@ -312,6 +370,34 @@ int upload_receivers(tw_solver *s)
     }
     if (n > 0)
         TW_CUDA(cudaMemcpyAsync(s->d_rcv, s->rcv_tab.data(), sizeof(int) * s->rcv_tab.size(), cudaMemcpyHostToDevice, s->st));
+    if (s->fused) {
+        // per-CTA receiver lists: a receiver belongs to the CTA whose segment owns its row and
+        // whose strip owns its column (fused_step.cu)
+        const int nctas = s->n_seg * s->n_strip;
+        std::vector<std::vector<int>> per(nctas);
+        for (int r = 0; r < n; r++) {
+            const int *q = &s->rcv_tab[4 * r];
+            const int seg = std::min(q[2] / s->seg_rows, s->n_seg - 1), strip = q[3] / FS_TY;
+            for (int f = 0; f < 2; f++)
+                if (q[f] >= 0) per[seg * s->n_strip + strip].insert(per[seg * s->n_strip + strip].end(), {q[f], q[2], q[3], 2 * r + f});
+        }
+        std::vector<int> off(nctas + 1, 0), list;
+        for (int c = 0; c < nctas; c++) {
+            off[c + 1] = off[c] + (int)per[c].size() / 4;
+            list.insert(list.end(), per[c].begin(), per[c].end());
+        }
+        if ((int)list.size() > s->rcv_list_cap) {
+            cudaFree(s->d_rcv_list);
+            s->d_rcv_list = nullptr;
+            int cap = 64;
+            while (cap < (int)list.size()) cap *= 2;
+            if (s->alloc((void **)&s->d_rcv_list, sizeof(int) * cap) != TW_OK) return TW_ERR_NOMEM;
+            s->rcv_list_cap = cap;
+        }
+        TW_CUDA(cudaMemcpyAsync(s->d_rcv_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, s->st));
+        if (!list.empty())
+            TW_CUDA(cudaMemcpyAsync(s->d_rcv_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, s->st));
+    }
     TW_CUDA(cudaStreamSynchronize(s->st));
     s->drop_graph();
     return TW_OK;
@@ -448,6 +534,31 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
         if (cp) cudaMemsetAsync(s->res[k], 0, n * s->esz, s->st);
         cudaMemsetAsync(s->coef[k], 0, n * csz, s->st);
         cudaMemsetAsync(s->w[k], 0, n * sizeof(double), s->st);
+    }
+    if (s->elastic) {
+        // fused elastic path: a second copy of the state and the strip x segment geometry
+        s->fused = true;
+        e = d.precision == TW_FP64 ? prepare_fused<double, double>() : prepare_fused<float, float>();
+        if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
+        for (int k = 0; k < 5; k++) {
+            const size_t n = (size_t)s->rows[k] * s->pitch;
+            if ((rc_ = s->alloc(&s->f2[k], n * s->esz)) != TW_OK) return fail(rc_);
+            cudaMemsetAsync(s->f2[k], 0, n * s->esz, s->st);
+            if (cp) {
+                if ((rc_ = s->alloc(&s->res2[k], n * s->esz)) != TW_OK) return fail(rc_);
+                cudaMemsetAsync(s->res2[k], 0, n * s->esz, s->st);
+            }
+        }
+        s->n_strip = (int)((My + 1 + FS_TY - 1) / FS_TY);
+        // about three CTAs per SM of a 148-SM B200; segments of at least 16 rows, the last one
+        // taking the remainder
+        const int target = std::max(1, 444 / s->n_strip);
+        s->seg_rows = std::max(16, (int)((Mx + target - 1) / target));
+        s->n_seg = std::max(1, (int)(Mx / s->seg_rows));
+        if ((rc_ = s->alloc((void **)&s->d_done, sizeof(int))) != TW_OK) return fail(rc_);
+        cudaMemsetAsync(s->d_done, 0, sizeof(int), s->st);
+        if ((rc_ = s->alloc((void **)&s->d_rcv_off, sizeof(int) * (s->n_seg * s->n_strip + 1))) != TW_OK) return fail(rc_);
+        cudaMemsetAsync(s->d_rcv_off, 0, sizeof(int) * (s->n_seg * s->n_strip + 1), s->st);
     }
     if ((rc_ = s->alloc((void **)&s->src_inc, sizeof(double) * d.max_steps)) != TW_OK) return fail(rc_);
     if ((rc_ = s->alloc((void **)&s->d_energy, sizeof(double) * 3 * d.max_steps)) != TW_OK) return fail(rc_);
@@ -613,7 +724,11 @@ int tw_reset(tw_solver *s)
         const size_t n = (size_t)s->rows[k] * s->pitch * s->esz;
         TW_CUDA(cudaMemsetAsync(s->f[k], 0, n, s->st));
         if (s->res[k]) TW_CUDA(cudaMemsetAsync(s->res[k], 0, n, s->st));
+        if (s->f2[k]) TW_CUDA(cudaMemsetAsync(s->f2[k], 0, n, s->st));
+        if (s->res2[k]) TW_CUDA(cudaMemsetAsync(s->res2[k], 0, n, s->st));
     }
+    if (s->d_done) TW_CUDA(cudaMemsetAsync(s->d_done, 0, sizeof(int), s->st));
+    s->parity = 0;
     TW_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * 3 * s->d.max_steps, s->st));
     if (s->d_traces) TW_CUDA(cudaMemsetAsync(s->d_traces, 0, sizeof(double) * 2 * (size_t)s->rcv_cap * s->d.max_steps, s->st));
     TW_CUDA(cudaMemsetAsync(s->d_step, 0, sizeof(int), s->st));
@@ -634,12 +749,18 @@ int tw_step(tw_solver *s, int n)
     // a graph of G steps captured once and replayed; leftover steps are launched directly
     const int G = 16;
     int left = n;
-    if (n >= G) {
+    if (s->fused && s->parity && left > 0 && n >= G) {
+        enqueue(s, 1, s->st);   // captured graphs start from the first buffer
+        left--;
+    }
+    if (left >= G) {
         if (!s->gexec || s->graph_steps != G) {
             s->drop_graph();
             cudaGraph_t graph;
             TW_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+            const int parity0 = s->parity;
             enqueue(s, G, s->st);
+            s->parity = parity0;   // capture only records; replays advance the parity below
             TW_CUDA(cudaStreamEndCapture(s->st, &graph));
             cudaError_t e = cudaGraphInstantiate(&s->gexec, graph, 0);
             cudaGraphDestroy(graph);
@@ -648,7 +769,7 @@ int tw_step(tw_solver *s, int n)
         }
         while (left >= G) {
             TW_CUDA(cudaGraphLaunch(s->gexec, s->st));
-            left -= G;
+            left -= G;   // G is even: the parity is unchanged
         }
     }
     if (left > 0) enqueue(s, left, s->st);
@@ -675,7 +796,7 @@ int tw_read_field(tw_solver *s, int grid, int field, double *host, long ld)
     const int slot = slot_of(s, grid, field);
     if (slot < 0 || ld < s->ref_cols[grid]) return TW_ERR_INVALID;
     TW_CUDA(cudaSetDevice(s->d.device));
-    return read_device_array(s, s->f[slot], s->d.precision, s->esz, slot, host, ld);
+    return read_device_array(s, cur_f(s, slot), s->d.precision, s->esz, slot, host, ld);
 }
 
 int tw_write_field(tw_solver *s, int grid, int field, const double *host, long ld)
@@ -684,7 +805,7 @@ int tw_write_field(tw_solver *s, int grid, int field, const double *host, long l
     const int slot = slot_of(s, grid, field);
     if (slot < 0 || ld < s->ref_cols[grid]) return TW_ERR_INVALID;
     TW_CUDA(cudaSetDevice(s->d.device));
-    return write_device_array(s, s->f[slot], s->d.precision, s->esz, slot, host, ld);
+    return write_device_array(s, cur_f(s, slot), s->d.precision, s->esz, slot, host, ld);
 }
 
 int tw_read_resid(tw_solver *s, int grid, int field, double *host, long ld)
@@ -693,7 +814,7 @@ int tw_read_resid(tw_solver *s, int grid, int field, double *host, long ld)
     const int slot = slot_of(s, grid, field);
     if (slot < 0 || ld < s->ref_cols[grid] || !s->res[slot]) return TW_ERR_INVALID;
     TW_CUDA(cudaSetDevice(s->d.device));
-    return read_device_array(s, s->res[slot], s->d.precision, s->esz, slot, host, ld);
+    return read_device_array(s, cur_res(s, slot), s->d.precision, s->esz, slot, host, ld);
 }
 
 int tw_write_resid(tw_solver *s, int grid, int field, const double *host, long ld)
@@ -702,7 +823,7 @@ int tw_write_resid(tw_solver *s, int grid, int field, const double *host, long l
     const int slot = slot_of(s, grid, field);
     if (slot < 0 || ld < s->ref_cols[grid] || !s->res[slot]) return TW_ERR_INVALID;
     TW_CUDA(cudaSetDevice(s->d.device));
-    return write_device_array(s, s->res[slot], s->d.precision, s->esz, slot, host, ld);
+    return write_device_array(s, cur_res(s, slot), s->d.precision, s->esz, slot, host, ld);
 }
 
 int tw_read_receivers(tw_solver *s, double *host)
@@ -762,7 +883,9 @@ int tw_profile(tw_solver *s, int n, double *ms)
     for (int k = 0; k < n; k++)
         for (int ph = 0; ph < 4; ph++) {
             cudaEventRecord(ev[(size_t)8 * k + 2 * ph], s->st);
-            if (ph != 2 || s->d.energy) {
+            if (s->fused) {
+                if (ph == 0) enqueue(s, 1, s->st);   // the whole step is one launch
+            } else if (ph != 2 || s->d.energy) {
                 if (f64) enqueue_phase<double, double>(s, ph, s->st);
                 else enqueue_phase<float, float>(s, ph, s->st);
             }
