@@ -1,25 +1,25 @@
 // Fused elastic time step: one launch per step, every field read once and written once.
 //
-// The two half-steps of forward_simulation.cpp:38-113 (velocities from stresses, then stresses
-// from the new velocities) are done by one kernel that sweeps rows. A CTA owns a strip of
-// FS_TY columns and a segment of rows. Each thread owns one column ("logical" column c =
-// y0 - FS_HALO + t) and walks down the rows:
-//   iteration k: stage old stress row k-1 (loaded at iteration k-1) into a shared ring;
-//                issue the global loads of iteration k+1;
-//                compute the velocities of row j = k - LAG_V;
-//                compute the stresses of row i = k - LAG_S;
-//                one __syncthreads.
-// x derivatives read the thread's own column from the rings; y derivatives read neighbouring
-// columns of a row staged at least one iteration earlier. The lags keep every SBP closure row
-// (rows 0..4 and the last five) in the rings when it is needed: a velocity row j reads old
-// stress rows up to j+2 (interior) or 4 (left closure); a stress row i reads new velocity rows
-// up to i+2 or 4. The FS_HALO columns on each side give the y derivatives of the stresses the
-// new velocities of the neighbouring strips, computed again here; rows outside the segment are
-// computed again in the same way. The state is double buffered (in -> out) because neighbouring
-// CTAs read old values that this CTA overwrites.
+// A step (forward_simulation.cpp:38-113) updates the velocities from the stresses, then the
+// stresses from the new velocities. This kernel does both in one pass over the grid, reading
+// the state from one buffer and writing it to the other (neighbouring CTAs read old values that
+// this CTA overwrites). Two kinds of CTA share the launch:
+//
+// * interior CTAs (rows [FS_ZONE, Mx - FS_ZONE)): eight independent warps, each streaming down
+//   a strip of FS_WARP_CORE columns with two columns per lane. The x stencil windows live in
+//   registers, the y taps come from the neighbouring lanes by warp shuffles, two lanes on each
+//   side are halo (their velocities feed the stress y taps of the core lanes). A warp computes
+//   velocity row j and then stress row j - 2, so no shared memory and no block barrier is used.
+//   These rows never touch an SBP closure or an SAT penalty.
+// * boundary CTAs (the FS_ZONE rows at each free surface, or the whole grid when it is small):
+//   a strip of FS_BND_TY columns, its threads split into row groups; phase 1 computes the
+//   velocities of the zone (and two rows beyond) from global memory with the closure and SAT
+//   operators into a shared tile, phase 2 the stresses from that tile.
 //
 // Per point the arithmetic and the order of the right-hand-side terms are those of
-// step_kernels.cu (hence of the reference), so results are bit-identical to the two-kernel path.
+// step_kernels.cu (hence of the reference): results are bit-identical.
+#include <type_traits>
+
 #include "kernels.h"
 #include "stepper.cuh"
 
@@ -27,13 +27,7 @@ namespace tw {
 
 namespace {
 
-constexpr int NT = FS_THREADS;
-constexpr int HALO = FS_HALO;
-constexpr int TY = FS_TY;
-constexpr int RS = 9;     // old stress rows kept
-constexpr int RV = 8;     // new velocity rows kept
-constexpr int LAG_V = 5;
-constexpr int LAG_S = 9;
+constexpr unsigned FULL = 0xffffffffu;
 
 __device__ __forceinline__ int pmod(int c, int n)
 {
@@ -41,327 +35,611 @@ __device__ __forceinline__ int pmod(int c, int n)
     return r < 0 ? r + n : r;
 }
 
-// thread-local energy accumulators (FP64)
+template <class C>
+struct P2 {
+    C a, b;
+};
+
+template <class S> struct Vec2;
+template <> struct Vec2<float> { using T = float2; };
+template <> struct Vec2<double> { using T = double2; };
+
+// a pair of values at physical columns pa, pb of one row (one vector load when they are
+// adjacent and aligned)
+template <class C, class S>
+__device__ __forceinline__ P2<C> ld2_any(const S *row, int pa, int pb)
+{
+    if (pb == pa + 1 && !(pa & 1)) {
+        const typename Vec2<S>::T v = *reinterpret_cast<const typename Vec2<S>::T *>(row + pa);
+        return {to_c<C>(v.x), to_c<C>(v.y)};
+    }
+    return {to_c<C>(row[pa]), to_c<C>(row[pb])};
+}
+
+template <class C>
+__device__ __forceinline__ P2<C> ldg2_any(const C *row, int pa, int pb)
+{
+    if (pb == pa + 1 && !(pa & 1)) {
+        const typename Vec2<C>::T v = __ldg(reinterpret_cast<const typename Vec2<C>::T *>(row + pa));
+        return {v.x, v.y};
+    }
+    return {__ldg(row + pa), __ldg(row + pb)};
+}
+
 struct EAcc {
     double p0 = 0., k = 0., p1 = 0.;
 };
 
+// neighbouring lanes' pairs: p = lane - 1 (columns c0-2, c0-1), n = lane + 1 (c0+2, c0+3)
 template <class C>
-struct Ring {
-    C *p;
-    int rows;
-    __device__ __forceinline__ C &at(int row, int t) const { return p[(row % rows) * NT + t]; }
-};
+__device__ __forceinline__ void lanes(const P2<C> &v, P2<C> &p, P2<C> &n)
+{
+    p.a = __shfl_up_sync(FULL, v.a, 1);
+    p.b = __shfl_up_sync(FULL, v.b, 1);
+    n.a = __shfl_down_sync(FULL, v.a, 1);
+    n.b = __shfl_down_sync(FULL, v.b, 1);
+}
 
-template <class S, class C, int CPST>
-struct Inputs {   // global values consumed by one iteration
-    C nn, mm0, mm1;                 // old stress row (to be staged)
-    C vmn, vnm, pmn, pnm;           // old velocities and 1/rho of the velocity row
-    C rmn, cmn, rnm, cnm;           // compensation values of the velocity row
-    C mu, lam, m2;                  // coefficients of the stress row
-    C rnn, cnn, rm0, cm0, rm1, cm1; // compensation values of the stress row
-    double wmn, wnm, wnn, wm3, wm4; // energy weights
+// y derivative of an N-type-y point from M-type taps c-2..c+1 (a: column c0, b: column c1)
+template <class C>
+__device__ __forceinline__ P2<C> dyNfromM(const Ops<C> &o, const P2<C> &v, const P2<C> &p, const P2<C> &n)
+{
+    const C ta[4] = {p.a, p.b, v.a, v.b}, tb[4] = {p.b, v.a, v.b, n.a};
+    P2<C> r{C(0), C(0)};
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        r.a = add(r.a, mul(ta[w], o.st[w]));
+        r.b = add(r.b, mul(tb[w], o.st[w]));
+    }
+    return r;
+}
+
+// y derivative of an M-type-y point from N-type taps c-1..c+2
+template <class C>
+__device__ __forceinline__ P2<C> dyMfromN(const Ops<C> &o, const P2<C> &v, const P2<C> &p, const P2<C> &n)
+{
+    const C ta[4] = {p.b, v.a, v.b, n.a}, tb[4] = {v.a, v.b, n.a, n.b};
+    P2<C> r{C(0), C(0)};
+#pragma unroll
+    for (int w = 0; w < 4; w++) {
+        r.a = add(r.a, mul(ta[w], o.st[w]));
+        r.b = add(r.b, mul(tb[w], o.st[w]));
+    }
+    return r;
+}
+
+template <class C>
+struct Row {   // global values one interior iteration consumes
+    P2<C> nn, mm0, mm1;           // old stress rows j+2, j+1, j
+    P2<C> vmn, vnm, pmn, pnm;     // old velocities and 1/rho of velocity row j
+    P2<C> rmn, rnm;               // compensation of velocity row j
+    P2<C> mu, lam, m2;            // coefficients of stress row j-2
+    P2<C> rnn, rm0, rm1;          // compensation of stress row j-2
+    P2<double> wmn, wnm, wnn, wm3, wm4;
 };
 
 }  // namespace
 
-template <class S, class C, int CPST, bool ENERGY>
-__global__ void __launch_bounds__(NT) k_elastic_fused(FusedArgs<S, C> a)
+// ------------------------------------------------------------------------------- interior warp
+// EDGE: the strip touches the periodic wrap or the end of a row, so lanes may have non-adjacent
+// physical columns, unowned columns or the seam; otherwise every pair is adjacent, aligned and
+// owned by the core lanes, and loads and stores are single vector accesses
+template <class S, class C, int CPST, bool ENERGY, bool EDGE>
+__device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int it, int rcv_b, int rcv_e, EAcc &E)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *sm = reinterpret_cast<C *>(smem_raw);
-    const Ring<C> rNN{sm + 0 * RS * NT, RS}, rM0{sm + 1 * RS * NT, RS}, rM1{sm + 2 * RS * NT, RS};
-    const Ring<C> rMN{sm + 3 * RS * NT, RV}, rNM{sm + 3 * RS * NT + RV * NT, RV};
     constexpr bool KR = Cpst<CPST>::keep_r, KC = Cpst<CPST>::keep_c;
+    const int lane = threadIdx.x & 31;
+    const int Mx = a.Mx, My = a.My, pitch = (int)a.pitch;
+    const int y0 = wstrip * FS_WARP_CORE;
+    const int c0 = y0 - 4 + 2 * lane, c1 = c0 + 1;
+    const int pM0 = pmod(c0, My), pM1 = pmod(c1, My);
+    const int pN0 = (c0 >= 0 && c0 <= My) ? c0 : pM0, pN1 = (c1 >= 0 && c1 <= My) ? c1 : pM1;
+    const bool core = lane >= 2 && lane < 30;
+    const bool oN0 = core && (!EDGE || c0 <= My), oN1 = core && (!EDGE || c1 <= My);
+    const bool oM0 = core && (!EDGE || c0 < My), oM1 = core && (!EDGE || c1 < My);
+    // balanced segments of the interior rows [FS_ZONE, Mx - FS_ZONE)
+    const int x0 = FS_ZONE + (int)((long)seg * a.int_rows / a.n_int_seg);
+    const int x1 = FS_ZONE + (int)((long)(seg + 1) * a.int_rows / a.n_int_seg);   // rows [x0, x1)
+    // NM columns next to the periodic seam read NN by the physical rule (column My and column 0
+    // of an N-type-y grid are distinct points)
+    const bool seam0 = EDGE && (c0 == -2 || c0 == -1 || c0 == My || c0 == My + 1);
+    const bool seam1 = EDGE && (c1 == -2 || c1 == -1 || c1 == My || c1 == My + 1);
 
-    const int t = threadIdx.x;
-    const int Mx = a.Mx, My = a.My;
-    const long pitch = a.pitch;
-    const int y0 = blockIdx.x * TY;
-    const int c = y0 - HALO + t;                          // logical column
-    const int pM = pmod(c, My);                           // M-type-y physical column
-    const int pN = (c >= 0 && c <= My) ? c : pM;          // N-type-y physical column (seam kept)
-    const bool core = t >= HALO && t < HALO + TY;
-    const bool ownN = core && c <= My, ownM = core && c < My;
-    const bool velT = t >= 2 && t < NT - 2;               // computes velocities (y taps t-2..t+2)
-
-    const int seg = blockIdx.y;
-    const int x0 = seg * a.seg_rows;
-    const int x1e = seg == a.n_seg - 1 ? Mx : x0 + a.seg_rows - 1;   // last owned row (N-type grids)
-    const int lb = max(x0 - 4, 0), le = min(x1e + 4, Mx);            // stress rows loaded
-    const int vb = max(x0 - 2, 0), ve = min(x1e + 2, Mx);            // velocity rows computed
-    const int it = *a.step;
-    const int cta = blockIdx.y * gridDim.x + blockIdx.x;
-    const int rcv_b = a.rcv_off[cta], rcv_e = a.rcv_off[cta + 1];
-
-    auto ldS = [&](int f, int row, int col) -> C { return to_c<C>(a.in[f][(long)row * pitch + col]); };
-    auto ldR = [&](int f, int row, int col) -> C { return to_c<C>(a.rin[f][(long)row * pitch + col]); };
-    auto ldK = [&](int f, int row, int col) -> C { return __ldg(a.coef[f] + (long)row * pitch + col); };
-    auto ldW = [&](int f, int row, int col) -> double { return __ldg(a.w[f] + (long)row * pitch + col); };
-
-    // global loads of iteration kk (stress row kk-1, velocity row kk-LAG_V, stress row kk-LAG_S)
-    auto fetch = [&](int kk, Inputs<S, C, CPST> &in) {
-        const int sr = kk - 1, j = kk - LAG_V, i = kk - LAG_S;
-        if (sr >= lb && sr <= le) {
-            in.nn = ldS(F_NN, sr, pN);
-            if (sr < Mx) { in.mm0 = ldS(F_MM0, sr, pM); in.mm1 = ldS(F_MM1, sr, pM); }
+    auto rowp = [&](const S *base, int r) { return base + r * pitch; };
+    auto ld2 = [&](const S *row, int pa, int pb) -> P2<C> {
+        if (!EDGE) {
+            const typename Vec2<S>::T v = *reinterpret_cast<const typename Vec2<S>::T *>(row + c0);
+            return {to_c<C>(v.x), to_c<C>(v.y)};
         }
-        if (velT && j >= vb && j <= ve) {
-            if (j < Mx) {
-                in.vmn = ldS(F_MN, j, pN);
-                in.pmn = ldK(F_MN, j, pN);
-                if (KR) in.rmn = ldR(F_MN, j, pN);
-                if (KC) in.cmn = ldR(F_MN, j, pN);
+        return ld2_any<C>(row, pa, pb);
+    };
+    auto ldg2 = [&](const auto *row, int pa, int pb) {
+        using T = typename std::remove_cv<typename std::remove_pointer<decltype(row)>::type>::type;
+        if (!EDGE) {
+            const typename Vec2<T>::T v = __ldg(reinterpret_cast<const typename Vec2<T>::T *>(row + c0));
+            return P2<T>{v.x, v.y};
+        }
+        return ldg2_any<T>(row, pa, pb);
+    };
+    auto fetch = [&](int j, Row<C> &in) {
+        in.nn = ld2(rowp(a.in[F_NN], j + 2), pN0, pN1);
+        in.mm0 = ld2(rowp(a.in[F_MM0], j + 1), pM0, pM1);
+        in.mm1 = ld2(rowp(a.in[F_MM1], j), pM0, pM1);
+        in.vmn = ld2(rowp(a.in[F_MN], j), pN0, pN1);
+        in.vnm = ld2(rowp(a.in[F_NM], j), pM0, pM1);
+        in.pmn = ldg2(a.coef[F_MN] + j * pitch, pN0, pN1);
+        in.pnm = ldg2(a.coef[F_NM] + j * pitch, pM0, pM1);
+        if (KR || KC) {
+            in.rmn = ld2(rowp(a.rin[F_MN], j), pN0, pN1);
+            in.rnm = ld2(rowp(a.rin[F_NM], j), pM0, pM1);
+        }
+        const int i = j - 2;
+        if (core && i >= x0 && i < x1) {
+            in.mu = ldg2(a.coef[F_NN] + i * pitch, pN0, pN1);
+            in.lam = ldg2(a.coef[F_MM0] + i * pitch, pM0, pM1);
+            in.m2 = ldg2(a.coef[F_MM1] + i * pitch, pM0, pM1);
+            if (KR || KC) {
+                in.rnn = ld2(rowp(a.rin[F_NN], i), pN0, pN1);
+                in.rm0 = ld2(rowp(a.rin[F_MM0], i), pM0, pM1);
+                in.rm1 = ld2(rowp(a.rin[F_MM1], i), pM0, pM1);
             }
-            in.vnm = ldS(F_NM, j, pM);
-            in.pnm = ldK(F_NM, j, pM);
-            if (KR) in.rnm = ldR(F_NM, j, pM);
-            if (KC) in.cnm = ldR(F_NM, j, pM);
-            if (ENERGY && core && j >= x0 && j <= x1e) {
-                if (j < Mx && ownN) in.wmn = ldW(F_MN, j, c);
-                if (ownM) in.wnm = ldW(F_NM, j, c);
+            if (ENERGY) {
+                in.wnn = ldg2(a.w[F_NN] + i * pitch, pN0, pN1);
+                in.wm3 = ldg2(a.w[F_MM0] + i * pitch, pM0, pM1);
+                in.wm4 = ldg2(a.w[F_MM1] + i * pitch, pM0, pM1);
             }
         }
-        if (core && i >= x0 && i <= x1e) {
-            if (ownN) {
-                in.mu = ldK(F_NN, i, c);
-                if (KR) in.rnn = ldR(F_NN, i, c);
-                if (KC) in.cnn = ldR(F_NN, i, c);
-                if (ENERGY) in.wnn = ldW(F_NN, i, c);
-            }
-            if (ownM && i < Mx) {
-                in.lam = ldK(F_MM0, i, c);
-                in.m2 = ldK(F_MM1, i, c);
-                if (KR) { in.rm0 = ldR(F_MM0, i, c); in.rm1 = ldR(F_MM1, i, c); }
-                if (KC) { in.cm0 = ldR(F_MM0, i, c); in.cm1 = ldR(F_MM1, i, c); }
-                if (ENERGY) { in.wm3 = ldW(F_MM0, i, c); in.wm4 = ldW(F_MM1, i, c); }
-            }
+        if (ENERGY && core && j >= x0 && j < x1) {
+            in.wmn = ldg2(a.w[F_MN] + j * pitch, pN0, pN1);
+            in.wnm = ldg2(a.w[F_NM] + j * pitch, pM0, pM1);
         }
     };
 
+    // this lane's receivers (at most RC of them in registers; more fall back to the CTA list)
+    constexpr int RC = 2;
+    int rq[RC], nr = 0;
+    bool rmany = false;
+    for (int q = rcv_b; q < rcv_e; q++) {
+        const int col = a.rcv[4 * q + 2];
+        if (core && (col == c0 || col == c1)) {
+            if (nr < RC) rq[nr++] = q;
+            else rmany = true;
+        }
+    }
+    auto record = [&](int slot, int row, int col, double v) {
+        auto hit = [&](int q) {
+            const int *e = a.rcv + 4 * q;
+            if (e[0] == slot && e[1] == row && e[2] == col) a.traces[(long)e[3] * a.max_steps + it] = v;
+        };
+        if (rmany) {
+            for (int q = rcv_b; q < rcv_e; q++) hit(q);
+        } else {
+#pragma unroll
+            for (int k = 0; k < RC; k++)
+                if (k < nr) hit(rq[k]);
+        }
+    };
+    // store the owned values of a pair (owned columns are physical: c0 >= 0 for core lanes)
+    auto put = [&](int f, int row, const P2<C> &s, const P2<C> &r, const P2<C> &cc, bool o0, bool o1) {
+        S *o = a.out[f] + row * pitch;
+        S *ro = KR || KC ? a.rout[f] + row * pitch : nullptr;
+        if ((o0 && !finite(s.a)) || (o1 && !finite(s.b))) atomicOr(a.flags, FLAG_NONFINITE);
+        if (!EDGE) {
+            if (o0) {
+                *reinterpret_cast<typename Vec2<S>::T *>(o + c0) = {to_s<S>(s.a), to_s<S>(s.b)};
+                if (KR) *reinterpret_cast<typename Vec2<S>::T *>(ro + c0) = {to_s<S>(r.a), to_s<S>(r.b)};
+                if (KC) *reinterpret_cast<typename Vec2<S>::T *>(ro + c0) = {to_s<S>(cc.a), to_s<S>(cc.b)};
+            }
+        } else if (o0 && o1 && !(c0 & 1)) {
+            *reinterpret_cast<typename Vec2<S>::T *>(o + c0) = {to_s<S>(s.a), to_s<S>(s.b)};
+            if (KR) *reinterpret_cast<typename Vec2<S>::T *>(ro + c0) = {to_s<S>(r.a), to_s<S>(r.b)};
+            if (KC) *reinterpret_cast<typename Vec2<S>::T *>(ro + c0) = {to_s<S>(cc.a), to_s<S>(cc.b)};
+        } else {
+            if (o0) { o[c0] = to_s<S>(s.a); if (KR) ro[c0] = to_s<S>(r.a); if (KC) ro[c0] = to_s<S>(cc.a); }
+            if (o1) { o[c1] = to_s<S>(s.b); if (KR) ro[c1] = to_s<S>(r.b); if (KC) ro[c1] = to_s<S>(cc.b); }
+        }
+        if (nr > 0 || rmany) {
+            if (o0) record(f, row, c0, (double)s.a);
+            if (o1) record(f, row, c1, (double)s.b);
+        }
+    };
+    // source increment (double)S + A dt / dx^2, rounded once; only the source row takes the branch
+    auto src_add = [&](int grid, int row, P2<C> &s, int pa, int pb) {
+        if (a.src_grid == grid && row == a.src_ix) {
+            if (pa == a.src_iy) s.a = to_s<C>(add((double)s.a, a.src_inc[it]));
+            if (pb == a.src_iy) s.b = to_s<C>(add((double)s.b, a.src_inc[it]));
+        }
+    };
+    auto pair0 = [&](bool keep, const P2<C> &v) { return P2<C>{keep ? v.a : C(0), keep ? v.b : C(0)}; };
+
+    // windows: NN rows j-2..j+2, MM0 rows j-2..j+1, MM1 rows j-2..j, MN rows j-4..j, NM rows j-3..j
+    P2<C> NNw[5], M0w[4], M1w[3], MNw[5], NMw[4];
+    const int jb = x0 - 2, je = x1 + 1;
+#pragma unroll
+    for (int q = 0; q < 4; q++) NNw[q] = ld2(rowp(a.in[F_NN], jb - 2 + q), pN0, pN1);
+#pragma unroll
+    for (int q = 0; q < 3; q++) M0w[q] = ld2(rowp(a.in[F_MM0], jb - 2 + q), pM0, pM1);
+#pragma unroll
+    for (int q = 0; q < 2; q++) M1w[q] = ld2(rowp(a.in[F_MM1], jb - 2 + q), pM0, pM1);
+    Row<C> cur, nxt;
+    fetch(jb, nxt);
+    for (int j = jb; j <= je; j++) {
+        cur = nxt;
+        if (j < je) fetch(j + 1, nxt);
+        NNw[4] = cur.nn;
+        M0w[3] = cur.mm0;
+        M1w[2] = cur.mm1;
+        const bool ownV = j >= x0 && j < x1;
+        // ---- velocities of row j
+        {   // MN: x from NN rows j-1..j+2, y from MM syy row j
+            P2<C> p, n;
+            lanes(M1w[2], p, n);
+            const P2<C> vy = dyNfromM(a.op, M1w[2], p, n);
+            P2<C> vx{C(0), C(0)};
+#pragma unroll
+            for (int w = 0; w < 4; w++) {
+                vx.a = add(vx.a, mul(NNw[1 + w].a, a.op.st[w]));
+                vx.b = add(vx.b, mul(NNw[1 + w].b, a.op.st[w]));
+            }
+            P2<C> r = pair0(KR, cur.rmn), cc = pair0(KC, cur.rmn);
+            r.a = add(r.a, mul(vx.a, cur.pmn.a));
+            r.b = add(r.b, mul(vx.b, cur.pmn.b));
+            r.a = add(r.a, mul(vy.a, cur.pmn.a));
+            r.b = add(r.b, mul(vy.b, cur.pmn.b));
+            P2<C> s = cur.vmn;
+            time_update<CPST>(s.a, r.a, cc.a);
+            time_update<CPST>(s.b, r.b, cc.b);
+            src_add(G_MN, j, s, pN0, pN1);
+            MNw[4] = s;
+            if (ownV) {
+                put(F_MN, j, s, r, cc, oN0, oN1);
+                if (ENERGY) {
+                    if (oN0) E.k = add(E.k, mul(mul((double)s.a, cur.wmn.a), (double)s.a));
+                    if (oN1) E.k = add(E.k, mul(mul((double)s.b, cur.wmn.b), (double)s.b));
+                }
+            }
+        }
+        {   // NM: x from MM sxx rows j-2..j+1, y from NN row j
+            P2<C> p, n;
+            lanes(NNw[2], p, n);
+            P2<C> vy = dyMfromN(a.op, NNw[2], p, n);
+            if (seam0 || seam1) {
+                const S *row = rowp(a.in[F_NN], j);
+                if (seam0) {
+                    vy.a = C(0);
+#pragma unroll
+                    for (int w = 0; w < 4; w++) vy.a = add(vy.a, mul(to_c<C>(row[nread(pM0 - 1 + w, My)]), a.op.st[w]));
+                }
+                if (seam1) {
+                    vy.b = C(0);
+#pragma unroll
+                    for (int w = 0; w < 4; w++) vy.b = add(vy.b, mul(to_c<C>(row[nread(pM1 - 1 + w, My)]), a.op.st[w]));
+                }
+            }
+            P2<C> vx{C(0), C(0)};
+#pragma unroll
+            for (int w = 0; w < 4; w++) {
+                vx.a = add(vx.a, mul(M0w[w].a, a.op.st[w]));
+                vx.b = add(vx.b, mul(M0w[w].b, a.op.st[w]));
+            }
+            P2<C> r = pair0(KR, cur.rnm), cc = pair0(KC, cur.rnm);
+            r.a = add(r.a, mul(vx.a, cur.pnm.a));
+            r.b = add(r.b, mul(vx.b, cur.pnm.b));
+            r.a = add(r.a, mul(vy.a, cur.pnm.a));
+            r.b = add(r.b, mul(vy.b, cur.pnm.b));
+            P2<C> s = cur.vnm;
+            time_update<CPST>(s.a, r.a, cc.a);
+            time_update<CPST>(s.b, r.b, cc.b);
+            src_add(G_NM, j, s, pM0, pM1);
+            NMw[3] = s;
+            if (ownV) {
+                put(F_NM, j, s, r, cc, oM0, oM1);
+                if (ENERGY) {
+                    if (oM0) E.k = add(E.k, mul(mul((double)s.a, cur.wnm.a), (double)s.a));
+                    if (oM1) E.k = add(E.k, mul(mul((double)s.b, cur.wnm.b), (double)s.b));
+                }
+            }
+        }
+        // ---- stresses of row i = j - 2
+        const int i = j - 2;
+        if (i >= x0) {
+            P2<C> p, n;
+            lanes(NMw[1], p, n);
+            const P2<C> vyN = dyNfromM(a.op, NMw[1], p, n);   // NN y from NM row i
+            lanes(MNw[2], p, n);
+            const P2<C> vyM = dyMfromN(a.op, MNw[2], p, n);   // MM y from MN row i
+            if (core) {
+                {   // NN: x from MN rows i-2..i+1
+                    P2<C> vx{C(0), C(0)};
+#pragma unroll
+                    for (int w = 0; w < 4; w++) {
+                        vx.a = add(vx.a, mul(MNw[w].a, a.op.st[w]));
+                        vx.b = add(vx.b, mul(MNw[w].b, a.op.st[w]));
+                    }
+                    P2<C> r = pair0(KR, cur.rnn), cc = pair0(KC, cur.rnn);
+                    r.a = add(r.a, mul(vx.a, cur.mu.a));
+                    r.b = add(r.b, mul(vx.b, cur.mu.b));
+                    r.a = add(r.a, mul(vyN.a, cur.mu.a));
+                    r.b = add(r.b, mul(vyN.b, cur.mu.b));
+                    const P2<C> old = NNw[0];
+                    P2<C> s = old;
+                    time_update<CPST>(s.a, r.a, cc.a);
+                    time_update<CPST>(s.b, r.b, cc.b);
+                    src_add(G_NN, i, s, c0, c1);
+                    put(F_NN, i, s, r, cc, oN0, oN1);
+                    if (ENERGY) {
+                        if (oN0) {
+                            E.p0 = add(E.p0, mul(mul((double)old.a, cur.wnn.a), (double)old.a));
+                            E.p1 = add(E.p1, mul(mul((double)s.a, cur.wnn.a), (double)s.a));
+                        }
+                        if (oN1) {
+                            E.p0 = add(E.p0, mul(mul((double)old.b, cur.wnn.b), (double)old.b));
+                            E.p1 = add(E.p1, mul(mul((double)s.b, cur.wnn.b), (double)s.b));
+                        }
+                    }
+                }
+                {   // MM: x from NM rows i-1..i+2
+                    P2<C> vx{C(0), C(0)};
+#pragma unroll
+                    for (int w = 0; w < 4; w++) {
+                        vx.a = add(vx.a, mul(NMw[w].a, a.op.st[w]));
+                        vx.b = add(vx.b, mul(NMw[w].b, a.op.st[w]));
+                    }
+                    P2<C> r0 = pair0(KR, cur.rm0), k0 = pair0(KC, cur.rm0);
+                    P2<C> r1 = pair0(KR, cur.rm1), k1 = pair0(KC, cur.rm1);
+                    const P2<C> L = cur.lam, M2 = cur.m2;
+                    r0.a = add(r0.a, mul(vx.a, L.a));   r0.b = add(r0.b, mul(vx.b, L.b));
+                    r1.a = add(r1.a, mul(vx.a, L.a));   r1.b = add(r1.b, mul(vx.b, L.b));
+                    r0.a = add(r0.a, mul(vx.a, M2.a));  r0.b = add(r0.b, mul(vx.b, M2.b));
+                    r0.a = add(r0.a, mul(vyM.a, L.a));  r0.b = add(r0.b, mul(vyM.b, L.b));
+                    r1.a = add(r1.a, mul(vyM.a, L.a));  r1.b = add(r1.b, mul(vyM.b, L.b));
+                    r1.a = add(r1.a, mul(vyM.a, M2.a)); r1.b = add(r1.b, mul(vyM.b, M2.b));
+                    const P2<C> o0 = M0w[0], o1 = M1w[0];
+                    P2<C> s0 = o0, s1 = o1;
+                    time_update<CPST>(s0.a, r0.a, k0.a);
+                    time_update<CPST>(s0.b, r0.b, k0.b);
+                    time_update<CPST>(s1.a, r1.a, k1.a);
+                    time_update<CPST>(s1.b, r1.b, k1.b);
+                    src_add(G_MM, i, s0, c0, c1);
+                    src_add(G_MM, i, s1, c0, c1);
+                    put(F_MM0, i, s0, r0, k0, oM0, oM1);
+                    put(F_MM1, i, s1, r1, k1, oM0, oM1);
+                    if (ENERGY) {
+                        if (oM0) {
+                            E.p0 = add(E.p0, mul(mul((double)o0.a, cur.wm3.a), (double)o0.a));
+                            E.p0 = add(E.p0, mul(mul((double)o1.a, cur.wm3.a), (double)o1.a));
+                            E.p0 = add(E.p0, mul(mul((double)o0.a, cur.wm4.a), (double)o1.a));
+                            E.p1 = add(E.p1, mul(mul((double)s0.a, cur.wm3.a), (double)s0.a));
+                            E.p1 = add(E.p1, mul(mul((double)s1.a, cur.wm3.a), (double)s1.a));
+                            E.p1 = add(E.p1, mul(mul((double)s0.a, cur.wm4.a), (double)s1.a));
+                        }
+                        if (oM1) {
+                            E.p0 = add(E.p0, mul(mul((double)o0.b, cur.wm3.b), (double)o0.b));
+                            E.p0 = add(E.p0, mul(mul((double)o1.b, cur.wm3.b), (double)o1.b));
+                            E.p0 = add(E.p0, mul(mul((double)o0.b, cur.wm4.b), (double)o1.b));
+                            E.p1 = add(E.p1, mul(mul((double)s0.b, cur.wm3.b), (double)s0.b));
+                            E.p1 = add(E.p1, mul(mul((double)s1.b, cur.wm3.b), (double)s1.b));
+                            E.p1 = add(E.p1, mul(mul((double)s0.b, cur.wm4.b), (double)s1.b));
+                        }
+                    }
+                }
+            }
+        }
+        // ---- slide the windows
+#pragma unroll
+        for (int q = 0; q < 4; q++) NNw[q] = NNw[q + 1];
+#pragma unroll
+        for (int q = 0; q < 3; q++) M0w[q] = M0w[q + 1];
+#pragma unroll
+        for (int q = 0; q < 2; q++) M1w[q] = M1w[q + 1];
+#pragma unroll
+        for (int q = 0; q < 4; q++) MNw[q] = MNw[q + 1];
+#pragma unroll
+        for (int q = 0; q < 3; q++) NMw[q] = NMw[q + 1];
+    }
+}
+
+// ------------------------------------------------------------------------------- boundary CTA
+template <class S, class C, int CPST, bool ENERGY>
+__device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int it, int rcv_b, int rcv_e, C *tile,
+                             EAcc &E)
+{
+    constexpr bool KR = Cpst<CPST>::keep_r, KC = Cpst<CPST>::keep_c;
+    constexpr int NT = FS_BND_W;                 // tile row length: the strip's logical columns
+    constexpr int RG = FS_BND_THREADS / FS_BND_W;   // row groups: thread rows t / NT walk rows g, g + RG, ...
+    const int t = threadIdx.x % NT, g = threadIdx.x / NT;
+    const int Mx = a.Mx, My = a.My;
+    const long pitch = a.pitch;
+    const int c = bstrip * FS_BND_TY - 4 + t;
+    const int pM = pmod(c, My), pN = (c >= 0 && c <= My) ? c : pM;
+    const bool core = t >= 4 && t < 4 + FS_BND_TY;
+    const bool ownN = core && c <= My, ownM = core && c < My;
+    const bool velT = t >= 2 && t < NT - 2;
+    int zr0, zr1;   // zone rows (N-type grids up to zr1, M-type up to min(zr1, Mx - 1))
+    if (a.n_zone == 1) { zr0 = 0; zr1 = Mx; }
+    else if (zone == 0) { zr0 = 0; zr1 = FS_ZONE - 1; }
+    else { zr0 = Mx - FS_ZONE; zr1 = Mx; }
+    const int vr0 = max(zr0 - 2, 0), vr1 = min(zr1 + 2, Mx);
+    C *tMN = tile, *tNM = tile + a.tile_rows * NT;
+
+    bool mine = false;   // does any receiver of the CTA sit in this thread's column
+    for (int q = rcv_b; q < rcv_e; q++) mine |= core && a.rcv[4 * q + 2] == c;
     auto record = [&](int slot, int row, double v) {
         for (int q = rcv_b; q < rcv_e; q++) {
             const int *e = a.rcv + 4 * q;
             if (e[0] == slot && e[1] == row && e[2] == c) a.traces[(long)e[3] * a.max_steps + it] = v;
         }
     };
-
-    auto store = [&](int f, int row, C s, C r, C cc, bool src) {
-        if (src) s = to_s<C>(add((double)s, a.src_inc[it]));
+    auto put = [&](int f, int row, C s, C r, C cc) {
         if (!finite(s)) atomicOr(a.flags, FLAG_NONFINITE);
         const long o = (long)row * pitch + c;
         a.out[f][o] = to_s<S>(s);
         if (KR) a.rout[f][o] = to_s<S>(r);
         if (KC) a.rout[f][o] = to_s<S>(cc);
-        return s;
+        if (mine) record(f, row, (double)s);
+    };
+    auto ldr = [&](int f, int row, int col, C &r, C &cc) {
+        r = C(0);
+        cc = C(0);
+        if (KR) r = to_c<C>(a.rin[f][(long)row * pitch + col]);
+        if (KC) cc = to_c<C>(a.rin[f][(long)row * pitch + col]);
     };
 
-    EAcc E;
-    Inputs<S, C, CPST> cur{}, nxt{};
-    fetch(lb + 1, nxt);
-    const int ke = x1e + LAG_S;
-    for (int k = lb + 1; k <= ke; k++) {
-        cur = nxt;
-        if (k + 1 <= ke) fetch(k + 1, nxt);
-        const int sr = k - 1;
-        if (sr >= lb && sr <= le) {
-            rNN.at(sr, t) = cur.nn;
-            if (sr < Mx) { rM0.at(sr, t) = cur.mm0; rM1.at(sr, t) = cur.mm1; }
-        }
-        // old stress rows up to k-1 are staged; rows up to k-2 are visible to other threads
-        const int j = k - LAG_V;
-        if (velT && j >= vb && j <= ve) {
-            const bool ownRow = j >= x0 && j <= x1e;
-            if (j < Mx) {   // MN: x from NN (DN closures), SAT from NN rows 0 / Mx, y from MM syy
-                C v = C(0);
-                if (j < 3) {
-#pragma unroll
-                    for (int w = 0; w < 5; w++) v = add(v, mul(rNN.at(w, t), a.op.dnL[j][w]));
-                } else if (j >= Mx - 3) {
-#pragma unroll
-                    for (int w = 0; w < 5; w++) v = add(v, mul(rNN.at(Mx - 4 + w, t), a.op.dnR[j - (Mx - 3)][w]));
-                } else {
-#pragma unroll
-                    for (int w = 0; w < 4; w++) v = add(v, mul(rNN.at(j - 1 + w, t), a.op.st[w]));
-                }
-                C r = KR ? cur.rmn : C(0), cc = KC ? cur.cmn : C(0);
-                const C P = cur.pmn;
+    // phase 1: velocities of rows vr0..vr1 at every velocity column (physical reads)
+    if (velT) {
+        for (int j = vr0 + g; j <= vr1; j += RG) {
+            const bool ownRow = j >= zr0 && j <= zr1;
+            if (j < Mx) {   // MN
+                C r, cc;
+                ldr(F_MN, j, pN, r, cc);
+                const C P = __ldg(a.coef[F_MN] + (long)j * pitch + pN);
+                C v = dx_from_N<C>(a.op, a.in[F_NN], pitch, Mx, j, pN);
                 r = add(r, mul(v, P));
-                if (j < 3) {
-                    const C send = add(C(0), mul(a.op.pN, rNN.at(0, t)));
-                    r = add(r, mul(mul(a.op.satML[j], sub(send, C(0))), P));
-                } else if (j >= Mx - 3) {
-                    const C send = add(C(0), mul(a.op.pN, rNN.at(Mx, t)));
-                    r = add(r, mul(mul(a.op.satMR[j - (Mx - 3)], sub(send, C(0))), P));
-                }
-                v = C(0);
-#pragma unroll
-                for (int w = 0; w < 4; w++) v = add(v, mul(rM1.at(j, t - 2 + w), a.op.st[w]));
+                if (sat_MN<C>(a.op, a.in[F_NN], pitch, Mx, j, pN, v)) r = add(r, mul(v, P));
+                v = dy_periodic<false, C>(a.op, a.in[F_MM1] + (long)j * pitch, My, pN);
                 r = add(r, mul(v, P));
-                C s = cur.vmn;
+                C s = to_c<C>(a.in[F_MN][(long)j * pitch + pN]);
                 time_update<CPST>(s, r, cc);
-                const bool src = a.src_grid == G_MN && j == a.src_ix && pN == a.src_iy;
-                if (src) s = to_s<C>(add((double)s, a.src_inc[it]));
-                rMN.at(j, t) = s;
+                if (a.src_grid == G_MN && j == a.src_ix)
+                    if (pN == a.src_iy) s = to_s<C>(add((double)s, a.src_inc[it]));
+                tMN[(j - vr0) * NT + t] = s;
                 if (ownRow && ownN) {
-                    store(F_MN, j, s, r, cc, false);
-                    if (ENERGY) E.k = add(E.k, mul(mul((double)s, cur.wmn), (double)s));
-                    if (rcv_b < rcv_e) record(F_MN, j, (double)s);
+                    put(F_MN, j, s, r, cc);
+                    if (ENERGY) E.k = add(E.k, mul(mul((double)s, __ldg(a.w[F_MN] + (long)j * pitch + c)), (double)s));
                 }
             }
-            {   // NM: x from MM sxx (DM closures), SAT from MM rows 0..2 / Mx-3..Mx-1, y from NN
-                C v = C(0);
-                if (j < 4) {
-#pragma unroll
-                    for (int w = 0; w < 5; w++) v = add(v, mul(rM0.at(w, t), a.op.dmL[j][w]));
-                } else if (j >= Mx - 3) {
-#pragma unroll
-                    for (int w = 0; w < 5; w++) v = add(v, mul(rM0.at(Mx - 5 + w, t), a.op.dmR[j - (Mx - 3)][w]));
-                } else {
-#pragma unroll
-                    for (int w = 0; w < 4; w++) v = add(v, mul(rM0.at(j - 2 + w, t), a.op.st[w]));
-                }
-                C r = KR ? cur.rnm : C(0), cc = KC ? cur.cnm : C(0);
-                const C P = cur.pnm;
+            {   // NM
+                C r, cc;
+                ldr(F_NM, j, pM, r, cc);
+                const C P = __ldg(a.coef[F_NM] + (long)j * pitch + pM);
+                C v = dx_from_M<C>(a.op, a.in[F_MM0], pitch, Mx, j, pM);
                 r = add(r, mul(v, P));
-                if (j == 0 || j == Mx) {
-                    C send = C(0);
-                    if (j == 0) {
-#pragma unroll
-                        for (int w = 0; w < 3; w++) send = add(send, mul(a.op.pML[w], rM0.at(w, t)));
-                        r = add(r, mul(mul(a.op.satNL, sub(send, C(0))), P));
-                    } else {
-#pragma unroll
-                        for (int w = 0; w < 3; w++) send = add(send, mul(a.op.pMR[w], rM0.at(Mx - 3 + w, t)));
-                        r = add(r, mul(mul(a.op.satNR, sub(send, C(0))), P));
-                    }
-                }
-                v = C(0);
-                if (!(c == -2 || c == -1 || c == My || c == My + 1)) {
-                    // taps c-1..c+2 of NN held in the strip's logical columns are the physical
-                    // taps of this column (the only NM columns whose values are used lie in
-                    // [-2, My+1]; of those, the four next to the seam differ)
-#pragma unroll
-                    for (int w = 0; w < 4; w++) v = add(v, mul(rNN.at(j, t - 1 + w), a.op.st[w]));
-                } else {
-                    // a column next to the periodic seam: NN column My and column 0 are distinct
-                    // points, so read NN by the physical rule
-                    const S *row = a.in[F_NN] + (long)j * pitch;
-#pragma unroll
-                    for (int w = 0; w < 4; w++) v = add(v, mul(to_c<C>(row[nread(pM - 1 + w, My)]), a.op.st[w]));
-                }
+                if (sat_NM<C>(a.op, a.in[F_MM0], pitch, Mx, j, pM, v)) r = add(r, mul(v, P));
+                v = dy_periodic<true, C>(a.op, a.in[F_NN] + (long)j * pitch, My, pM);
                 r = add(r, mul(v, P));
-                C s = cur.vnm;
+                C s = to_c<C>(a.in[F_NM][(long)j * pitch + pM]);
                 time_update<CPST>(s, r, cc);
-                const bool src = a.src_grid == G_NM && j == a.src_ix && pM == a.src_iy;
-                if (src) s = to_s<C>(add((double)s, a.src_inc[it]));
-                rNM.at(j, t) = s;
+                if (a.src_grid == G_NM && j == a.src_ix)
+                    if (pM == a.src_iy) s = to_s<C>(add((double)s, a.src_inc[it]));
+                tNM[(j - vr0) * NT + t] = s;
                 if (ownRow && ownM) {
-                    store(F_NM, j, s, r, cc, false);
-                    if (ENERGY) E.k = add(E.k, mul(mul((double)s, cur.wnm), (double)s));
-                    if (rcv_b < rcv_e) record(F_NM, j, (double)s);
+                    put(F_NM, j, s, r, cc);
+                    if (ENERGY) E.k = add(E.k, mul(mul((double)s, __ldg(a.w[F_NM] + (long)j * pitch + c)), (double)s));
                 }
             }
         }
-        const int i = k - LAG_S;
-        if (core && i >= x0 && i <= x1e) {
-            if (ownN) {   // NN: x from MN (DM closures), y from NM
-                C v = C(0);
-                if (i < 4) {
-#pragma unroll
-                    for (int w = 0; w < 5; w++) v = add(v, mul(rMN.at(w, t), a.op.dmL[i][w]));
-                } else if (i >= Mx - 3) {
-#pragma unroll
-                    for (int w = 0; w < 5; w++) v = add(v, mul(rMN.at(Mx - 5 + w, t), a.op.dmR[i - (Mx - 3)][w]));
-                } else {
-#pragma unroll
-                    for (int w = 0; w < 4; w++) v = add(v, mul(rMN.at(i - 2 + w, t), a.op.st[w]));
-                }
-                C r = KR ? cur.rnn : C(0), cc = KC ? cur.cnn : C(0);
-                const C P = cur.mu;
+    }
+    __syncthreads();
+    // phase 2: stresses of the zone rows from the velocity tile
+    if (core) {
+        for (int i = zr0 + g; i <= zr1; i += RG) {
+            const long o = (long)i * pitch + c;
+            if (ownN) {   // NN
+                C r, cc;
+                ldr(F_NN, i, c, r, cc);
+                const C P = __ldg(a.coef[F_NN] + o);
+                C v = dxM<C>(a.op, Mx, i, [&](int rr) { return tMN[(rr - vr0) * NT + t]; });
                 r = add(r, mul(v, P));
                 v = C(0);
 #pragma unroll
-                for (int w = 0; w < 4; w++) v = add(v, mul(rNM.at(i, t - 2 + w), a.op.st[w]));
+                for (int w = 0; w < 4; w++) v = add(v, mul(tNM[(i - vr0) * NT + t - 2 + w], a.op.st[w]));
                 r = add(r, mul(v, P));
-                const C old = rNN.at(i, t);
-                if (ENERGY) E.p0 = add(E.p0, mul(mul((double)old, cur.wnn), (double)old));
+                const C old = to_c<C>(a.in[F_NN][o]);
                 C s = old;
                 time_update<CPST>(s, r, cc);
-                s = store(F_NN, i, s, r, cc, a.src_grid == G_NN && i == a.src_ix && c == a.src_iy);
-                if (ENERGY) E.p1 = add(E.p1, mul(mul((double)s, cur.wnn), (double)s));
-                if (rcv_b < rcv_e) record(F_NN, i, (double)s);
-            }
-            if (ownM && i < Mx) {   // MM: x from NM (DN closures), y from MN
-                C v = C(0);
-                if (i < 3) {
-#pragma unroll
-                    for (int w = 0; w < 5; w++) v = add(v, mul(rNM.at(w, t), a.op.dnL[i][w]));
-                } else if (i >= Mx - 3) {
-#pragma unroll
-                    for (int w = 0; w < 5; w++) v = add(v, mul(rNM.at(Mx - 4 + w, t), a.op.dnR[i - (Mx - 3)][w]));
-                } else {
-#pragma unroll
-                    for (int w = 0; w < 4; w++) v = add(v, mul(rNM.at(i - 1 + w, t), a.op.st[w]));
+                if (a.src_grid == G_NN && i == a.src_ix)
+                    if (c == a.src_iy) s = to_s<C>(add((double)s, a.src_inc[it]));
+                put(F_NN, i, s, r, cc);
+                if (ENERGY) {
+                    const double w = __ldg(a.w[F_NN] + o);
+                    E.p0 = add(E.p0, mul(mul((double)old, w), (double)old));
+                    E.p1 = add(E.p1, mul(mul((double)s, w), (double)s));
                 }
-                C r0 = KR ? cur.rm0 : C(0), c0 = KC ? cur.cm0 : C(0);
-                C r1 = KR ? cur.rm1 : C(0), c1 = KC ? cur.cm1 : C(0);
-                const C L = cur.lam, M2 = cur.m2;
+            }
+            if (ownM && i < Mx) {   // MM
+                C r0, k0, r1, k1;
+                ldr(F_MM0, i, c, r0, k0);
+                ldr(F_MM1, i, c, r1, k1);
+                const C L = __ldg(a.coef[F_MM0] + o), M2 = __ldg(a.coef[F_MM1] + o);
+                C v = dxN<C>(a.op, Mx, i, [&](int rr) { return tNM[(rr - vr0) * NT + t]; });
                 r0 = add(r0, mul(v, L));
                 r1 = add(r1, mul(v, L));
                 r0 = add(r0, mul(v, M2));
                 v = C(0);
 #pragma unroll
-                for (int w = 0; w < 4; w++) v = add(v, mul(rMN.at(i, t - 1 + w), a.op.st[w]));
+                for (int w = 0; w < 4; w++) v = add(v, mul(tMN[(i - vr0) * NT + t - 1 + w], a.op.st[w]));
                 r0 = add(r0, mul(v, L));
                 r1 = add(r1, mul(v, L));
                 r1 = add(r1, mul(v, M2));
-                const C o0 = rM0.at(i, t), o1 = rM1.at(i, t);
-                if (ENERGY) {
-                    E.p0 = add(E.p0, mul(mul((double)o0, cur.wm3), (double)o0));
-                    E.p0 = add(E.p0, mul(mul((double)o1, cur.wm3), (double)o1));
-                    E.p0 = add(E.p0, mul(mul((double)o0, cur.wm4), (double)o1));
-                }
+                const C o0 = to_c<C>(a.in[F_MM0][o]), o1 = to_c<C>(a.in[F_MM1][o]);
                 C s0 = o0, s1 = o1;
-                time_update<CPST>(s0, r0, c0);
-                time_update<CPST>(s1, r1, c1);
-                const bool src = a.src_grid == G_MM && i == a.src_ix && c == a.src_iy;
-                s0 = store(F_MM0, i, s0, r0, c0, src);
-                s1 = store(F_MM1, i, s1, r1, c1, src);
-                if (ENERGY) {
-                    E.p1 = add(E.p1, mul(mul((double)s0, cur.wm3), (double)s0));
-                    E.p1 = add(E.p1, mul(mul((double)s1, cur.wm3), (double)s1));
-                    E.p1 = add(E.p1, mul(mul((double)s0, cur.wm4), (double)s1));
+                time_update<CPST>(s0, r0, k0);
+                time_update<CPST>(s1, r1, k1);
+                if (a.src_grid == G_MM && i == a.src_ix && c == a.src_iy) {   // (branch taken by one thread)
+                    s0 = to_s<C>(add((double)s0, a.src_inc[it]));
+                    s1 = to_s<C>(add((double)s1, a.src_inc[it]));
                 }
-                if (rcv_b < rcv_e) { record(F_MM0, i, (double)s0); record(F_MM1, i, (double)s1); }
+                put(F_MM0, i, s0, r0, k0);
+                put(F_MM1, i, s1, r1, k1);
+                if (ENERGY) {
+                    const double w3 = __ldg(a.w[F_MM0] + o), w4 = __ldg(a.w[F_MM1] + o);
+                    E.p0 = add(E.p0, mul(mul((double)o0, w3), (double)o0));
+                    E.p0 = add(E.p0, mul(mul((double)o1, w3), (double)o1));
+                    E.p0 = add(E.p0, mul(mul((double)o0, w4), (double)o1));
+                    E.p1 = add(E.p1, mul(mul((double)s0, w3), (double)s0));
+                    E.p1 = add(E.p1, mul(mul((double)s1, w3), (double)s1));
+                    E.p1 = add(E.p1, mul(mul((double)s0, w4), (double)s1));
+                }
             }
         }
-        __syncthreads();
     }
+}
 
+// ------------------------------------------------------------------------------- the launch
+template <class S, class C, int CPST, bool ENERGY>
+__global__ void __launch_bounds__(FS_THREADS_MAX, TW_FS_MIN_BLOCKS) k_elastic_fused(FusedArgs<S, C> a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int it = *a.step;
+    const int cta = blockIdx.x;
+    const int rcv_b = a.rcv_off[cta], rcv_e = a.rcv_off[cta + 1];
+    EAcc E;
+    const int n_int = a.n_int_seg * a.n_int_x;
+    if (cta < n_int) {   // interior CTA (segment, group of FS_WARPS warp strips)
+        const int seg = cta / a.n_int_x, wstrip = (cta % a.n_int_x) * FS_WARPS + (threadIdx.x >> 5);
+        const int y0 = wstrip * FS_WARP_CORE;
+        if (wstrip < a.n_wstrip) {
+            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false>(a, wstrip, seg, it, rcv_b, rcv_e, E);
+            else interior_warp<S, C, CPST, ENERGY, true>(a, wstrip, seg, it, rcv_b, rcv_e, E);
+        }
+    } else {             // boundary CTA (zone, strip)
+        const int b = cta - n_int;
+        boundary_cta<S, C, CPST, ENERGY>(a, b % a.n_bstrip, b / a.n_bstrip, it, rcv_b, rcv_e,
+                                         reinterpret_cast<C *>(smem_raw), E);
+    }
     if (ENERGY) {
-        __shared__ double red[3][NT / 32];
+        __shared__ double red[3][FS_THREADS_MAX / 32];
         double e3[3] = {E.p0, E.k, E.p1};
 #pragma unroll
         for (int q = 0; q < 3; q++) {
             double v = e3[q];
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-            if ((t & 31) == 0) red[q][t >> 5] = v;
+            for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+            if ((threadIdx.x & 31) == 0) red[q][threadIdx.x >> 5] = v;
         }
         __syncthreads();
-        if (t < 3) {
+        if (threadIdx.x < 3) {
             double v = 0.;
-            for (int w = 0; w < NT / 32; w++) v += red[t][w];
-            if (it < a.max_steps) atomicAdd(a.energy + (long)t * a.max_steps + it, 0.5 * v);
+            for (int w = 0; w < (int)(blockDim.x >> 5); w++) v += red[threadIdx.x][w];
+            if (it < a.max_steps && v != 0.) atomicAdd(a.energy + (long)threadIdx.x * a.max_steps + it, 0.5 * v);
         }
     }
     // the last CTA to finish advances the step counter
     __syncthreads();
-    if (t == 0) {
+    if (threadIdx.x == 0) {
         __threadfence();
         const int ticket = atomicAdd(a.done, 1);
-        if (ticket == gridDim.x * gridDim.y - 1) {
+        if (ticket == gridDim.x - 1) {
             *a.done = 0;
             *a.step = it + 1;
             __threadfence();
@@ -369,41 +647,44 @@ __global__ void __launch_bounds__(NT) k_elastic_fused(FusedArgs<S, C> a)
     }
 }
 
-// ---------------------------------------------------------------- launcher
+// ------------------------------------------------------------------------------- launcher
 namespace {
-template <class C>
-constexpr size_t fused_smem() { return sizeof(C) * (size_t)(3 * RS + 2 * RV) * NT; }
-
 template <class S, class C, int N>
-cudaError_t set_attr()
+cudaError_t set_attr(int smem)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)fused_smem<C>());
+    cudaError_t e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_elastic_fused<S, C, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)fused_smem<C>());
+    return cudaFuncSetAttribute(k_elastic_fused<S, C, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
 }  // namespace
 
-// shared-memory opt-in for every variant; called at handle creation, outside any stream capture
+template <class S, class C>
+size_t fused_smem_bytes(int tile_rows)
+{
+    return sizeof(C) * 2 * (size_t)tile_rows * FS_BND_W;
+}
+
+// shared-memory opt-in for every variant at the largest tile; called at handle creation,
+// outside any stream capture
 template <class S, class C>
 cudaError_t prepare_fused()
 {
+    const int smem = (int)fused_smem_bytes<S, C>(FS_SMALL_MX + 1);
     cudaError_t e;
-    if ((e = set_attr<S, C, 0>()) != cudaSuccess) return e;
-    if ((e = set_attr<S, C, 1>()) != cudaSuccess) return e;
-    if ((e = set_attr<S, C, 2>()) != cudaSuccess) return e;
-    if ((e = set_attr<S, C, 3>()) != cudaSuccess) return e;
-    if ((e = set_attr<S, C, 4>()) != cudaSuccess) return e;
-    if ((e = set_attr<S, C, 5>()) != cudaSuccess) return e;
-    return set_attr<S, C, 6>();
+    if ((e = set_attr<S, C, 0>(smem)) != cudaSuccess) return e;
+    if ((e = set_attr<S, C, 1>(smem)) != cudaSuccess) return e;
+    if ((e = set_attr<S, C, 2>(smem)) != cudaSuccess) return e;
+    if ((e = set_attr<S, C, 3>(smem)) != cudaSuccess) return e;
+    if ((e = set_attr<S, C, 4>(smem)) != cudaSuccess) return e;
+    if ((e = set_attr<S, C, 5>(smem)) != cudaSuccess) return e;
+    return set_attr<S, C, 6>(smem);
 }
 
 template <class S, class C>
 void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, cudaStream_t st)
 {
-    const dim3 grid(a.n_strip, a.n_seg), block(NT);
-    const size_t smem = fused_smem<C>();
+    const dim3 grid(a.n_int_seg * a.n_int_x + a.n_zone * a.n_bstrip), block(FS_THREADS_MAX);
+    const size_t smem = fused_smem_bytes<S, C>(a.tile_rows);
 #define TW_FUSED_CASE(N)                                                              \
     case N:                                                                           \
         if (energy) k_elastic_fused<S, C, N, true><<<grid, block, smem, st>>>(a);    \

@@ -53,10 +53,29 @@ struct EnergyArgs {
 template <class S, class C>
 void launch_energy(const EnergyArgs<S, C> &e, cudaStream_t st);
 
-// fused elastic step (fused_step.cu): one CTA per strip of FS_TY columns x segment of rows
-constexpr int FS_THREADS = 256;
-constexpr int FS_HALO = 4;
-constexpr int FS_TY = FS_THREADS - 2 * FS_HALO;
+// fused elastic step (fused_step.cu): interior CTAs of FS_WARPS independent warps, each warp a
+// strip of FS_WARP_CORE columns over a segment of interior rows; boundary CTAs of
+// FS_BND_THREADS threads for the FS_ZONE rows at each free surface (or the whole grid when
+// Mx < FS_SMALL_MX)
+// tuning constants (a build may override them with -D)
+#ifndef TW_FS_WARPS
+#define TW_FS_WARPS 4                 // warps per interior CTA
+#endif
+#ifndef TW_FS_MIN_BLOCKS
+#define TW_FS_MIN_BLOCKS 4            // CTAs per SM the register allocation is sized for
+#endif
+#ifndef TW_FS_CTAS_PER_SM
+#define TW_FS_CTAS_PER_SM 8           // CTAs per SM the row segmentation aims at (two waves)
+#endif
+constexpr int FS_WARP_CORE = 56;      // 28 core lanes x 2 columns; 2 halo lanes on each side
+constexpr int FS_WARPS = TW_FS_WARPS;
+constexpr int FS_ZONE = 8;
+// both CTA kinds share the launch and its block size
+constexpr int FS_THREADS_MAX = FS_WARPS * 32;
+constexpr int FS_BND_THREADS = FS_THREADS_MAX;   // row groups of FS_BND_W threads
+constexpr int FS_BND_W = 64;                 // logical columns of a boundary strip (4 halo on each side)
+constexpr int FS_BND_TY = FS_BND_W - 8;      // core columns of a boundary strip
+constexpr int FS_SMALL_MX = 24;
 
 template <class S, class C>
 struct FusedArgs {
@@ -68,7 +87,11 @@ struct FusedArgs {
     long pitch;
     int Mx, My;
     Ops<C> op;
-    int seg_rows, n_seg, n_strip;
+    int n_int_seg, int_rows;  // interior rows [FS_ZONE, Mx - FS_ZONE) = int_rows, in n_int_seg balanced segments
+    int n_zone;               // 2 boundary zones, or 1 zone holding the whole grid
+    int n_wstrip, n_bstrip;   // interior warp strips, boundary strips
+    int n_int_x;              // interior CTAs per segment (groups of FS_WARPS warp strips)
+    int tile_rows;
     const double *src_inc;
     int src_grid, src_ix, src_iy;
     int *step;                // read by every CTA; the last CTA to finish advances it
@@ -77,7 +100,8 @@ struct FusedArgs {
     int max_steps;
     const double *w[5];       // energy weights (ENERGY only)
     double *energy;           // [3][max_steps]: E_p0, E_k, E_p1
-    const int *rcv_off;       // receivers owned by each CTA (CSR over blockIdx.y * n_strip + blockIdx.x)
+    const int *rcv_off;       // receivers owned by each CTA (CSR over blockIdx.x: interior CTAs
+                              // segment-major, then boundary CTAs zone-major)
     const int *rcv;           // [n][4]: field slot, row, column, trace row (2 * receiver + field)
     double *traces;
 };

@@ -71,7 +71,7 @@ struct tw_solver {
     bool fused = false;
     void *f2[5] = {}, *res2[5] = {};
     int parity = 0;                   // which buffer holds the current state (0: f/res, 1: f2/res2)
-    int seg_rows = 0, n_seg = 1, n_strip = 1;
+    int n_int_seg = 0, int_rows = 0, n_zone = 1, n_wstrip = 0, n_bstrip = 1, n_int_x = 0, tile_rows = 1;
     int *d_done = nullptr, *d_rcv_off = nullptr, *d_rcv_list = nullptr;
     int rcv_list_cap = 0;
     double *w[5] = {}, *mat[5] = {};
@@ -237,9 +237,13 @@ void enqueue_fused_step(tw_solver *s, cudaStream_t st)
     a.Mx = (int)s->d.Mx;
     a.My = (int)s->d.My;
     a.op = make_ops<C>((double)s->d.num_dx / (double)s->d.den_dx, s->d.dt, false);
-    a.seg_rows = s->seg_rows;
-    a.n_seg = s->n_seg;
-    a.n_strip = s->n_strip;
+    a.n_int_seg = s->n_int_seg;
+    a.int_rows = s->int_rows;
+    a.n_zone = s->n_zone;
+    a.n_wstrip = s->n_wstrip;
+    a.n_bstrip = s->n_bstrip;
+    a.n_int_x = s->n_int_x;
+    a.tile_rows = s->tile_rows;
     a.src_inc = s->src_inc;
     a.src_grid = s->src_grid;
     a.src_ix = (int)s->src_ix;
@@ -373,13 +377,24 @@ int upload_receivers(tw_solver *s)
     if (s->fused) {
         // per-CTA receiver lists: a receiver belongs to the CTA whose segment owns its row and
         // whose strip owns its column (fused_step.cu)
-        const int nctas = s->n_seg * s->n_strip;
+        const int n_int = s->n_int_seg * s->n_int_x;
+        const int nctas = n_int + s->n_zone * s->n_bstrip;
         std::vector<std::vector<int>> per(nctas);
+        const int Mx = (int)s->d.Mx;
         for (int r = 0; r < n; r++) {
             const int *q = &s->rcv_tab[4 * r];
-            const int seg = std::min(q[2] / s->seg_rows, s->n_seg - 1), strip = q[3] / FS_TY;
+            const int row = q[2], col = q[3];
+            int cta;
+            if (s->n_zone == 1 || row < FS_ZONE || row >= Mx - FS_ZONE) {
+                const int zone = (s->n_zone == 1 || row < FS_ZONE) ? 0 : 1;
+                cta = n_int + zone * s->n_bstrip + col / FS_BND_TY;
+            } else {
+                int seg = 0;   // the balanced segment holding the row (fused_step.cu)
+                while (FS_ZONE + (int)((long)(seg + 1) * s->int_rows / s->n_int_seg) <= row) seg++;
+                cta = seg * s->n_int_x + col / FS_WARP_CORE / FS_WARPS;
+            }
             for (int f = 0; f < 2; f++)
-                if (q[f] >= 0) per[seg * s->n_strip + strip].insert(per[seg * s->n_strip + strip].end(), {q[f], q[2], q[3], 2 * r + f});
+                if (q[f] >= 0) per[cta].insert(per[cta].end(), {q[f], row, col, 2 * r + f});
         }
         std::vector<int> off(nctas + 1, 0), list;
         for (int c = 0; c < nctas; c++) {
@@ -549,16 +564,29 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
                 cudaMemsetAsync(s->res2[k], 0, n * s->esz, s->st);
             }
         }
-        s->n_strip = (int)((My + 1 + FS_TY - 1) / FS_TY);
-        // about three CTAs per SM of a 148-SM B200; segments of at least 16 rows, the last one
-        // taking the remainder
-        const int target = std::max(1, 444 / s->n_strip);
-        s->seg_rows = std::max(16, (int)((Mx + target - 1) / target));
-        s->n_seg = std::max(1, (int)(Mx / s->seg_rows));
+        s->n_bstrip = (int)((My + 1 + FS_BND_TY - 1) / FS_BND_TY);
+        s->n_wstrip = (int)((My + 1 + FS_WARP_CORE - 1) / FS_WARP_CORE);
+        if (Mx < FS_SMALL_MX) {
+            s->n_int_seg = 0;
+            s->n_zone = 1;
+            s->tile_rows = (int)Mx + 1;
+        } else {
+            // interior segments sized for about two 8-warp CTAs per SM of a 148-SM B200, at least
+            // 8 rows each, the last one taking the remainder
+            s->n_zone = 2;
+            s->tile_rows = 12;
+            s->n_int_x = (s->n_wstrip + FS_WARPS - 1) / FS_WARPS;
+            s->int_rows = (int)Mx - 2 * FS_ZONE;
+            // one wave of TW_FS_CTAS_PER_SM CTAs on each of the 148 SMs, the boundary CTAs
+            // included; segments of 8 rows or more
+            const int target = std::max(1, (148 * TW_FS_CTAS_PER_SM - 2 * s->n_bstrip) / s->n_int_x);
+            s->n_int_seg = std::max(1, std::min(target, s->int_rows / 8));
+        }
+        const int nctas = s->n_int_seg * s->n_int_x + s->n_zone * s->n_bstrip;
         if ((rc_ = s->alloc((void **)&s->d_done, sizeof(int))) != TW_OK) return fail(rc_);
         cudaMemsetAsync(s->d_done, 0, sizeof(int), s->st);
-        if ((rc_ = s->alloc((void **)&s->d_rcv_off, sizeof(int) * (s->n_seg * s->n_strip + 1))) != TW_OK) return fail(rc_);
-        cudaMemsetAsync(s->d_rcv_off, 0, sizeof(int) * (s->n_seg * s->n_strip + 1), s->st);
+        if ((rc_ = s->alloc((void **)&s->d_rcv_off, sizeof(int) * (nctas + 1))) != TW_OK) return fail(rc_);
+        cudaMemsetAsync(s->d_rcv_off, 0, sizeof(int) * (nctas + 1), s->st);
     }
     if ((rc_ = s->alloc((void **)&s->src_inc, sizeof(double) * d.max_steps)) != TW_OK) return fail(rc_);
     if ((rc_ = s->alloc((void **)&s->d_energy, sizeof(double) * 3 * d.max_steps)) != TW_OK) return fail(rc_);
@@ -902,6 +930,7 @@ int tw_profile(tw_solver *s, int n, double *ms)
     for (auto &x : ev) cudaEventDestroy(x);
     if (e != cudaSuccess) return cuda_fail(e, "tw_profile");
     for (int ph = 0; ph < 4; ph++) ms[ph] = acc[ph] / n;
+    if (s->fused) ms[1] = ms[2] = ms[3] = 0.;   // the fused step launches nothing else
     s->steps_done += n;
     return TW_OK;
 }

@@ -45,45 +45,57 @@ __device__ __forceinline__ C ld(const __nv_bfloat16 *p, long i) { return to_c<C>
 template <class C>
 __device__ __forceinline__ C ld(const __half *p, long i) { return to_c<C>(p[i]); }
 
-// derivative along x of an M-type-x grid (rows 0..Mx-1) from its N-type neighbour with rows
+// derivative along x of an M-type-x row ix (rows 0..Mx-1) from its N-type neighbour with rows
 // 0..Mx: DN closures on 3 rows at each end, interior shifts {-1,0,1,2} (grid_drvt.tpp:312-466,
-// grid.hpp:361-362).
-template <class C, class S>
-__device__ __forceinline__ C dx_from_N(const Ops<C> &o, const S *nb, long pitch, int Mx, int ix, int iy)
+// grid.hpp:361-362). get(r) returns the neighbour's value at row r of this column.
+template <class C, class G>
+__device__ __forceinline__ C dxN(const Ops<C> &o, int Mx, int ix, G get)
 {
     C v = C(0);
     if (ix < 3) {
 #pragma unroll
-        for (int w = 0; w < 5; w++) v = add(v, mul(ld<C>(nb, (long)w * pitch + iy), o.dnL[ix][w]));
+        for (int w = 0; w < 5; w++) v = add(v, mul(get(w), o.dnL[ix][w]));
     } else if (ix >= Mx - 3) {
         const int r = ix - (Mx - 3);
 #pragma unroll
-        for (int w = 0; w < 5; w++) v = add(v, mul(ld<C>(nb, (long)(Mx - 4 + w) * pitch + iy), o.dnR[r][w]));
+        for (int w = 0; w < 5; w++) v = add(v, mul(get(Mx - 4 + w), o.dnR[r][w]));
     } else {
 #pragma unroll
-        for (int w = 0; w < 4; w++) v = add(v, mul(ld<C>(nb, (long)(ix - 1 + w) * pitch + iy), o.st[w]));
+        for (int w = 0; w < 4; w++) v = add(v, mul(get(ix - 1 + w), o.st[w]));
     }
     return v;
 }
 
-// derivative along x of an N-type-x grid (rows 0..Mx) from its M-type neighbour with rows
+// derivative along x of an N-type-x row ix (rows 0..Mx) from its M-type neighbour with rows
 // 0..Mx-1: DM closures on 4 rows at each end, interior shifts {-2,-1,0,1}.
-template <class C, class S>
-__device__ __forceinline__ C dx_from_M(const Ops<C> &o, const S *nb, long pitch, int Mx, int ix, int iy)
+template <class C, class G>
+__device__ __forceinline__ C dxM(const Ops<C> &o, int Mx, int ix, G get)
 {
     C v = C(0);
     if (ix < 4) {
 #pragma unroll
-        for (int w = 0; w < 5; w++) v = add(v, mul(ld<C>(nb, (long)w * pitch + iy), o.dmL[ix][w]));
+        for (int w = 0; w < 5; w++) v = add(v, mul(get(w), o.dmL[ix][w]));
     } else if (ix >= Mx - 3) {
         const int r = ix - (Mx - 3);
 #pragma unroll
-        for (int w = 0; w < 5; w++) v = add(v, mul(ld<C>(nb, (long)(Mx - 5 + w) * pitch + iy), o.dmR[r][w]));
+        for (int w = 0; w < 5; w++) v = add(v, mul(get(Mx - 5 + w), o.dmR[r][w]));
     } else {
 #pragma unroll
-        for (int w = 0; w < 4; w++) v = add(v, mul(ld<C>(nb, (long)(ix - 2 + w) * pitch + iy), o.st[w]));
+        for (int w = 0; w < 4; w++) v = add(v, mul(get(ix - 2 + w), o.st[w]));
     }
     return v;
+}
+
+template <class C, class S>
+__device__ __forceinline__ C dx_from_N(const Ops<C> &o, const S *nb, long pitch, int Mx, int ix, int iy)
+{
+    return dxN<C>(o, Mx, ix, [&](int r) { return ld<C>(nb, (long)r * pitch + iy); });
+}
+
+template <class C, class S>
+__device__ __forceinline__ C dx_from_M(const Ops<C> &o, const S *nb, long pitch, int Mx, int ix, int iy)
+{
+    return dxM<C>(o, Mx, ix, [&](int r) { return ld<C>(nb, (long)r * pitch + iy); });
 }
 
 // periodic x derivative (single-core acoustic tree): an N-type row reads M-type rows ix-2..ix+1
