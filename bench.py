@@ -16,6 +16,11 @@ stepping, trace and energy readback inside the timed region); `roofline` = the d
 algorithmic bytes per launch over its CUDA-event duration against the measured HBM copy
 bandwidth; `cpu_baseline` = the reference's own CPU solver (oracle/_ref) on a bounded sample.
 `--impl reference` times only the reference's CPU solver on the host cores.
+
+`--workload mixed` measures the mixed-precision configuration instead: elastic 8192 x 8192,
+seeded Gaussian-random-field medium, 2000 steps, every storage variant (FP64, FP32, BF16 and
+FP16, plain and split) device-timed, with the relative L2 / Linf field error and the trace error
+of each against the FP64 run of the same scheme.
 """
 from __future__ import annotations
 
@@ -346,6 +351,96 @@ def run_ours(args, dist: Dist):
     dist.finish()
 
 
+# ---------------------------------------------------------------- mixed-precision workload
+MIX_N = 8192
+MIX_CORR = 32.0        # correlation length of the medium, cells
+MIX_SEED = 20261203 + 3
+
+
+def grf_model(n: int, seed: int):
+    """Padded (n+2)^2 node model: vp a Gaussian random field (white noise filtered by a Gaussian
+    whose autocorrelation exp(-r^2 / (2 L^2)) has L = MIX_CORR cells), normalised to mean 3.0
+    and standard deviation 0.3; vs = vp / sqrt(3); rho = 2.0."""
+    import torch
+    m = n + 2
+    w = torch.from_numpy(np.random.default_rng(seed).standard_normal((m, m))).cuda()
+    k = torch.fft.fftfreq(m, device="cuda", dtype=torch.float64)
+    sigma = MIX_CORR / np.sqrt(2.0)   # kernel width: g * g has variance 2 sigma^2 = L^2
+    g = torch.exp(-2 * np.pi ** 2 * sigma ** 2 * (k[:, None] ** 2 + k[None, :] ** 2))
+    f = torch.fft.ifft2(torch.fft.fft2(w) * g).real
+    f = (f - f.mean()) / f.std()
+    vp = (3.0 + 0.3 * f).cpu().numpy()
+    del w, g, f
+    torch.cuda.empty_cache()
+    return np.full_like(vp, 2.0), vp, vp / np.sqrt(3.0)
+
+
+def run_mixed(args):
+    import torch
+    tw = load_twave()
+    torch.cuda.set_device(0)
+    n, K = MIX_N, args.steps
+    rho, vp, vs = grf_model(n, MIX_SEED)
+    dx = 1.0 / DEN_DX
+    dt = CFL * dx / (np.sqrt(2.0) * vp.max())
+    # 64 receivers on the NM grid along a row 160 cells from the source, within reach in 2000 steps
+    rx, ry = np.full(64, n // 2 - 160), n // 2 - 320 + 10 * np.arange(64)
+    variants = [("f64", "00", 120), ("f32", "00", 60), ("bf16", "00", 40), ("bf16", "split", 60),
+                ("fp16", "00", 40), ("fp16", "split", 60)]
+    peak, peak_note = measured_peaks()
+    keys = [(tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)]
+    ref = None
+    out = []
+    for prec, cpst, bpu in variants:
+        s = tw.Solver(n, n, 1, DEN_DX, dt, physics=tw.ELASTIC, precision=prec, cpst=cpst, central_f=F0,
+                      time_delay=DELAY, max_steps=args.warmup + K, energy=False)
+        s.set_material_model(rho, vp, vs)
+        s.set_source(tw.MM, n // 2, n // 2)
+        s.add_receivers(tw.NM, rx, ry)
+        stream = torch.cuda.ExternalStream(s.stream())
+        # warm-up on a copy of the run: reset afterwards so every variant steps K from rest
+        s.run(args.warmup)
+        s.reset()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.step(K)
+        e1.record(stream)
+        e1.synchronize()
+        s.sync()
+        ms = e0.elapsed_time(e1)
+        fields = [s.read_field(g, f) for g, f in keys]
+        traces = s.read_receivers()
+        s.close()
+        gpts = n * n * K / (ms / 1e3) / 1e9
+        row = {"precision": prec, "compensation": cpst, "gpts": gpts, "ms_per_step": ms / K,
+               "bytes_per_update": bpu, "hbm_frac": gpts * bpu / peak}
+        if ref is None:
+            ref = (fields, traces)
+            row.update({"l2_err": 0.0, "linf_err": 0.0, "trace_err": 0.0})
+        else:
+            num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(fields, ref[0]))
+            den = sum(float(np.sum(b ** 2)) for b in ref[0])
+            linf = max(float(np.abs(a - b).max()) for a, b in zip(fields, ref[0]))
+            scale = max(float(np.abs(b).max()) for b in ref[0])
+            row.update({"l2_err": (num / den) ** 0.5, "linf_err": linf / scale,
+                        "trace_err": float(np.linalg.norm(traces - ref[1]) / np.linalg.norm(ref[1]))})
+        del fields, traces
+        out.append(row)
+    best = max((r for r in out if r["precision"] in ("bf16", "fp16") and r["l2_err"] <= 1e-4),
+               key=lambda r: r["gpts"], default=None)
+    line = {"metric": METRIC, "value": best["gpts"] if best else None, "unit": UNIT, "n_gpus": 1, "steps": K,
+            "warmup": args.warmup, "higher_is_better": True, "dtype": f"{best['precision']} storage, f32 arithmetic"
+            if best else None, "data": "synthetic",
+            "config": {"workload": f"mixed precision: elastic {n}x{n}, Gaussian-random-field medium (vp mean 3.0, "
+                                   f"std 0.3, correlation length {MIX_CORR:g} cells, vs = vp/sqrt(3), rho = 2.0), "
+                                   f"CFL 0.4, Ricker f0=15 at the centre, 64 receivers on an NM row 160 cells from it",
+                       "errors": "relative L2 over all five fields, Linf / max |FP64|, trace L2, vs the FP64 run",
+                       "l2": f"inputs far larger than L2, no flush", "peak": f"{peak} GB/s {peak_note}"},
+            "variants": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -354,12 +449,17 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", choices=["elastic2048", "mixed"], default="elastic2048")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
     dist = Dist()
     if args.impl == "reference":
         run_reference_arm(args, dist)
+        return
+    if args.workload == "mixed":
+        if dist.rank == 0:
+            run_mixed(args)
         return
     run_ours(args, dist)
 

@@ -52,12 +52,19 @@ enum tw_physics { TW_ELASTIC = 0, TW_ACOUSTIC = 1 };
  * y is always periodic, as in the reference (grid_drvt.tpp:1-3). */
 enum tw_bc { TW_BC_SAT_FREE = 0, TW_BC_PERIODIC = 1 };
 /* storage type of the fields; FP64/FP32 compute in the storage type (namespace_type.cuh:16-22);
- * BF16/FP16 store 16-bit fields and compute in FP32 */
+ * BF16/FP16 (elastic) store 16-bit fields, compute in FP32 and keep FP32 coefficients. The
+ * reference's 16-bit mode (PRCSFLAG 16) also computes in 16 bits; this one rounds only what it
+ * stores. */
 enum tw_precision { TW_FP64 = 0, TW_FP32 = 1, TW_BF16 = 2, TW_FP16 = 3 };
 /* time-update compensation, grid.hpp:550-566 / grid_update.tpp:1-127 ("N" = flops used for the
- * lost bits, "C" = separate array, "R" = the right-hand-side array holds them) */
+ * lost bits, "C" = separate array, "R" = the right-hand-side array holds them). Codes 1-6 need
+ * FP64/FP32 storage. TW_CPST_SPLIT (no reference counterpart; BF16/FP16 only) is a compensated
+ * (Kahan-style) two-term storage: each value is kept as hi + lo, lo = the rounding error of
+ * hi, both 16-bit; the stencil, the energy and the receivers read the FP32 sum hi + lo, and the
+ * update rounds the new FP32 value to hi and its remainder to lo. tw_read_field returns hi + lo,
+ * tw_read_resid lo. */
 enum tw_cpst { TW_CPST_00 = 0, TW_CPST_M3C = 1, TW_CPST_M3R = 2, TW_CPST_3C = 3,
-               TW_CPST_3R = 4, TW_CPST_6C = 5, TW_CPST_6R = 6 };
+               TW_CPST_3R = 4, TW_CPST_6C = 5, TW_CPST_6R = 6, TW_CPST_SPLIT = 7 };
 enum tw_grid { TW_NN = 0, TW_MN = 1, TW_NM = 2, TW_MM = 3 };
 
 typedef struct {

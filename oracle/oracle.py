@@ -20,7 +20,8 @@ except ImportError:  # loaded by path
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_build", "libtwave_oracle.so")
-CPST_INDEX = {"00": 0, "-3C": 1, "-3R": 2, "3C": 3, "3R": 4, "6C": 5, "6R": 6}
+CPST_INDEX = {"00": 0, "-3C": 1, "-3R": 2, "3C": 3, "3R": 4, "6C": 5, "6R": 6, "split": 7}
+STORE16 = {"bf16": 2, "fp16": 3}   # mixed precision: 16-bit storage, FP32 arithmetic
 GRID_INDEX = {("N", "N"): 0, ("M", "N"): 1, ("N", "M"): 2, ("M", "M"): 3}
 
 _lib = None
@@ -107,9 +108,11 @@ def elastic_run(case: refrun.ElasticCase, precision: str = "f64", fields0=None, 
                 coefs=None, weights=None) -> refrun.ElasticResult:
     """Run the restated elastic stepper. fields0/resid0: optional initial state (5 arrays,
     reference sizes). coefs/weights: optional overrides of the stored coefficients
-    (keys NN_mu, MN_irho, NM_irho, MM_lambda, MM_2mu) and energy weights."""
+    (keys NN_mu, MN_irho, NM_irho, MM_lambda, MM_2mu) and energy weights. precision "bf16" /
+    "fp16" runs the mixed-precision restatement (FP32 arithmetic and coefficients, 16-bit field
+    storage; case.cpst "00" or "split")."""
     T = np.float64 if precision == "f64" else np.float32
-    stored, w = elastic_coefficients(case, precision)
+    stored, w = elastic_coefficients(case, "f64" if precision == "f64" else "f32")
     if coefs is not None:
         stored.update({k: np.ascontiguousarray(v, T) for k, v in coefs.items()})
     if weights is not None:
@@ -137,7 +140,10 @@ def elastic_run(case: refrun.ElasticCase, precision: str = "f64", fields0=None, 
     traces = np.zeros((n, 2, Nt))
     E_k, E_p0, E_p1 = np.zeros(Nt), np.zeros(Nt), np.zeros(Nt)
     FA = C.c_void_p * 5
-    fn = lib().two_elastic_run_f64 if precision == "f64" else lib().two_elastic_run_f32
+    if precision in STORE16:
+        fn = lambda cfgp, *rest: lib().two_elastic_run_mixed(cfgp, STORE16[precision], *rest)
+    else:
+        fn = lib().two_elastic_run_f64 if precision == "f64" else lib().two_elastic_run_f32
     rc = fn(C.byref(cfg), _p(stored["NN_mu"]), _p(stored["MN_irho"]), _p(stored["NM_irho"]),
             _p(stored["MM_lambda"]), _p(stored["MM_2mu"]), _p(w["NN"]), _p(w["MN"]), _p(w["NM"]),
             _p(w["MM_P1"]), _p(w["MM_P2"]), FA(*[f.ctypes.data for f in fields]),

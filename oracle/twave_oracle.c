@@ -95,6 +95,24 @@ int two_material_map(int Mx, int My, int num_dx, int den_dx, int Mx_prmt, int My
     return rc ? -1 : 0;
 }
 
+/* Storage rounding of the mixed-precision mode (no counterpart in the reference, whose 16-bit
+ * build computes in 16 bits): 0 none, 2 BF16, 3 FP16, each round-to-nearest-even from FP32,
+ * as cuda_bf16.h's __float2bfloat16_rn and cuda_fp16.h's __float2half_rn round. Set only for
+ * the duration of two_elastic_run_mixed. */
+static int oracle_store16 = 0;
+
+static float oracle_round16(float x)
+{
+    if (oracle_store16 == 3) return (float)(_Float16)x;
+    if (oracle_store16 == 2) {
+        unsigned u;
+        memcpy(&u, &x, 4);
+        if ((u & 0x7f800000u) != 0x7f800000u) u = (u + 0x7fffu + ((u >> 16) & 1u)) & 0xffff0000u;
+        memcpy(&x, &u, 4);
+    }
+    return x;
+}
+
 #define T double
 #define SFX _f64
 #include "twave_oracle_body.inc"
@@ -106,3 +124,18 @@ int two_material_map(int Mx, int My, int num_dx, int den_dx, int Mx_prmt, int My
 #include "twave_oracle_body.inc"
 #undef T
 #undef SFX
+
+int two_elastic_run_mixed(const two_elastic_cfg *cfg, int store16, const float *NN_mu, const float *MN_irho,
+                          const float *NM_irho, const float *MM_lambda, const float *MM_2mu, const double *w_NN,
+                          const double *w_MN, const double *w_NM, const double *w_MM1, const double *w_MM2,
+                          float *const fields[5], float *const resid[5], double *traces, double *E_k,
+                          double *E_p0, double *E_p1)
+{
+    if (store16 != 2 && store16 != 3) return -1;
+    if (cfg->cpst != 0 && cfg->cpst != 7) return -1;
+    oracle_store16 = store16;
+    const int rc = two_elastic_run_f32(cfg, NN_mu, MN_irho, NM_irho, MM_lambda, MM_2mu, w_NN, w_MN, w_NM, w_MM1,
+                                       w_MM2, fields, resid, traces, E_k, E_p0, E_p1);
+    oracle_store16 = 0;
+    return rc;
+}

@@ -66,6 +66,16 @@ int two_elastic_run_f32(const two_elastic_cfg *cfg, const float *NN_mu, const fl
                         const double *w_MM1, const double *w_MM2, float *const fields[5],
                         float *const resid[5], double *traces, double *E_k, double *E_p0, double *E_p1);
 
+/* Mixed precision (no counterpart in the reference): the FP32 stepper above with every new
+ * field value rounded to storage: store16 2 = BF16, 3 = FP16; cfg->cpst 0 (plain) or 7 (split:
+ * each value kept as hi + lo, lo = the rounded rest, reads take their FP32 sum). fields hold the
+ * values the stepper reads (hi, or hi + lo); under code 7 resid receives lo. */
+int two_elastic_run_mixed(const two_elastic_cfg *cfg, int store16, const float *NN_mu, const float *MN_irho,
+                          const float *NM_irho, const float *MM_lambda, const float *MM_2mu, const double *w_NN,
+                          const double *w_MN, const double *w_NM, const double *w_MM1, const double *w_MM2,
+                          float *const fields[5], float *const resid[5], double *traces, double *E_k,
+                          double *E_p0, double *E_p1);
+
 /* singlecore/ acoustic stepper, periodic on all sides (namespaces.hpp:566-778,
  * cpu_acoustic.cpp:231-345). Grids: Vx (Nx+1)xNy, Vy Nx x(Ny+1), P Nx x Ny.
  * coef: 1/rho on Vx and Vy, kappa on P. cpst: 0 ('0'), 3 ('3'), 6 ('6').

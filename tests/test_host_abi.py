@@ -66,6 +66,10 @@ def _desc(tw, **kw):
     (dict(physics=5), -1), (dict(cpst=9), -1), (dict(source_scaling=0.0), -1),
     (dict(physics=0, bc_x=1), -10),                 # elastic needs the SAT x boundaries
     (dict(physics=1, bc_x=1, cpst=5), -10),         # the single-core tree has no 'C' compensation
+    (dict(precision=4), -1),
+    (dict(precision=2, cpst=4), -10),               # 16-bit storage: plain or split only
+    (dict(precision=1, cpst=7), -10),               # the split pair needs 16-bit storage
+    (dict(physics=1, precision=3), -10),            # 16-bit storage is elastic only
 ])
 def test_create_rejects_bad_descriptors_before_touching_the_device(tw, kw, code):
     h = C.c_void_p()

@@ -1,0 +1,85 @@
+"""Mixed precision on the GPU: BF16 / FP16 field storage with FP32 arithmetic.
+
+Two codes: "00" stores each new value rounded to 16 bits; "split" stores the pair hi + lo (lo =
+the rounded remainder) and every read takes their FP32 sum, a compensated (Kahan-style) storage
+of about 16 (BF16) or 22 (FP16) significant bits. Fields and traces must equal the oracle's
+mixed-precision restatement bit for bit (energies: FP64 sums, relative 1e-12), and the split
+code must stay close to an FP64 run of the same scheme: within 1e-4 (relative L2) with FP16
+storage, 1e-3 with BF16.
+"""
+import numpy as np
+import pytest
+
+from cases import elastic_case, product_elastic
+from oracle import oracle as orc
+
+pytestmark = pytest.mark.gpu
+E_RTOL = 1e-12
+KEYS = ("NN", "MN", "NM", "MM0", "MM1")
+
+
+def round16(a, prec):
+    import torch
+    t = torch.tensor(np.asarray(a, np.float32))
+    return t.to(torch.bfloat16 if prec == "bf16" else torch.float16).to(torch.float32).double().numpy()
+
+
+def _state(Mx, My, seed, prec, cpst, scale=1e-2):
+    rng = np.random.default_rng(seed)
+    shapes = [(Mx + 1, My + 1), (Mx, My + 1), (Mx + 1, My), (Mx, My), (Mx, My)]
+    f = [(rng.standard_normal(s) * scale).astype(np.float32).astype(np.float64) for s in shapes]
+    # plain 16-bit storage holds 16-bit values; the split pair is formed from the FP32 value
+    return [round16(a, prec) for a in f] if cpst == "00" else f
+
+
+def energy_close(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return np.abs(a - b).max() <= E_RTOL * max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("cpst", ["00", "split"])
+@pytest.mark.parametrize("prec", ["bf16", "fp16"])
+@pytest.mark.parametrize("Mx,My,Nt", [(24, 40, 3), (37, 45, 3), (8, 4, 3), (70, 500, 6)])
+def test_mixed_matches_oracle(cpst, prec, Mx, My, Nt):
+    den = max(Mx, My)
+    rcvs = [("N", "M", 2, den, 2 * (My - 1) + 1, 2 * den), ("M", "M", 2 * (Mx // 2) + 1, 2 * den, 2 * (My // 2) + 1, 2 * den),
+            ("N", "N", Mx, den, My, den), ("M", "N", 2 * (Mx - 1) + 1, 2 * den, 0, 1)]
+    case = elastic_case(Mx, My, seed=Mx + My, cpst=cpst, Nt=Nt, rcvs=rcvs)
+    f0 = _state(Mx, My, 3, prec, cpst)
+    want = orc.elastic_run(case, prec, fields0=f0)
+    got = product_elastic(case, prec, fields0=f0)
+    for k, v in got["fields"].items():
+        assert np.array_equal(v, want.fields[k]), k
+    if cpst == "split":
+        for k, v in zip(KEYS, got["resid"]):
+            assert np.array_equal(v, want.resid[k]), ("lo", k)
+    assert np.array_equal(got["traces"], want.traces)
+    for k in ("E_k", "E_p0", "E_p1"):
+        assert energy_close(got[k], getattr(want, k)), k
+
+
+def test_split_storage_error_against_fp64():
+    """A source-driven run from rest on a layered medium (160 x 160, 1200 steps): relative L2
+    error of all fields together and of the traces against FP64. FP16 split storage meets 1e-4
+    (measured on a B200: 1.3e-5); BF16 split storage does not (4.8e-4: 16 significant bits) and is
+    held to 1e-3; plain 16-bit storage drifts far more (BF16 0.36, FP16 0.05) and is only checked
+    for sanity."""
+    Mx = My = 160
+    den = 500
+    rcvs = [("N", "M", 8, den, 2 * k + 1, 2 * den) for k in range(4, My, 16)]
+    base = dict(Nt=1200, model="layered", den_dx=den, rcvs=rcvs, time_delay=0.06)
+    ref = product_elastic(elastic_case(Mx, My, seed=9, **base), "f64", energy=False)
+    errs = {}
+    for prec in ("bf16", "fp16"):
+        for cpst in ("00", "split"):
+            got = product_elastic(elastic_case(Mx, My, seed=9, cpst=cpst, **base), prec, energy=False)
+            num = sum(np.sum((got["fields"][k] - ref["fields"][k]) ** 2) for k in KEYS)
+            den_ = sum(np.sum(ref["fields"][k] ** 2) for k in KEYS)
+            tr = np.linalg.norm(got["traces"] - ref["traces"]) / np.linalg.norm(ref["traces"])
+            errs[(prec, cpst)] = (np.sqrt(num / den_), tr)
+    print({k: f"{v[0]:.2e}/{v[1]:.2e}" for k, v in errs.items()})
+    bound = {"fp16": 1e-4, "bf16": 1e-3}
+    for prec in ("bf16", "fp16"):
+        assert errs[(prec, "split")][0] <= bound[prec] and errs[(prec, "split")][1] <= bound[prec], errs
+        assert errs[(prec, "00")][0] < 1.0, errs
+    assert errs[("fp16", "split")][0] < errs[("bf16", "split")][0]

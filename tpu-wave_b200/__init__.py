@@ -23,7 +23,7 @@ HEADER = os.path.join(HERE, "..", "include", "twave.h")
 ELASTIC, ACOUSTIC = 0, 1
 SAT_FREE, PERIODIC = 0, 1
 FP64, FP32, BF16, FP16 = 0, 1, 2, 3
-CPST = {"00": 0, "-3C": 1, "-3R": 2, "3C": 3, "3R": 4, "6C": 5, "6R": 6}
+CPST = {"00": 0, "-3C": 1, "-3R": 2, "3C": 3, "3R": 4, "6C": 5, "6R": 6, "split": 7}
 NN, MN, NM, MM = 0, 1, 2, 3
 GRID = {("N", "N"): NN, ("M", "N"): MN, ("N", "M"): NM, ("M", "M"): MM}
 PRECISION = {"f64": FP64, "f32": FP32, "bf16": BF16, "fp16": FP16}

@@ -29,17 +29,20 @@ __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 
 // one time update of a field value s with right-hand side r and compensation c, following
 // grid_update.tpp:1-127 (codes of enum tw_cpst). keep_r: the code keeps its residual in R;
-// keep_c: in the separate C array.
+// keep_c: in the separate C array. split (code 7, 16-bit storage only): every value is stored
+// as a pair hi + lo of the storage type, lo = the rounding error of hi, and every read takes
+// their sum in the compute type; the update itself is a plain s + r.
 template <int CPST> struct Cpst {
     static constexpr bool keep_r = (CPST == 2 || CPST == 4 || CPST == 6);
     static constexpr bool keep_c = (CPST == 1 || CPST == 3 || CPST == 5);
-    static constexpr bool any = keep_r || keep_c;
+    static constexpr bool split = (CPST == 7);
+    static constexpr bool any = keep_r || keep_c || split;
 };
 
 template <int CPST, class C>
 __device__ __forceinline__ void time_update(C &s, C &r, C &c)
 {
-    if constexpr (CPST == 0) {
+    if constexpr (CPST == 0 || CPST == 7) {
         s = add(s, r);
     } else if constexpr (CPST == 1 || CPST == 3) {   // update_3C / update_3C_fast2sum
         const C y = add(r, c);
@@ -61,6 +64,20 @@ __device__ __forceinline__ void time_update(C &s, C &r, C &c)
         const C db = sub(b, pb);
         s = t;
         if constexpr (CPST == 5) c = add(da, db); else r = add(da, db);
+    }
+}
+
+// a new value as the storage keeps it: rounded to S (a pair hi + lo under the split code);
+// identity when storage and compute types agree
+template <class S, class C, int CPST>
+__device__ __forceinline__ C quant(C v)
+{
+    if constexpr (sizeof(S) == sizeof(C)) {
+        return v;
+    } else {
+        const C hi = to_c<C>(to_s<S>(v));
+        if constexpr (Cpst<CPST>::split) return add(hi, to_c<C>(to_s<S>(sub(v, hi))));
+        return hi;
     }
 }
 

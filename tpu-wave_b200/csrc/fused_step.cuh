@@ -18,6 +18,10 @@
 //
 // Per point the arithmetic and the order of the right-hand-side terms are those of
 // step_kernels.cu (hence of the reference): results are bit-identical.
+//
+// The templates are instantiated per storage type in fused_f64.cu, fused_f32.cu, fused_bf16.cu
+// and fused_f16.cu (separate translation units, compiled in parallel).
+#pragma once
 #include <type_traits>
 
 #include "kernels.h"
@@ -43,6 +47,8 @@ struct P2 {
 template <class S> struct Vec2;
 template <> struct Vec2<float> { using T = float2; };
 template <> struct Vec2<double> { using T = double2; };
+template <> struct Vec2<__nv_bfloat16> { using T = __nv_bfloat162; };
+template <> struct Vec2<__half> { using T = __half2; };
 
 // a pair of values at physical columns pa, pb of one row (one vector load when they are
 // adjacent and aligned)
@@ -127,7 +133,7 @@ struct Row {   // global values one interior iteration consumes
 template <class S, class C, int CPST, bool ENERGY, bool EDGE>
 __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int it, int rcv_b, int rcv_e, EAcc &E)
 {
-    constexpr bool KR = Cpst<CPST>::keep_r, KC = Cpst<CPST>::keep_c;
+    constexpr bool KR = Cpst<CPST>::keep_r, KC = Cpst<CPST>::keep_c, SPLIT = Cpst<CPST>::split;
     const int lane = threadIdx.x & 31;
     const int Mx = a.Mx, My = a.My, pitch = (int)a.pitch;
     const int y0 = wstrip * FS_WARP_CORE;
@@ -161,12 +167,22 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
         }
         return ldg2_any<T>(row, pa, pb);
     };
+    // a field value pair as the stencil reads it (hi + lo under the split code)
+    auto ld2f = [&](int f, int r, int pa, int pb) -> P2<C> {
+        P2<C> v = ld2(rowp(a.in[f], r), pa, pb);
+        if constexpr (SPLIT) {
+            const P2<C> l = ld2(rowp(a.rin[f], r), pa, pb);
+            v.a = add(v.a, l.a);
+            v.b = add(v.b, l.b);
+        }
+        return v;
+    };
     auto fetch = [&](int j, Row<C> &in) {
-        in.nn = ld2(rowp(a.in[F_NN], j + 2), pN0, pN1);
-        in.mm0 = ld2(rowp(a.in[F_MM0], j + 1), pM0, pM1);
-        in.mm1 = ld2(rowp(a.in[F_MM1], j), pM0, pM1);
-        in.vmn = ld2(rowp(a.in[F_MN], j), pN0, pN1);
-        in.vnm = ld2(rowp(a.in[F_NM], j), pM0, pM1);
+        in.nn = ld2f(F_NN, j + 2, pN0, pN1);
+        in.mm0 = ld2f(F_MM0, j + 1, pM0, pM1);
+        in.mm1 = ld2f(F_MM1, j, pM0, pM1);
+        in.vmn = ld2f(F_MN, j, pN0, pN1);
+        in.vnm = ld2f(F_NM, j, pM0, pM1);
         in.pmn = ldg2(a.coef[F_MN] + j * pitch, pN0, pN1);
         in.pnm = ldg2(a.coef[F_NM] + j * pitch, pM0, pM1);
         if (KR || KC) {
@@ -220,23 +236,29 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
         }
     };
     // store the owned values of a pair (owned columns are physical: c0 >= 0 for core lanes)
+    // the second array holds the residual (R, C codes) or the low part lo = s - hi (split)
+    constexpr bool TWO = Cpst<CPST>::any;
     auto put = [&](int f, int row, const P2<C> &s, const P2<C> &r, const P2<C> &cc, bool o0, bool o1) {
+        using V2 = typename Vec2<S>::T;
         S *o = a.out[f] + row * pitch;
-        S *ro = KR || KC ? a.rout[f] + row * pitch : nullptr;
+        S *ro = TWO ? a.rout[f] + row * pitch : nullptr;
         if ((o0 && !finite(s.a)) || (o1 && !finite(s.b))) atomicOr(a.flags, FLAG_NONFINITE);
+        const S h0 = to_s<S>(s.a), h1 = to_s<S>(s.b);
+        S l0{}, l1{};
+        if constexpr (SPLIT) { l0 = to_s<S>(sub(s.a, to_c<C>(h0))); l1 = to_s<S>(sub(s.b, to_c<C>(h1))); }
+        if constexpr (KR) { l0 = to_s<S>(r.a); l1 = to_s<S>(r.b); }
+        if constexpr (KC) { l0 = to_s<S>(cc.a); l1 = to_s<S>(cc.b); }
         if (!EDGE) {
             if (o0) {
-                *reinterpret_cast<typename Vec2<S>::T *>(o + c0) = {to_s<S>(s.a), to_s<S>(s.b)};
-                if (KR) *reinterpret_cast<typename Vec2<S>::T *>(ro + c0) = {to_s<S>(r.a), to_s<S>(r.b)};
-                if (KC) *reinterpret_cast<typename Vec2<S>::T *>(ro + c0) = {to_s<S>(cc.a), to_s<S>(cc.b)};
+                *reinterpret_cast<V2 *>(o + c0) = V2{h0, h1};
+                if (TWO) *reinterpret_cast<V2 *>(ro + c0) = V2{l0, l1};
             }
         } else if (o0 && o1 && !(c0 & 1)) {
-            *reinterpret_cast<typename Vec2<S>::T *>(o + c0) = {to_s<S>(s.a), to_s<S>(s.b)};
-            if (KR) *reinterpret_cast<typename Vec2<S>::T *>(ro + c0) = {to_s<S>(r.a), to_s<S>(r.b)};
-            if (KC) *reinterpret_cast<typename Vec2<S>::T *>(ro + c0) = {to_s<S>(cc.a), to_s<S>(cc.b)};
+            *reinterpret_cast<V2 *>(o + c0) = V2{h0, h1};
+            if (TWO) *reinterpret_cast<V2 *>(ro + c0) = V2{l0, l1};
         } else {
-            if (o0) { o[c0] = to_s<S>(s.a); if (KR) ro[c0] = to_s<S>(r.a); if (KC) ro[c0] = to_s<S>(cc.a); }
-            if (o1) { o[c1] = to_s<S>(s.b); if (KR) ro[c1] = to_s<S>(r.b); if (KC) ro[c1] = to_s<S>(cc.b); }
+            if (o0) { o[c0] = h0; if (TWO) ro[c0] = l0; }
+            if (o1) { o[c1] = h1; if (TWO) ro[c1] = l1; }
         }
         if (nr > 0 || rmany) {
             if (o0) record(f, row, c0, (double)s.a);
@@ -251,16 +273,21 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
         }
     };
     auto pair0 = [&](bool keep, const P2<C> &v) { return P2<C>{keep ? v.a : C(0), keep ? v.b : C(0)}; };
+    // a new value as storage keeps it (16-bit storage rounds here, before any later use)
+    auto q2 = [&](P2<C> &v) {
+        v.a = quant<S, C, CPST>(v.a);
+        v.b = quant<S, C, CPST>(v.b);
+    };
 
     // windows: NN rows j-2..j+2, MM0 rows j-2..j+1, MM1 rows j-2..j, MN rows j-4..j, NM rows j-3..j
     P2<C> NNw[5], M0w[4], M1w[3], MNw[5], NMw[4];
     const int jb = x0 - 2, je = x1 + 1;
 #pragma unroll
-    for (int q = 0; q < 4; q++) NNw[q] = ld2(rowp(a.in[F_NN], jb - 2 + q), pN0, pN1);
+    for (int q = 0; q < 4; q++) NNw[q] = ld2f(F_NN, jb - 2 + q, pN0, pN1);
 #pragma unroll
-    for (int q = 0; q < 3; q++) M0w[q] = ld2(rowp(a.in[F_MM0], jb - 2 + q), pM0, pM1);
+    for (int q = 0; q < 3; q++) M0w[q] = ld2f(F_MM0, jb - 2 + q, pM0, pM1);
 #pragma unroll
-    for (int q = 0; q < 2; q++) M1w[q] = ld2(rowp(a.in[F_MM1], jb - 2 + q), pM0, pM1);
+    for (int q = 0; q < 2; q++) M1w[q] = ld2f(F_MM1, jb - 2 + q, pM0, pM1);
     Row<C> cur, nxt;
     fetch(jb, nxt);
     for (int j = jb; j <= je; j++) {
@@ -290,6 +317,7 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
             time_update<CPST>(s.a, r.a, cc.a);
             time_update<CPST>(s.b, r.b, cc.b);
             src_add(G_MN, j, s, pN0, pN1);
+            q2(s);
             MNw[4] = s;
             if (ownV) {
                 put(F_MN, j, s, r, cc, oN0, oN1);
@@ -304,16 +332,21 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
             lanes(NNw[2], p, n);
             P2<C> vy = dyMfromN(a.op, NNw[2], p, n);
             if (seam0 || seam1) {
-                const S *row = rowp(a.in[F_NN], j);
+                const S *row = rowp(a.in[F_NN], j), *lrow = SPLIT ? rowp(a.rin[F_NN], j) : nullptr;
+                auto nnv = [&](int col) {
+                    C v = to_c<C>(row[col]);
+                    if constexpr (SPLIT) v = add(v, to_c<C>(lrow[col]));
+                    return v;
+                };
                 if (seam0) {
                     vy.a = C(0);
 #pragma unroll
-                    for (int w = 0; w < 4; w++) vy.a = add(vy.a, mul(to_c<C>(row[nread(pM0 - 1 + w, My)]), a.op.st[w]));
+                    for (int w = 0; w < 4; w++) vy.a = add(vy.a, mul(nnv(nread(pM0 - 1 + w, My)), a.op.st[w]));
                 }
                 if (seam1) {
                     vy.b = C(0);
 #pragma unroll
-                    for (int w = 0; w < 4; w++) vy.b = add(vy.b, mul(to_c<C>(row[nread(pM1 - 1 + w, My)]), a.op.st[w]));
+                    for (int w = 0; w < 4; w++) vy.b = add(vy.b, mul(nnv(nread(pM1 - 1 + w, My)), a.op.st[w]));
                 }
             }
             P2<C> vx{C(0), C(0)};
@@ -331,6 +364,7 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
             time_update<CPST>(s.a, r.a, cc.a);
             time_update<CPST>(s.b, r.b, cc.b);
             src_add(G_NM, j, s, pM0, pM1);
+            q2(s);
             NMw[3] = s;
             if (ownV) {
                 put(F_NM, j, s, r, cc, oM0, oM1);
@@ -366,6 +400,7 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
                     time_update<CPST>(s.a, r.a, cc.a);
                     time_update<CPST>(s.b, r.b, cc.b);
                     src_add(G_NN, i, s, c0, c1);
+                    q2(s);
                     put(F_NN, i, s, r, cc, oN0, oN1);
                     if (ENERGY) {
                         if (oN0) {
@@ -402,6 +437,8 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
                     time_update<CPST>(s1.b, r1.b, k1.b);
                     src_add(G_MM, i, s0, c0, c1);
                     src_add(G_MM, i, s1, c0, c1);
+                    q2(s0);
+                    q2(s1);
                     put(F_MM0, i, s0, r0, k0, oM0, oM1);
                     put(F_MM1, i, s1, r1, k1, oM0, oM1);
                     if (ENERGY) {
@@ -444,7 +481,7 @@ template <class S, class C, int CPST, bool ENERGY>
 __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int it, int rcv_b, int rcv_e, C *tile,
                              EAcc &E)
 {
-    constexpr bool KR = Cpst<CPST>::keep_r, KC = Cpst<CPST>::keep_c;
+    constexpr bool KR = Cpst<CPST>::keep_r, KC = Cpst<CPST>::keep_c, SPLIT = Cpst<CPST>::split;
     constexpr int NT = FS_BND_W;                 // tile row length: the strip's logical columns
     constexpr int RG = FS_BND_THREADS / FS_BND_W;   // row groups: thread rows t / NT walk rows g, g + RG, ...
     const int t = threadIdx.x % NT, g = threadIdx.x / NT;
@@ -473,10 +510,17 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
     auto put = [&](int f, int row, C s, C r, C cc) {
         if (!finite(s)) atomicOr(a.flags, FLAG_NONFINITE);
         const long o = (long)row * pitch + c;
-        a.out[f][o] = to_s<S>(s);
+        const S h = to_s<S>(s);
+        a.out[f][o] = h;
         if (KR) a.rout[f][o] = to_s<S>(r);
         if (KC) a.rout[f][o] = to_s<S>(cc);
+        if (SPLIT) a.rout[f][o] = to_s<S>(sub(s, to_c<C>(h)));
         if (mine) record(f, row, (double)s);
+    };
+    // a field as the stencil reads it: the stored array, or the pair hi + lo under the split code
+    auto FA = [&](int f) {
+        if constexpr (SPLIT) return HiLo<S>{a.in[f], a.rin[f]};
+        else return a.in[f];
     };
     auto ldr = [&](int f, int row, int col, C &r, C &cc) {
         r = C(0);
@@ -493,15 +537,16 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
                 C r, cc;
                 ldr(F_MN, j, pN, r, cc);
                 const C P = __ldg(a.coef[F_MN] + (long)j * pitch + pN);
-                C v = dx_from_N<C>(a.op, a.in[F_NN], pitch, Mx, j, pN);
+                C v = dx_from_N<C>(a.op, FA(F_NN), pitch, Mx, j, pN);
                 r = add(r, mul(v, P));
-                if (sat_MN<C>(a.op, a.in[F_NN], pitch, Mx, j, pN, v)) r = add(r, mul(v, P));
-                v = dy_periodic<false, C>(a.op, a.in[F_MM1] + (long)j * pitch, My, pN);
+                if (sat_MN<C>(a.op, FA(F_NN), pitch, Mx, j, pN, v)) r = add(r, mul(v, P));
+                v = dy_periodic<false, C>(a.op, FA(F_MM1) + (long)j * pitch, My, pN);
                 r = add(r, mul(v, P));
-                C s = to_c<C>(a.in[F_MN][(long)j * pitch + pN]);
+                C s = ld<C>(FA(F_MN), (long)j * pitch + pN);
                 time_update<CPST>(s, r, cc);
                 if (a.src_grid == G_MN && j == a.src_ix)
                     if (pN == a.src_iy) s = to_s<C>(add((double)s, a.src_inc[it]));
+                s = quant<S, C, CPST>(s);
                 tMN[(j - vr0) * NT + t] = s;
                 if (ownRow && ownN) {
                     put(F_MN, j, s, r, cc);
@@ -512,15 +557,16 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
                 C r, cc;
                 ldr(F_NM, j, pM, r, cc);
                 const C P = __ldg(a.coef[F_NM] + (long)j * pitch + pM);
-                C v = dx_from_M<C>(a.op, a.in[F_MM0], pitch, Mx, j, pM);
+                C v = dx_from_M<C>(a.op, FA(F_MM0), pitch, Mx, j, pM);
                 r = add(r, mul(v, P));
-                if (sat_NM<C>(a.op, a.in[F_MM0], pitch, Mx, j, pM, v)) r = add(r, mul(v, P));
-                v = dy_periodic<true, C>(a.op, a.in[F_NN] + (long)j * pitch, My, pM);
+                if (sat_NM<C>(a.op, FA(F_MM0), pitch, Mx, j, pM, v)) r = add(r, mul(v, P));
+                v = dy_periodic<true, C>(a.op, FA(F_NN) + (long)j * pitch, My, pM);
                 r = add(r, mul(v, P));
-                C s = to_c<C>(a.in[F_NM][(long)j * pitch + pM]);
+                C s = ld<C>(FA(F_NM), (long)j * pitch + pM);
                 time_update<CPST>(s, r, cc);
                 if (a.src_grid == G_NM && j == a.src_ix)
                     if (pM == a.src_iy) s = to_s<C>(add((double)s, a.src_inc[it]));
+                s = quant<S, C, CPST>(s);
                 tNM[(j - vr0) * NT + t] = s;
                 if (ownRow && ownM) {
                     put(F_NM, j, s, r, cc);
@@ -544,11 +590,12 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
 #pragma unroll
                 for (int w = 0; w < 4; w++) v = add(v, mul(tNM[(i - vr0) * NT + t - 2 + w], a.op.st[w]));
                 r = add(r, mul(v, P));
-                const C old = to_c<C>(a.in[F_NN][o]);
+                const C old = ld<C>(FA(F_NN), o);
                 C s = old;
                 time_update<CPST>(s, r, cc);
                 if (a.src_grid == G_NN && i == a.src_ix)
                     if (c == a.src_iy) s = to_s<C>(add((double)s, a.src_inc[it]));
+                s = quant<S, C, CPST>(s);
                 put(F_NN, i, s, r, cc);
                 if (ENERGY) {
                     const double w = __ldg(a.w[F_NN] + o);
@@ -571,7 +618,7 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
                 r0 = add(r0, mul(v, L));
                 r1 = add(r1, mul(v, L));
                 r1 = add(r1, mul(v, M2));
-                const C o0 = to_c<C>(a.in[F_MM0][o]), o1 = to_c<C>(a.in[F_MM1][o]);
+                const C o0 = ld<C>(FA(F_MM0), o), o1 = ld<C>(FA(F_MM1), o);
                 C s0 = o0, s1 = o1;
                 time_update<CPST>(s0, r0, k0);
                 time_update<CPST>(s1, r1, k1);
@@ -579,6 +626,8 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
                     s0 = to_s<C>(add((double)s0, a.src_inc[it]));
                     s1 = to_s<C>(add((double)s1, a.src_inc[it]));
                 }
+                s0 = quant<S, C, CPST>(s0);
+                s1 = quant<S, C, CPST>(s1);
                 put(F_MM0, i, s0, r0, k0);
                 put(F_MM1, i, s1, r1, k1);
                 if (ENERGY) {
@@ -671,13 +720,18 @@ cudaError_t prepare_fused()
 {
     const int smem = (int)fused_smem_bytes<S, C>(FS_SMALL_MX + 1);
     cudaError_t e;
-    if ((e = set_attr<S, C, 0>(smem)) != cudaSuccess) return e;
-    if ((e = set_attr<S, C, 1>(smem)) != cudaSuccess) return e;
-    if ((e = set_attr<S, C, 2>(smem)) != cudaSuccess) return e;
-    if ((e = set_attr<S, C, 3>(smem)) != cudaSuccess) return e;
-    if ((e = set_attr<S, C, 4>(smem)) != cudaSuccess) return e;
-    if ((e = set_attr<S, C, 5>(smem)) != cudaSuccess) return e;
-    return set_attr<S, C, 6>(smem);
+    if constexpr (sizeof(S) < sizeof(C)) {   // 16-bit storage: plain or split
+        if ((e = set_attr<S, C, 0>(smem)) != cudaSuccess) return e;
+        return set_attr<S, C, 7>(smem);
+    } else {
+        if ((e = set_attr<S, C, 0>(smem)) != cudaSuccess) return e;
+        if ((e = set_attr<S, C, 1>(smem)) != cudaSuccess) return e;
+        if ((e = set_attr<S, C, 2>(smem)) != cudaSuccess) return e;
+        if ((e = set_attr<S, C, 3>(smem)) != cudaSuccess) return e;
+        if ((e = set_attr<S, C, 4>(smem)) != cudaSuccess) return e;
+        if ((e = set_attr<S, C, 5>(smem)) != cudaSuccess) return e;
+        return set_attr<S, C, 6>(smem);
+    }
 }
 
 template <class S, class C>
@@ -690,21 +744,23 @@ void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, cudaStream_t 
         if (energy) k_elastic_fused<S, C, N, true><<<grid, block, smem, st>>>(a);    \
         else k_elastic_fused<S, C, N, false><<<grid, block, smem, st>>>(a);          \
         break;
-    switch (cpst) {
-        TW_FUSED_CASE(0)
-        TW_FUSED_CASE(1)
-        TW_FUSED_CASE(2)
-        TW_FUSED_CASE(3)
-        TW_FUSED_CASE(4)
-        TW_FUSED_CASE(5)
-        TW_FUSED_CASE(6)
+    if constexpr (sizeof(S) < sizeof(C)) {
+        switch (cpst) {
+            TW_FUSED_CASE(0)
+            TW_FUSED_CASE(7)
+        }
+    } else {
+        switch (cpst) {
+            TW_FUSED_CASE(0)
+            TW_FUSED_CASE(1)
+            TW_FUSED_CASE(2)
+            TW_FUSED_CASE(3)
+            TW_FUSED_CASE(4)
+            TW_FUSED_CASE(5)
+            TW_FUSED_CASE(6)
+        }
     }
 #undef TW_FUSED_CASE
 }
-
-template cudaError_t prepare_fused<double, double>();
-template cudaError_t prepare_fused<float, float>();
-template void launch_fused<double, double>(const FusedArgs<double, double> &, int, bool, cudaStream_t);
-template void launch_fused<float, float>(const FusedArgs<float, float> &, int, bool, cudaStream_t);
 
 }  // namespace tw

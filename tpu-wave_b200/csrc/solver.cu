@@ -289,8 +289,12 @@ void enqueue(tw_solver *s, int n, cudaStream_t st)
 {
     if (s->fused) {
         for (int k = 0; k < n; k++) {
-            if (s->d.precision == TW_FP64) enqueue_fused_step<double, double>(s, st);
-            else enqueue_fused_step<float, float>(s, st);
+            switch (s->d.precision) {
+            case TW_FP64: enqueue_fused_step<double, double>(s, st); break;
+            case TW_FP32: enqueue_fused_step<float, float>(s, st); break;
+            case TW_BF16: enqueue_fused_step<__nv_bfloat16, float>(s, st); break;
+            default: enqueue_fused_step<__half, float>(s, st); break;
+            }
         }
         return;
     }
@@ -435,26 +439,40 @@ double from_storage(int prec, const void *src, long i)
     return (double)__half2float(((const __half *)src)[i]);
 }
 
-// copy a device array (rows x pitch) of `esz`-byte values to the host in the reference layout
-int read_device_array(tw_solver *s, const void *dev, int prec, int esz, int slot, double *host, long ld)
+// copy a device array (rows x pitch) of `esz`-byte values to the host in the reference layout;
+// with `lo` (split storage) the value is the FP32 sum hi + lo, as the stepper reads it
+int read_device_array(tw_solver *s, const void *dev, int prec, int esz, int slot, double *host, long ld,
+                      const void *lo = nullptr)
 {
     const long R = s->rows[slot], Cn = s->cols[slot];
-    std::vector<char> buf((size_t)R * Cn * esz);
+    std::vector<char> buf((size_t)R * Cn * esz), lbuf(lo ? buf.size() : 0);
     TW_CUDA(cudaMemcpy2DAsync(buf.data(), Cn * esz, dev, s->pitch * esz, Cn * esz, R, cudaMemcpyDeviceToHost, s->st));
+    if (lo) TW_CUDA(cudaMemcpy2DAsync(lbuf.data(), Cn * esz, lo, s->pitch * esz, Cn * esz, R, cudaMemcpyDeviceToHost, s->st));
     TW_CUDA(cudaStreamSynchronize(s->st));
     for (long ix = 0; ix < R; ix++)
-        for (long iy = 0; iy < Cn; iy++) host[ix * ld + iy] = from_storage(prec, buf.data(), ix * Cn + iy);
+        for (long iy = 0; iy < Cn; iy++) {
+            const long i = ix * Cn + iy;
+            host[ix * ld + iy] = lo ? (double)((float)from_storage(prec, buf.data(), i) + (float)from_storage(prec, lbuf.data(), i))
+                                    : from_storage(prec, buf.data(), i);
+        }
     return TW_OK;
 }
 
-int write_device_array(tw_solver *s, void *dev, int prec, int esz, int slot, const double *host, long ld)
+// the inverse; with `lo` (split storage) hi = the value rounded to storage, lo = the rounded rest
+int write_device_array(tw_solver *s, void *dev, int prec, int esz, int slot, const double *host, long ld,
+                       void *lo = nullptr)
 {
     const long R = s->rows[slot], Cn = s->cols[slot];
-    std::vector<double> tmp((size_t)R * Cn);
+    std::vector<double> tmp((size_t)R * Cn), rest(lo ? tmp.size() : 0);
     for (long ix = 0; ix < R; ix++)
         for (long iy = 0; iy < Cn; iy++) tmp[ix * Cn + iy] = host[ix * ld + iy];
-    std::vector<char> buf((size_t)R * Cn * esz);
+    std::vector<char> buf((size_t)R * Cn * esz), lbuf(lo ? buf.size() : 0);
     to_storage(prec, tmp.data(), buf.data(), R * Cn);
+    if (lo) {
+        for (long i = 0; i < R * Cn; i++) rest[i] = (double)((float)tmp[i] - (float)from_storage(prec, buf.data(), i));
+        to_storage(prec, rest.data(), lbuf.data(), R * Cn);
+        TW_CUDA(cudaMemcpy2DAsync(lo, s->pitch * esz, lbuf.data(), Cn * esz, Cn * esz, R, cudaMemcpyHostToDevice, s->st));
+    }
     TW_CUDA(cudaMemcpy2DAsync(dev, s->pitch * esz, buf.data(), Cn * esz, Cn * esz, R, cudaMemcpyHostToDevice, s->st));
     TW_CUDA(cudaStreamSynchronize(s->st));
     s->drop_graph();
@@ -501,8 +519,13 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
     if (d.physics != TW_ELASTIC && d.physics != TW_ACOUSTIC) return TW_ERR_INVALID;
     if (d.bc_x != TW_BC_SAT_FREE && d.bc_x != TW_BC_PERIODIC) return TW_ERR_INVALID;
     if (d.physics == TW_ELASTIC && d.bc_x == TW_BC_PERIODIC) return TW_ERR_UNSUPPORTED;
-    if (d.precision != TW_FP64 && d.precision != TW_FP32) return TW_ERR_UNSUPPORTED;
-    if (d.cpst < TW_CPST_00 || d.cpst > TW_CPST_6R) return TW_ERR_INVALID;
+    if (d.precision < TW_FP64 || d.precision > TW_FP16) return TW_ERR_INVALID;
+    if (d.cpst < TW_CPST_00 || d.cpst > TW_CPST_SPLIT) return TW_ERR_INVALID;
+    const bool narrow = d.precision == TW_BF16 || d.precision == TW_FP16;
+    // 16-bit storage (elastic only): plain, or the split pair hi + lo; the split pair needs a
+    // storage type narrower than the FP32 compute type
+    if (narrow && (d.physics != TW_ELASTIC || (d.cpst != TW_CPST_00 && d.cpst != TW_CPST_SPLIT))) return TW_ERR_UNSUPPORTED;
+    if (!narrow && d.cpst == TW_CPST_SPLIT) return TW_ERR_UNSUPPORTED;
     if (d.bc_x == TW_BC_PERIODIC && d.cpst != TW_CPST_00 && d.cpst != TW_CPST_3R && d.cpst != TW_CPST_6R)
         return TW_ERR_UNSUPPORTED;   // the single-core tree offers '0', '3', '6' (namespaces.hpp:665-667)
     if (d.Mx < 8 || d.My < 4 || d.Mx > (1L << 30) / 2 || d.My > (1L << 30) / 2) return TW_ERR_INVALID;
@@ -553,7 +576,12 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
     if (s->elastic) {
         // fused elastic path: a second copy of the state and the strip x segment geometry
         s->fused = true;
-        e = d.precision == TW_FP64 ? prepare_fused<double, double>() : prepare_fused<float, float>();
+        switch (d.precision) {
+        case TW_FP64: e = prepare_fused<double, double>(); break;
+        case TW_FP32: e = prepare_fused<float, float>(); break;
+        case TW_BF16: e = prepare_fused<__nv_bfloat16, float>(); break;
+        default: e = prepare_fused<__half, float>(); break;
+        }
         if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
         for (int k = 0; k < 5; k++) {
             const size_t n = (size_t)s->rows[k] * s->pitch;
@@ -824,7 +852,8 @@ int tw_read_field(tw_solver *s, int grid, int field, double *host, long ld)
     const int slot = slot_of(s, grid, field);
     if (slot < 0 || ld < s->ref_cols[grid]) return TW_ERR_INVALID;
     TW_CUDA(cudaSetDevice(s->d.device));
-    return read_device_array(s, cur_f(s, slot), s->d.precision, s->esz, slot, host, ld);
+    return read_device_array(s, cur_f(s, slot), s->d.precision, s->esz, slot, host, ld,
+                             s->d.cpst == TW_CPST_SPLIT ? cur_res(s, slot) : nullptr);
 }
 
 int tw_write_field(tw_solver *s, int grid, int field, const double *host, long ld)
@@ -833,7 +862,8 @@ int tw_write_field(tw_solver *s, int grid, int field, const double *host, long l
     const int slot = slot_of(s, grid, field);
     if (slot < 0 || ld < s->ref_cols[grid]) return TW_ERR_INVALID;
     TW_CUDA(cudaSetDevice(s->d.device));
-    return write_device_array(s, cur_f(s, slot), s->d.precision, s->esz, slot, host, ld);
+    return write_device_array(s, cur_f(s, slot), s->d.precision, s->esz, slot, host, ld,
+                              s->d.cpst == TW_CPST_SPLIT ? cur_res(s, slot) : nullptr);
 }
 
 int tw_read_resid(tw_solver *s, int grid, int field, double *host, long ld)

@@ -45,6 +45,15 @@ __device__ __forceinline__ C ld(const __nv_bfloat16 *p, long i) { return to_c<C>
 template <class C>
 __device__ __forceinline__ C ld(const __half *p, long i) { return to_c<C>(p[i]); }
 
+// a field stored as a pair hi + lo (split compensation): reads return the sum
+template <class S>
+struct HiLo {
+    const S *hi, *lo;
+    __device__ __forceinline__ HiLo operator+(long o) const { return {hi + o, lo + o}; }
+};
+template <class C, class S>
+__device__ __forceinline__ C ld(HiLo<S> p, long i) { return add(ld<C>(p.hi, i), ld<C>(p.lo, i)); }
+
 // derivative along x of an M-type-x row ix (rows 0..Mx-1) from its N-type neighbour with rows
 // 0..Mx: DN closures on 3 rows at each end, interior shifts {-1,0,1,2} (grid_drvt.tpp:312-466,
 // grid.hpp:361-362). get(r) returns the neighbour's value at row r of this column.
@@ -86,14 +95,14 @@ __device__ __forceinline__ C dxM(const Ops<C> &o, int Mx, int ix, G get)
     return v;
 }
 
-template <class C, class S>
-__device__ __forceinline__ C dx_from_N(const Ops<C> &o, const S *nb, long pitch, int Mx, int ix, int iy)
+template <class C, class A>
+__device__ __forceinline__ C dx_from_N(const Ops<C> &o, A nb, long pitch, int Mx, int ix, int iy)
 {
     return dxN<C>(o, Mx, ix, [&](int r) { return ld<C>(nb, (long)r * pitch + iy); });
 }
 
-template <class C, class S>
-__device__ __forceinline__ C dx_from_M(const Ops<C> &o, const S *nb, long pitch, int Mx, int ix, int iy)
+template <class C, class A>
+__device__ __forceinline__ C dx_from_M(const Ops<C> &o, A nb, long pitch, int Mx, int ix, int iy)
 {
     return dxM<C>(o, Mx, ix, [&](int r) { return ld<C>(nb, (long)r * pitch + iy); });
 }
@@ -114,8 +123,8 @@ __device__ __forceinline__ C dx_periodic(const Ops<C> &o, const S *nb, long pitc
 
 // periodic y derivative (grid.hpp:361-362, grid_drvt.tpp:45-167): an N-type-y point reads
 // M-type columns iy-2..iy+1 (wrapped), an M-type-y point reads N-type columns iy-1..iy+2
-template <bool FROM_N, class C, class S>
-__device__ __forceinline__ C dy_periodic(const Ops<C> &o, const S *row, int My, int iy)
+template <bool FROM_N, class C, class A>
+__device__ __forceinline__ C dy_periodic(const Ops<C> &o, A row, int My, int iy)
 {
     C v = C(0);
 #pragma unroll
@@ -128,8 +137,8 @@ __device__ __forceinline__ C dy_periodic(const Ops<C> &o, const S *row, int My, 
 
 // SAT penalty of the M-type-x velocity grid MN (rows 0..2 and Mx-3..Mx-1): the boundary value
 // of the NN neighbour (projection {1}) times eta*A_inv_projection (grid_drvt.tpp:563-693)
-template <class C, class S>
-__device__ __forceinline__ bool sat_MN(const Ops<C> &o, const S *nn, long pitch, int Mx, int ix, int iy, C &v)
+template <class C, class A>
+__device__ __forceinline__ bool sat_MN(const Ops<C> &o, A nn, long pitch, int Mx, int ix, int iy, C &v)
 {
     if (ix < 3) {
         const C send = add(C(0), mul(o.pN, ld<C>(nn, iy)));
@@ -146,8 +155,8 @@ __device__ __forceinline__ bool sat_MN(const Ops<C> &o, const S *nn, long pitch,
 
 // SAT penalty of the N-type-x velocity grid NM (rows 0 and Mx): sxx extrapolated to the
 // boundary with {15/8, -5/4, 3/8} over three MM rows
-template <class C, class S>
-__device__ __forceinline__ bool sat_NM(const Ops<C> &o, const S *mm, long pitch, int Mx, int ix, int iy, C &v)
+template <class C, class A>
+__device__ __forceinline__ bool sat_NM(const Ops<C> &o, A mm, long pitch, int Mx, int ix, int iy, C &v)
 {
     if (ix == 0) {
         C send = C(0);
