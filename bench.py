@@ -21,6 +21,11 @@ bandwidth; `cpu_baseline` = the reference's own CPU solver (oracle/_ref) on a bo
 seeded Gaussian-random-field medium, 2000 steps, every storage variant (FP64, FP32, BF16 and
 FP16, plain and split) device-timed, with the relative L2 / Linf field error and the trace error
 of each against the FP64 run of the same scheme.
+
+`--workload batch` measures batching: 64 acoustic shots (periodic, FP32) of sizes drawn from
+{256, 512, 1024, 2048}^2, each with its own seeded 8-layer medium and source, stepped together by
+one batched launch per half-step (launch shape from the autotuner) against the same 64 handles
+solved one after another; the traces of the two must agree bit for bit.
 """
 from __future__ import annotations
 
@@ -441,6 +446,88 @@ def run_mixed(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- batched acoustic workload
+BATCH_SEED = 20261203 + 4
+
+
+def batch_shots(tw, n_shots: int, steps: int):
+    rng = np.random.default_rng(BATCH_SEED)
+    shots, cells = [], 0
+    for k in range(n_shots):
+        side = int(rng.choice([256, 512, 1024, 2048]))
+        nl = 8
+        c_l, rho_l = rng.uniform(1.0, 3.0, nl), rng.uniform(1.0, 2.5, nl)
+        dx = 1.0 / side
+        dt = 0.5 * dx / (np.sqrt(2.0) * c_l.max())
+        sx, sy = (int(v) for v in rng.integers(8, side - 8, 2))
+        s = tw.Solver(side, side, 1, side, dt, physics=tw.ACOUSTIC, bc_x=tw.PERIODIC, precision="f32", cpst="00",
+                      central_f=10.0, time_delay=0.1, max_steps=steps + 64, energy=False)
+        lay = np.minimum(np.arange(side + 1) * nl // side, nl - 1)
+        lay[side] = lay[0]   # the periodic seam row repeats row 0
+        rho_x = rho_l[lay][:, None] * np.ones((1, side))            # Vx: (side+1) x side
+        rho_y = rho_l[lay[:side]][:, None] * np.ones((1, side + 1))  # Vy: side x (side+1)
+        kap = (rho_l * c_l ** 2)[lay[:side]][:, None] * np.ones((1, side))
+        s.set_material_grid(tw.NM, 0, rho_x)
+        s.set_material_grid(tw.MN, 0, rho_y)
+        s.set_material_grid(tw.MM, 0, kap)
+        s.set_source(tw.MM, sx, sy)
+        s.add_receivers(tw.MM, np.full(16, (sx + 10) % side), (sy + np.arange(16) * (side // 16)) % side)
+        shots.append(s)
+        cells += side * side
+    return shots, cells
+
+
+def run_batch(args):
+    import torch
+    tw = load_twave()
+    torch.cuda.set_device(0)
+    K = args.steps
+    shots, cells = batch_shots(tw, 64, K)
+    # 64 sequential plain solves (each handle stepped alone, graphs of 16 steps)
+    for s in shots:
+        s.run(args.warmup)
+        s.reset()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for s in shots:
+        s.run(K)
+    t_seq = time.perf_counter() - t0
+    seq_traces = [s.read_receivers() for s in shots]
+    for s in shots:
+        s.reset()
+    b = tw.Batch(shots)
+    tuned_ms = b.tune(8)
+    shape = b.shape()
+    b.run(args.warmup)
+    for s in shots:
+        s.reset()
+    clocks = ClockSampler(0)
+    clocks.start()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.run(K)
+    t_bat = time.perf_counter() - t0
+    clk = clocks.stop()
+    same = all(np.array_equal(s.read_receivers(), t) for s, t in zip(shots, seq_traces))
+    b.close()
+    for s in shots:
+        s.close()
+    peak, peak_note = measured_peaks()
+    v_bat, v_seq = cells * K / t_bat / 1e9, cells * K / t_seq / 1e9
+    line = {"metric": METRIC, "value": v_bat, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": args.warmup,
+            "ms_per_step": t_bat / K * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batching: 64 acoustic periodic shots, sides drawn from {256,512,1024,2048} (seeded), "
+                                   "8-layer media c ~ U(1,3), rho ~ U(1,2.5), Ricker f0=10, CFL 0.5, 16 receivers each",
+                       "cells_per_step": cells, "timing": "host clock around the whole run, synchronised (both arms)"},
+            "sequential": {"value": v_seq, "unit": UNIT, "seconds": t_seq},
+            "batched": {"seconds": t_bat, "shape": shape, "tuned_ms_per_step": tuned_ms,
+                        "speedup_vs_sequential": t_seq / t_bat, "traces_identical_to_sequential": same,
+                        "hbm_frac_at_36B": v_bat * 36 / peak, "peak": f"{peak} GB/s {peak_note}"},
+            "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -449,7 +536,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["elastic2048", "mixed"], default="elastic2048")
+    ap.add_argument("--workload", choices=["elastic2048", "mixed", "batch"], default="elastic2048")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
@@ -457,9 +544,9 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args, dist)
         return
-    if args.workload == "mixed":
+    if args.workload in ("mixed", "batch"):
         if dist.rank == 0:
-            run_mixed(args)
+            (run_mixed if args.workload == "mixed" else run_batch)(args)
         return
     run_ours(args, dist)
 

@@ -187,6 +187,34 @@ TW_API int tw_material_map_noalloc(const double *d_rho, const double *d_vp, cons
                                    int den_dx, double *d_NN_mu, double *d_MN_rho, double *d_NM_rho,
                                    double *d_MM_lambda, double *d_MM_2mu, void *stream);
 
+/* ---- batched shots ---------------------------------------------------------------------
+ * No counterpart in the reference, which runs one shot per process. A batch advances many
+ * acoustic handles (the shots: independent grids of any sizes) together: each half-step is ONE
+ * launch over the tiles of all shots and one more launch records every shot's receivers, so
+ * small shots no longer pay a launch per half-step each; G steps are replayed from a CUDA graph.
+ * Each shot equals the same handle stepped alone with tw_step, bit for bit.
+ * Requirements: acoustic handles on one device with the same precision (FP64/FP32),
+ * compensation ('0', '3R', '6R') and x boundary, energy off, material set. The batch copies each
+ * shot's set-up (source, receivers, buffers) at tw_batch_create: re-create it after changing a
+ * shot's source or receivers. Shots stay usable on their own (readback, tw_step); tw_batch_step
+ * orders itself after the shots' queued work and their later work after the batch. */
+typedef struct tw_batch tw_batch;
+TW_API int tw_batch_create(tw_batch **out, tw_solver *const *shots, int n);
+TW_API void tw_batch_destroy(tw_batch *b);
+/* Launch shape: blocks of tx x ty threads (tx*ty <= 256, a multiple of 32), rows_per_thread rows
+ * per thread, `ctas` persistent CTAs walking the tile list (0: one CTA per tile). */
+TW_API int tw_batch_set_shape(tw_batch *b, int tx, int ty, int rows_per_thread, int ctas);
+TW_API int tw_batch_get_shape(tw_batch *b, int *shape4);
+/* Autotuner: times `steps` batched steps for each candidate shape (tx in {32, 64, 128, 256},
+ * 1/2/4 rows per thread, one CTA per tile or 4/8/16 persistent CTAs per SM), keeps the fastest
+ * and returns its ms per step. It steps the shots, so it RESETS every shot afterwards
+ * (tw_reset: fields, records and step counters zeroed); call it before setting initial fields. */
+TW_API int tw_batch_tune(tw_batch *b, int steps, double *best_ms);
+/* Advance every shot n steps (asynchronous); each shot's record must hold n more steps. */
+TW_API int tw_batch_step(tw_batch *b, int n);
+/* Wait for the batch; returns the first sticky error of any shot. */
+TW_API int tw_batch_sync(tw_batch *b);
+
 TW_API const char *tw_strerror(int status);
 TW_API const char *tw_last_cuda_error(void);
 

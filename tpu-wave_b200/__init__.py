@@ -90,6 +90,14 @@ def lib() -> C.CDLL:
         L.tw_material_map_noalloc.argtypes = [vp, vp, vp, C.c_long, C.c_long, C.c_int, C.c_int, C.c_long, C.c_long,
                                               C.c_int, C.c_int, vp, vp, vp, vp, vp, vp]
         L.tw_location_to_index.argtypes = [C.c_char, C.c_long, C.c_long, C.c_int, C.c_int, lp]
+        L.tw_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
+        L.tw_batch_destroy.argtypes = [vp]
+        L.tw_batch_destroy.restype = None
+        L.tw_batch_set_shape.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.tw_batch_get_shape.argtypes = [vp, C.POINTER(C.c_int)]
+        L.tw_batch_tune.argtypes = [vp, C.c_int, dp]
+        L.tw_batch_step.argtypes = [vp, C.c_int]
+        L.tw_batch_sync.argtypes = [vp]
         L.tw_strerror.restype = C.c_char_p
         L.tw_strerror.argtypes = [C.c_int]
         L.tw_last_cuda_error.restype = C.c_char_p
@@ -270,3 +278,49 @@ class Solver:
         p = C.c_void_p()
         _ok(lib().tw_get_stream(self.h, C.byref(p)), "tw_get_stream")
         return p.value or 0
+
+
+class Batch:
+    """Many acoustic Solver handles stepped together (one launch per half-step for all shots).
+    The shots keep their own set-up and readback; see tw_batch_create."""
+
+    def __init__(self, shots):
+        self.shots = list(shots)
+        arr = (C.c_void_p * len(self.shots))(*[s.h for s in self.shots])
+        self.h = C.c_void_p()
+        _ok(lib().tw_batch_create(C.byref(self.h), arr, len(self.shots)), "tw_batch_create")
+
+    def close(self):
+        if self.h:
+            lib().tw_batch_destroy(self.h)
+            self.h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_shape(self, tx: int, ty: int, rows_per_thread: int = 1, ctas: int = 0):
+        _ok(lib().tw_batch_set_shape(self.h, tx, ty, rows_per_thread, ctas), "tw_batch_set_shape")
+
+    def shape(self):
+        out = (C.c_int * 4)()
+        _ok(lib().tw_batch_get_shape(self.h, out), "tw_batch_get_shape")
+        return tuple(out)
+
+    def tune(self, steps: int = 8) -> float:
+        """Pick the fastest launch shape; resets every shot afterwards."""
+        ms = C.c_double()
+        _ok(lib().tw_batch_tune(self.h, steps, C.byref(ms)), "tw_batch_tune")
+        return ms.value
+
+    def step(self, n: int):
+        _ok(lib().tw_batch_step(self.h, n), "tw_batch_step")
+
+    def sync(self):
+        _ok(lib().tw_batch_sync(self.h), "tw_batch_sync")
+
+    def run(self, n: int):
+        self.step(n)
+        self.sync()

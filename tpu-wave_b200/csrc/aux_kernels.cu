@@ -204,7 +204,7 @@ template void launch_energy<float, float>(const EnergyArgs<float, float> &, cuda
 
 // ---------------------------------------------------------------- receivers + step counter
 template <class S>
-__global__ void k_gather(GatherArgs<S> g)
+__device__ __forceinline__ void gather_block(const GatherArgs<S> &g)
 {
     const int it = *g.step;
     if (it < g.max_steps) {
@@ -222,11 +222,32 @@ __global__ void k_gather(GatherArgs<S> g)
 }
 
 template <class S>
+__global__ void k_gather(GatherArgs<S> g)
+{
+    gather_block(g);
+}
+
+// one block per shot of a batch
+template <class S>
+__global__ void k_batch_gather(const GatherArgs<S> *g)
+{
+    gather_block(g[blockIdx.x]);
+}
+
+template <class S>
 void launch_gather(const GatherArgs<S> &g, cudaStream_t st)
 {
     k_gather<S><<<1, 256, 0, st>>>(g);
 }
 template void launch_gather<double>(const GatherArgs<double> &, cudaStream_t);
 template void launch_gather<float>(const GatherArgs<float> &, cudaStream_t);
+
+template <class S>
+void launch_batch_gather(const GatherArgs<S> *g, int n_shots, cudaStream_t st)
+{
+    k_batch_gather<S><<<n_shots, 128, 0, st>>>(g);
+}
+template void launch_batch_gather<double>(const GatherArgs<double> *, int, cudaStream_t);
+template void launch_batch_gather<float>(const GatherArgs<float> *, int, cudaStream_t);
 
 }  // namespace tw

@@ -123,5 +123,25 @@ struct GatherArgs {
 };
 template <class S>
 void launch_gather(const GatherArgs<S> &g, cudaStream_t st);
+// receiver gather of every shot of a batch (one block per shot; g in device memory)
+template <class S>
+void launch_batch_gather(const GatherArgs<S> *g, int n_shots, cudaStream_t st);
+
+// batched acoustic stepping (batch.cu): the shots of a batch are independent grids; one launch
+// per half-step covers the tiles of all of them. A tile is tx columns x ty * rpt rows of a shot's
+// N-sized region, handled by a tx x ty block (rpt rows per thread); `ctas` persistent CTAs walk
+// the tile list (ctas >= the tile count: one CTA per tile).
+template <class S, class C>
+struct BatchShot {
+    StepArgs<S, C> a;
+    int tiles_x;              // tiles along y
+    int tile_off;             // index of the shot's first tile
+};
+struct BatchShape {
+    int tx, ty, rpt, ctas;
+};
+template <class S, class C>
+void launch_batch_half(int periodic, int cpst, int half, const BatchShot<S, C> *shots, const int *tile_shot,
+                       int n_tiles, const BatchShape &b, cudaStream_t st);
 
 }  // namespace tw

@@ -980,3 +980,275 @@ int tw_get_stream(tw_solver *s, void **stream)
 }
 
 }  // extern "C"
+
+// ======================================================================== batched shots
+// Many acoustic handles advanced together: one launch per half-step covers the tiles of every
+// shot (batch.cu), one launch gathers every shot's receivers and advances every step counter.
+struct tw_batch {
+    std::vector<tw_solver *> shots;
+    int precision = TW_FP32, cpst = 0, periodic = 0, device = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t done = nullptr;
+    void *d_shots = nullptr, *d_gather = nullptr;
+    int *d_tile_shot = nullptr;
+    int tile_cap = 0, n_tiles = 0;
+    BatchShape shape{32, 8, 1, 0};
+    cudaGraphExec_t gexec = nullptr;
+    int graph_steps = 0;
+
+    void drop_graph()
+    {
+        if (gexec) cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+        graph_steps = 0;
+    }
+    ~tw_batch()
+    {
+        drop_graph();
+        cudaFree(d_shots); cudaFree(d_gather); cudaFree(d_tile_shot);
+        if (done) cudaEventDestroy(done);
+        if (st) cudaStreamDestroy(st);
+    }
+};
+
+namespace {
+
+bool shape_ok(const BatchShape &b)
+{
+    return b.tx >= 1 && b.ty >= 1 && b.tx * b.ty <= 256 && (b.tx * b.ty) % 32 == 0 && b.rpt >= 1 && b.rpt <= 64 &&
+           b.ctas >= 0;
+}
+
+// tile list and per-shot arguments for a launch shape
+template <class S, class C>
+int batch_layout_t(tw_batch *b, const BatchShape &shape)
+{
+    const int n = (int)b->shots.size();
+    std::vector<BatchShot<S, C>> sh(n);
+    std::vector<GatherArgs<S>> ga(n);
+    std::vector<int> tile_shot;
+    for (int k = 0; k < n; k++) {
+        tw_solver *s = b->shots[k];
+        const long rows = s->d.Mx + 1, cols = s->d.My + 1;   // the N-sized region covers every grid
+        const long tx = (cols + shape.tx - 1) / shape.tx, ty = (rows + (long)shape.ty * shape.rpt - 1) / ((long)shape.ty * shape.rpt);
+        if ((long)tile_shot.size() + tx * ty > (1L << 30)) return TW_ERR_INVALID;
+        sh[k].a = step_args<S, C>(s);
+        sh[k].tiles_x = (int)tx;
+        sh[k].tile_off = (int)tile_shot.size();
+        tile_shot.insert(tile_shot.end(), (size_t)(tx * ty), k);
+        GatherArgs<S> &g = ga[k];
+        for (int q = 0; q < 5; q++) g.f[q] = (const S *)s->f[q];
+        g.rcv = s->d_rcv;
+        g.n_rcv = (int)(s->rcv_tab.size() / 4);
+        g.pitch = s->pitch;
+        g.traces = s->d_traces;
+        g.max_steps = s->d.max_steps;
+        g.step = s->d_step;
+        g.flags = s->d_flags;
+    }
+    if ((int)tile_shot.size() > b->tile_cap) {
+        cudaFree(b->d_tile_shot);
+        b->d_tile_shot = nullptr;
+        TW_CUDA(cudaMalloc((void **)&b->d_tile_shot, sizeof(int) * tile_shot.size()));
+        b->tile_cap = (int)tile_shot.size();
+    }
+    if (!b->d_shots) {
+        TW_CUDA(cudaMalloc(&b->d_shots, sizeof(BatchShot<S, C>) * n));
+        TW_CUDA(cudaMalloc(&b->d_gather, sizeof(GatherArgs<S>) * n));
+    }
+    TW_CUDA(cudaMemcpyAsync(b->d_shots, sh.data(), sizeof(BatchShot<S, C>) * n, cudaMemcpyHostToDevice, b->st));
+    TW_CUDA(cudaMemcpyAsync(b->d_gather, ga.data(), sizeof(GatherArgs<S>) * n, cudaMemcpyHostToDevice, b->st));
+    TW_CUDA(cudaMemcpyAsync(b->d_tile_shot, tile_shot.data(), sizeof(int) * tile_shot.size(), cudaMemcpyHostToDevice, b->st));
+    TW_CUDA(cudaStreamSynchronize(b->st));
+    b->n_tiles = (int)tile_shot.size();
+    b->shape = shape;
+    if (b->shape.ctas == 0) b->shape.ctas = b->n_tiles;
+    b->drop_graph();
+    return TW_OK;
+}
+
+int batch_layout(tw_batch *b, const BatchShape &shape)
+{
+    return b->precision == TW_FP64 ? batch_layout_t<double, double>(b, shape) : batch_layout_t<float, float>(b, shape);
+}
+
+template <class S, class C>
+void enqueue_batch_t(tw_batch *b, int n, cudaStream_t st)
+{
+    const auto *sh = (const BatchShot<S, C> *)b->d_shots;
+    for (int k = 0; k < n; k++) {
+        launch_batch_half<S, C>(b->periodic, b->cpst, 0, sh, b->d_tile_shot, b->n_tiles, b->shape, st);
+        launch_batch_half<S, C>(b->periodic, b->cpst, 1, sh, b->d_tile_shot, b->n_tiles, b->shape, st);
+        launch_batch_gather<S>((const GatherArgs<S> *)b->d_gather, (int)b->shots.size(), st);
+    }
+}
+
+void enqueue_batch(tw_batch *b, int n, cudaStream_t st)
+{
+    if (b->precision == TW_FP64) enqueue_batch_t<double, double>(b, n, st);
+    else enqueue_batch_t<float, float>(b, n, st);
+}
+
+}  // namespace
+
+extern "C" {
+
+int tw_batch_create(tw_batch **out, tw_solver *const *shots, int n)
+{
+    if (!out || !shots || n < 1) return TW_ERR_INVALID;
+    *out = nullptr;
+    const tw_solver *s0 = shots[0];
+    if (!s0) return TW_ERR_INVALID;
+    for (int k = 0; k < n; k++) {
+        const tw_solver *s = shots[k];
+        if (!s) return TW_ERR_INVALID;
+        for (int q = 0; q < k; q++)
+            if (shots[q] == s) return TW_ERR_INVALID;
+        if (s->elastic || s->d.energy) return TW_ERR_UNSUPPORTED;
+        if (s->d.cpst != TW_CPST_00 && s->d.cpst != TW_CPST_3R && s->d.cpst != TW_CPST_6R) return TW_ERR_UNSUPPORTED;
+        if (s->d.device != s0->d.device || s->d.precision != s0->d.precision || s->d.cpst != s0->d.cpst ||
+            s->d.bc_x != s0->d.bc_x)
+            return TW_ERR_UNSUPPORTED;
+        if (!s->mat_ready) return TW_ERR_STATE;
+    }
+    tw_batch *b = new (std::nothrow) tw_batch();
+    if (!b) return TW_ERR_NOMEM;
+    b->shots.assign(shots, shots + n);
+    b->precision = s0->d.precision;
+    b->cpst = s0->d.cpst;
+    b->periodic = s0->periodic;
+    b->device = s0->d.device;
+    auto fail = [&](int code) { delete b; return code; };
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+    if (e != cudaSuccess) return fail(cuda_fail(e, "tw_batch_create"));
+    const int rc = batch_layout(b, BatchShape{32, 8, 1, 0});
+    if (rc != TW_OK) return fail(rc);
+    *out = b;
+    return TW_OK;
+}
+
+void tw_batch_destroy(tw_batch *b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->st) cudaStreamSynchronize(b->st);
+    delete b;
+}
+
+int tw_batch_set_shape(tw_batch *b, int tx, int ty, int rows_per_thread, int ctas)
+{
+    if (!b) return TW_ERR_INVALID;
+    const BatchShape sh{tx, ty, rows_per_thread, ctas};
+    if (!shape_ok(sh)) return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(b->device));
+    return batch_layout(b, sh);
+}
+
+int tw_batch_get_shape(tw_batch *b, int *shape4)
+{
+    if (!b || !shape4) return TW_ERR_INVALID;
+    shape4[0] = b->shape.tx;
+    shape4[1] = b->shape.ty;
+    shape4[2] = b->shape.rpt;
+    shape4[3] = b->shape.ctas;
+    return TW_OK;
+}
+
+int tw_batch_tune(tw_batch *b, int steps, double *best_ms)
+{
+    if (!b || steps < 1) return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(b->device));
+    for (tw_solver *s : b->shots) {
+        TW_CUDA(cudaStreamSynchronize(s->st));
+        if (steps + 1 > s->d.max_steps) steps = s->d.max_steps - 1;
+    }
+    if (steps < 1) return TW_ERR_RECORD_FULL;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    std::vector<BatchShape> cand;
+    for (int tx : {32, 64, 128, 256})
+        for (int rpt : {1, 2, 4})
+            for (int per_sm : {0, 4, 8, 16}) cand.push_back(BatchShape{tx, 256 / tx, rpt, per_sm * sms});
+    cudaEvent_t e0, e1;
+    TW_CUDA(cudaEventCreate(&e0));
+    TW_CUDA(cudaEventCreate(&e1));
+    double best = 1e300;
+    BatchShape pick = b->shape;
+    int rc = TW_OK;
+    for (const BatchShape &c : cand) {
+        if ((rc = batch_layout(b, c)) != TW_OK) break;
+        for (tw_solver *s : b->shots) cudaMemsetAsync(s->d_step, 0, sizeof(int), b->st);
+        enqueue_batch(b, 1, b->st);
+        cudaEventRecord(e0, b->st);
+        enqueue_batch(b, steps, b->st);
+        cudaEventRecord(e1, b->st);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) { rc = cuda_fail(e, "tw_batch_tune"); break; }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms / steps < best) { best = ms / steps; pick = c; }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != TW_OK) return rc;
+    if ((rc = batch_layout(b, pick)) != TW_OK) return rc;
+    for (tw_solver *s : b->shots)
+        if ((rc = tw_reset(s)) != TW_OK) return rc;
+    if (best_ms) *best_ms = best;
+    return TW_OK;
+}
+
+int tw_batch_step(tw_batch *b, int n)
+{
+    if (!b || n < 0) return TW_ERR_INVALID;
+    for (tw_solver *s : b->shots)
+        if (s->steps_done + (long)n > s->d.max_steps) return TW_ERR_RECORD_FULL;
+    if (n == 0) return TW_OK;
+    TW_CUDA(cudaSetDevice(b->device));
+    for (tw_solver *s : b->shots) TW_CUDA(cudaStreamSynchronize(s->st));   // queued single-shot work first
+    const int G = 16;
+    int left = n;
+    if (left >= G) {
+        if (!b->gexec || b->graph_steps != G) {
+            b->drop_graph();
+            cudaGraph_t graph;
+            TW_CUDA(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+            enqueue_batch(b, G, b->st);
+            TW_CUDA(cudaStreamEndCapture(b->st, &graph));
+            cudaError_t e = cudaGraphInstantiate(&b->gexec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+            b->graph_steps = G;
+        }
+        while (left >= G) {
+            TW_CUDA(cudaGraphLaunch(b->gexec, b->st));
+            left -= G;
+        }
+    }
+    if (left > 0) enqueue_batch(b, left, b->st);
+    TW_CUDA(cudaGetLastError());
+    // later work on each shot's own stream (readback, single-shot steps) waits for the batch
+    TW_CUDA(cudaEventRecord(b->done, b->st));
+    for (tw_solver *s : b->shots) {
+        TW_CUDA(cudaStreamWaitEvent(s->st, b->done, 0));
+        s->steps_done += n;
+    }
+    return TW_OK;
+}
+
+int tw_batch_sync(tw_batch *b)
+{
+    if (!b) return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(b->device));
+    TW_CUDA(cudaStreamSynchronize(b->st));
+    int first = TW_OK;
+    for (tw_solver *s : b->shots) {
+        const int rc = tw_sync(s);
+        if (rc != TW_OK && first == TW_OK) first = rc;
+    }
+    return first;
+}
+
+}  // extern "C"
