@@ -26,6 +26,12 @@ of each against the FP64 run of the same scheme.
 {256, 512, 1024, 2048}^2, each with its own seeded 8-layer medium and source, stepped together by
 one batched launch per half-step (launch shape from the autotuner) against the same 64 handles
 solved one after another; the traces of the two must agree bit for bit.
+
+`--workload adjoint` measures the adjoint gradient: elastic 1024 x 1024 FP32, 2000 steps, 8
+shots along row 16, 256 receivers on NM row 4; observed traces from the layered medium with a 5 %
+Gaussian anomaly, gradient of the misfit with respect to rho, vp, vs of the layered medium,
+checkpoints every 50 steps; checked against central differences (h = 1e-3) along 8 random
+directions and by the dot-product identity of the state map (FP64).
 """
 from __future__ import annotations
 
@@ -528,6 +534,143 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- adjoint workload
+ADJ_N = 1024
+ADJ_SEED = 20261203 + 5
+
+
+def adjoint_media():
+    rng = np.random.default_rng(ADJ_SEED)
+    nl, n = 8, ADJ_N
+    vp_l, rho_l = rng.uniform(1.5, 4.5, nl), rng.uniform(1.8, 2.7, nl)
+    P = (n + 2, n + 2)
+    layer = np.minimum(np.arange(n + 2) * nl // (n + 1), nl - 1)
+    vp = np.repeat(vp_l[layer][:, None], n + 2, axis=1)
+    rho = np.repeat(rho_l[layer][:, None], n + 2, axis=1)
+    vs = vp / np.sqrt(3.0) * rng.uniform(0.9, 1.1, P)
+    X, Y = np.meshgrid(np.arange(n + 2), np.arange(n + 2), indexing="ij")
+    bump = 1.0 + 0.05 * np.exp(-((X - 150.0) ** 2 + (Y - n / 2) ** 2) / (2 * 40.0 ** 2))
+    return rho, vp, vs, bump
+
+
+def run_adjoint(args):
+    import torch
+    tw = load_twave()
+    torch.cuda.set_device(0)
+    n, K = ADJ_N, args.steps
+    rho, vp, vs, bump = adjoint_media()
+    dt = CFL * (1.0 / DEN_DX) / (np.sqrt(2.0) * (vp * bump).max())
+    shots = [(16, 64 + 128 * k) for k in range(8)]
+    rx, ry = np.full(256, 4), 4 * np.arange(256)
+
+    def make(prec, r, p, q, src, energy=False):
+        s = tw.Solver(n, n, 1, DEN_DX, dt, precision=prec, cpst="00", central_f=F0, time_delay=DELAY,
+                      max_steps=K, energy=energy)
+        s.set_material_model(r, p, q)
+        if src is not None:
+            s.set_source(tw.MM, *src)
+        s.add_receivers(tw.NM, rx, ry)
+        return s
+
+    def traces(prec, r, p, q, src):
+        s = make(prec, r, p, q, src)
+        s.run(K)
+        t = s.read_receivers()
+        s.close()
+        return t
+
+    obs = [traces("f32", rho, vp * bump, vs * bump, src) for src in shots]
+    # forward alone (device time), then the gradient call (host clock, synchronised), per shot
+    s = make("f32", rho, vp, vs, shots[0])
+    stream = torch.cuda.ExternalStream(s.stream())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step(K)
+    e1.record(stream)
+    s.sync()
+    fwd_ms = e0.elapsed_time(e1)
+    s.close()
+    g = {"rho": 0., "vp": 0., "vs": 0.}
+    J0 = 0.
+    t_grad = 0.
+    for src, o in zip(shots, obs):
+        s = make("f32", rho, vp, vs, src)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = s.adjoint_gradient(K, o, ckpt_every=50)
+        t_grad += time.perf_counter() - t0
+        s.close()
+        J0 += out["misfit"]
+        for k in g:
+            g[k] = g[k] + out[k]
+
+    # the same gradient in FP64, and central differences of the FP64 misfit along 8 random
+    # directions (unit normal perturbations of every node value of rho, vp, vs; h = 1e-3 and 1e-4)
+    obs64 = [traces("f64", rho, vp * bump, vs * bump, src) for src in shots]
+    g64 = {"rho": 0., "vp": 0., "vs": 0.}
+    for src, o in zip(shots, obs64):
+        s = make("f64", rho, vp, vs, src)
+        out = s.adjoint_gradient(K, o, ckpt_every=50)
+        s.close()
+        for k in g64:
+            g64[k] = g64[k] + out[k]
+
+    def misfit64(r, p, q):
+        return sum(0.5 * float(np.sum((traces("f64", r, p, q, src) - o) ** 2)) for src, o in zip(shots, obs64))
+
+    rng = np.random.default_rng(ADJ_SEED + 1)
+    fd_rows = []
+    for k in range(8):
+        d = [rng.standard_normal(rho.shape) for _ in range(3)]
+        ana64 = sum(float(np.sum(g64[key] * dd)) for key, dd in zip(("rho", "vp", "vs"), d))
+        ana32 = sum(float(np.sum(g[key] * dd)) for key, dd in zip(("rho", "vp", "vs"), d))
+        row = {"adjoint_f64": ana64, "adjoint_f32": ana32, "f32_vs_f64_rel": abs(ana32 - ana64) / abs(ana64)}
+        for h in (1e-3, 1e-4):
+            fd = (misfit64(rho + h * d[0], vp + h * d[1], vs + h * d[2]) -
+                  misfit64(rho - h * d[0], vp - h * d[1], vs - h * d[2])) / (2 * h)
+            row[f"fd_h{h:g}"] = fd
+            row[f"rel_err_h{h:g}"] = abs(fd - ana64) / abs(ana64)
+        fd_rows.append(row)
+    # dot-product identity of the state map L (initial fields -> traces), FP64, one shot, no source
+    srng = np.random.default_rng(ADJ_SEED + 2)
+    slots = [(tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)]
+    shapes = [(n + 1, n + 1), (n, n + 1), (n + 1, n), (n, n), (n, n)]
+    x = [srng.standard_normal(sh) for sh in shapes]
+    s = make("f64", rho, vp, vs, None)
+    for (gr, f), a in zip(slots, x):
+        s.write_field(gr, f, a)
+    s.run(K)
+    dd = s.read_receivers()
+    s.close()
+    y = srng.standard_normal(dd.shape)
+    y[:, 1, :] = 0.
+    s = make("f64", rho, vp, vs, None)
+    for (gr, f), a in zip(slots, x):
+        s.write_field(gr, f, a)
+    out = s.adjoint_gradient(K, dd - y, ckpt_every=50, model=False, state=True)
+    s.close()
+    lhs = float(np.sum(dd * y))
+    rhs = float(sum(np.sum(a * out["state"][k]) for a, k in zip(x, ("NN", "MN", "NM", "MM0", "MM1"))))
+    cells = n * n * K * len(shots)
+    line = {"metric": METRIC, "value": cells / t_grad / 1e9, "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": 0,
+            "higher_is_better": True, "dtype": "f32 fields, f64 gradient accumulation", "data": "synthetic",
+            "config": {"workload": f"adjoint gradient: elastic {n}x{n} FP32, {K} steps, 8 shots on MM row 16, 256 receivers "
+                                   "on NM row 4, 8-layer medium, observed data from a 5 % Gaussian anomaly in vp and vs, "
+                                   "checkpoints every 50 steps",
+                       "value": "cell-steps of the forward problem per second of the whole gradient call "
+                                "(forward sweep, segment recomputation, adjoint sweep), summed over the 8 shots"},
+            "forward_ms_per_step": fwd_ms / K, "forward_gpts": n * n * K / (fwd_ms / 1e3) / 1e9,
+            "gradient_seconds_per_shot": t_grad / len(shots),
+            "gradient_over_forward_time": (t_grad / len(shots)) / (fwd_ms / 1e3),
+            "misfit": J0, "finite_differences": {"field_precision": "f64 (FD and its adjoint); f32 adjoint compared",
+                                                 "directions": fd_rows,
+                                                 "max_rel_err_h1e-3": max(r["rel_err_h0.001"] for r in fd_rows),
+                                                 "max_rel_err_h1e-4": max(r["rel_err_h0.0001"] for r in fd_rows),
+                                                 "max_f32_vs_f64_rel": max(r["f32_vs_f64_rel"] for r in fd_rows)},
+            "dot_product_test_f64": {"lhs": lhs, "rhs": rhs, "rel_err": abs(lhs - rhs) / abs(lhs)}}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -536,7 +679,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["elastic2048", "mixed", "batch"], default="elastic2048")
+    ap.add_argument("--workload", choices=["elastic2048", "mixed", "batch", "adjoint"], default="elastic2048")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
@@ -544,9 +687,9 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args, dist)
         return
-    if args.workload in ("mixed", "batch"):
+    if args.workload in ("mixed", "batch", "adjoint"):
         if dist.rank == 0:
-            (run_mixed if args.workload == "mixed" else run_batch)(args)
+            {"mixed": run_mixed, "batch": run_batch, "adjoint": run_adjoint}[args.workload](args)
         return
     run_ours(args, dist)
 

@@ -187,6 +187,27 @@ TW_API int tw_material_map_noalloc(const double *d_rho, const double *d_vp, cons
                                    int den_dx, double *d_NN_mu, double *d_MN_rho, double *d_NM_rho,
                                    double *d_MM_lambda, double *d_MM_2mu, void *stream);
 
+/* ---- adjoint gradient ---------------------------------------------------------------------
+ * No counterpart in the reference (it has no adjoint). Full-waveform gradient of the misfit
+ * J = 1/2 sum_{r,f,it} (trace[r][f][it] - obs[r][f][it])^2 by the discrete adjoint of the elastic
+ * step (transposed SBP derivatives, closures and SAT penalties): a forward sweep of nt steps
+ * from the handle's current state (steps_done must be 0) keeping a checkpoint every ckpt_every
+ * steps, then a backward sweep that recomputes each segment from its checkpoint and steps the
+ * adjoint through it. Elastic, compensation "00", FP64 or FP32 fields; gradients accumulate in
+ * FP64. obs: [n_rcv][2][nt] like tw_read_receivers (entries of single-field receivers ignored).
+ * Outputs (any may be NULL):
+ *   misfit        J;
+ *   g_grid[5]     dJ/d(material on each grid) at reference sizes: NN mu, MN rho, NM rho,
+ *                 MM lambda, MM 2mu (the quantities tw_set_material_grid takes);
+ *   g_rho/vp/vs   dJ/d(padded node model of tw_set_material_model), its layout ((Mx_prmt+2) x
+ *                 (My_prmt+2)); TW_ERR_STATE when the material came from tw_set_material_grid;
+ *   g_state[5]    dJ/d(initial fields NN, MN, NM, MM0, MM1) at reference sizes.
+ * Afterwards the handle holds the state and records of tw_step(nt). Device memory for the call:
+ * (nt/ckpt_every + ckpt_every + 2) states plus 15 field-sized arrays. */
+TW_API int tw_adjoint_gradient(tw_solver *s, int nt, const double *obs, int ckpt_every, double *misfit,
+                               double *const *g_grid, double *g_rho, double *g_vp, double *g_vs,
+                               double *const *g_state);
+
 /* ---- batched shots ---------------------------------------------------------------------
  * No counterpart in the reference, which runs one shot per process. A batch advances many
  * acoustic handles (the shots: independent grids of any sizes) together: each half-step is ONE

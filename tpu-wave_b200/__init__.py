@@ -90,6 +90,7 @@ def lib() -> C.CDLL:
         L.tw_material_map_noalloc.argtypes = [vp, vp, vp, C.c_long, C.c_long, C.c_int, C.c_int, C.c_long, C.c_long,
                                               C.c_int, C.c_int, vp, vp, vp, vp, vp, vp]
         L.tw_location_to_index.argtypes = [C.c_char, C.c_long, C.c_long, C.c_int, C.c_int, lp]
+        L.tw_adjoint_gradient.argtypes = [vp, C.c_int, dp, C.c_int, dp, C.POINTER(dp), dp, dp, dp, C.POINTER(dp)]
         L.tw_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
         L.tw_batch_destroy.argtypes = [vp]
         L.tw_batch_destroy.restype = None
@@ -180,6 +181,7 @@ class Solver:
             if a.size != P:
                 raise ValueError(f"model arrays must hold (Mx_prmt+2)*(My_prmt+2) = {P} values")
         _ok(lib().tw_set_material_model(self.h, *[_dp(a) for a in arrs], Mxp, Myp, nd, dd), "tw_set_material_model")
+        self.model_shape = (Mxp + 2, Myp + 2)
 
     def set_material_grid(self, grid: int, idx: int, coef):
         a = np.ascontiguousarray(np.asarray(coef, np.float64))
@@ -273,6 +275,30 @@ class Solver:
         ms = np.zeros(4)
         _ok(lib().tw_profile(self.h, n, _dp(ms)), "tw_profile")
         return ms
+
+    def adjoint_gradient(self, nt: int, obs, ckpt_every: int = 50, model: bool = True, state: bool = False):
+        """Misfit and gradients (tw_adjoint_gradient). obs: [n_rcv, 2, nt]. Returns a dict with
+        "misfit", "grid" (NN mu, MN rho, NM rho, MM lambda, MM 2mu), and "rho", "vp", "vs" (padded
+        node model, when model=True) and "state" (initial fields, when state=True)."""
+        o = np.ascontiguousarray(np.asarray(obs, np.float64).reshape(self.n_rcv, 2, nt)) if self.n_rcv else np.zeros(1)
+        shapes = [self.shape(g) for g in (NN, MN, NM, MM, MM)]
+        grid = [np.zeros(sh) for sh in shapes]
+        garr = (C.POINTER(C.c_double) * 5)(*[_dp(g) for g in grid])
+        out = {"grid": dict(zip(("NN_mu", "MN_rho", "NM_rho", "MM_lambda", "MM_2mu"), grid))}
+        mdl = [None, None, None]
+        if model:
+            mdl = [np.zeros(self.model_shape) for _ in range(3)]
+        st = [np.zeros(sh) for sh in shapes] if state else None
+        sarr = (C.POINTER(C.c_double) * 5)(*[_dp(g) for g in st]) if state else None
+        J = C.c_double()
+        _ok(lib().tw_adjoint_gradient(self.h, nt, _dp(o), ckpt_every, C.byref(J), garr,
+                                      *[(_dp(m) if m is not None else None) for m in mdl], sarr), "tw_adjoint_gradient")
+        out["misfit"] = J.value
+        if model:
+            out["rho"], out["vp"], out["vs"] = mdl
+        if state:
+            out["state"] = dict(zip(("NN", "MN", "NM", "MM0", "MM1"), st))
+        return out
 
     def stream(self) -> int:
         p = C.c_void_p()

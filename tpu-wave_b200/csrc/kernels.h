@@ -110,6 +110,33 @@ void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, cudaStream_t 
 template <class S, class C>
 cudaError_t prepare_fused();
 
+// discrete adjoint of the elastic step (adjoint.cu)
+template <class C>
+struct AdjArgs {
+    C *lam[5];                // adjoint state (field slots), rows x pitch
+    C *w[5];                  // temporaries by slot: W_nn, Z_mn, Z_nm, W_xx, W_yy
+    const C *coef[5];         // stepping coefficients: mu, 1/rho, 1/rho, lambda, 2mu
+    const C *u0[5];           // forward state u_n (its stresses feed the 1/rho gradients)
+    const C *u1[5];           // forward state u_{n+1} (its velocities feed the mu, lambda, 2mu gradients)
+    double *g[5];             // gradients with respect to the stepping coefficients
+    long pitch;
+    int Mx, My;
+    Ops<C> op;
+    const int *rcv;           // receiver table (slot0, slot1, row, column)
+    int n_rcv;
+    const double *resid;      // residuals [n_rcv][2][nt]
+    int nt;
+};
+template <class C>
+void launch_adjoint_step(const AdjArgs<C> &a, cudaStream_t st);
+template <class C>
+void launch_adjoint_inject(const AdjArgs<C> &a, int it, cudaStream_t st);
+void launch_interp_T(int rows, int cols, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
+                     long Nx_prmt, long Ny_prmt, const double *gin, double *gnode, cudaStream_t st);
+void launch_model_derive_T(const double *rho, const double *vp, const double *vs, long n, const double *g_mu,
+                           const double *g_lam, const double *g_m2, const double *g_rho_direct, double *g_rho,
+                           double *g_vp, double *g_vs, cudaStream_t st);
+
 template <class S>
 struct GatherArgs {
     const S *f[5];

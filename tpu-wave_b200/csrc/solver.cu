@@ -12,6 +12,7 @@
 #include <cstdio>
 #include <cstring>
 #include <algorithm>
+#include <array>
 #include <new>
 #include <string>
 #include <vector>
@@ -75,6 +76,11 @@ struct tw_solver {
     int *d_done = nullptr, *d_rcv_off = nullptr, *d_rcv_list = nullptr;
     int rcv_list_cap = 0;
     double *w[5] = {}, *mat[5] = {};
+    // the padded node model of the last tw_set_material_model (rho, vp, vs), for the model gradient
+    double *model = nullptr;
+    long model_Mxp = 0, model_Myp = 0;
+    int model_ndM = 0, model_ddM = 0;
+    bool model_set = false;
     bool mat_set[5] = {};
     bool mat_dirty = true, mat_ready = false;
     double *src_inc = nullptr;
@@ -114,7 +120,7 @@ tw_solver::~tw_solver()
         cudaFree(f[k]); cudaFree(res[k]); cudaFree(coef[k]); cudaFree(w[k]); cudaFree(mat[k]);
     }
     for (int k = 0; k < 5; k++) { cudaFree(f2[k]); cudaFree(res2[k]); }
-    cudaFree(d_done); cudaFree(d_rcv_off); cudaFree(d_rcv_list);
+    cudaFree(d_done); cudaFree(d_rcv_off); cudaFree(d_rcv_list); cudaFree(model);
     cudaFree(src_inc); cudaFree(d_step); cudaFree(d_flags); cudaFree(d_rcv); cudaFree(d_err);
     cudaFree(d_traces); cudaFree(d_energy);
     if (st) cudaStreamDestroy(st);
@@ -680,6 +686,23 @@ int tw_set_material_model(tw_solver *s, const double *rho, const double *vp, con
     if ((e = cudaStreamSynchronize(s->st)) != cudaSuccess) return done(cuda_fail(e, "model"));
     if (herr) return done(TW_ERR_MODEL_BOUNDS);
     rc = finalize_material(s);
+    if (rc == TW_OK) {   // keep rho, vp, vs for the model gradient (tw_adjoint_gradient)
+        if (s->model && (s->model_Mxp != Mx_prmt || s->model_Myp != My_prmt)) {
+            cudaFree(s->model);
+            s->model = nullptr;
+        }
+        if (!s->model && (e = cudaMalloc((void **)&s->model, sizeof(double) * 3 * P)) != cudaSuccess) {
+            s->model = nullptr;
+            return done(cuda_fail(e, "model copy"));
+        }
+        if ((e = cudaMemcpyAsync(s->model, buf, sizeof(double) * 3 * P, cudaMemcpyDeviceToDevice, s->st)) != cudaSuccess)
+            return done(cuda_fail(e, "model copy"));
+        s->model_Mxp = Mx_prmt;
+        s->model_Myp = My_prmt;
+        s->model_ndM = num_dxM;
+        s->model_ddM = den_dxM;
+        s->model_set = true;
+    }
     return done(rc);
 }
 
@@ -698,6 +721,7 @@ int tw_set_material_grid(tw_solver *s, int grid, int idx, const double *coef, lo
     TW_CUDA(cudaStreamSynchronize(s->st));
     s->mat_set[slot] = true;
     s->mat_dirty = true;
+    s->model_set = false;   // the node model no longer describes the material
     bool all = true;
     for (int k = 0; k < 5; k++) all = all && (!s->has_slot(k) || s->mat_set[k]);
     if (all) {
@@ -980,6 +1004,213 @@ int tw_get_stream(tw_solver *s, void **stream)
 }
 
 }  // extern "C"
+
+// ======================================================================== adjoint gradient
+namespace {
+
+// device copy of a whole state (five field slots, rows x pitch) between the solver and a buffer
+int copy_state(tw_solver *s, void *const *dst, void *const *src)
+{
+    for (int k = 0; k < 5; k++)
+        if (s->has_slot(k))
+            TW_CUDA(cudaMemcpyAsync(dst[k], src[k], (size_t)s->rows[k] * s->pitch * s->esz, cudaMemcpyDeviceToDevice, s->st));
+    return TW_OK;
+}
+
+struct DevBuf {   // zeroed device allocations of one gradient call, freed on every exit
+    cudaStream_t st;
+    std::vector<void *> p;
+    explicit DevBuf(cudaStream_t s) : st(s) {}
+    ~DevBuf()
+    {
+        cudaStreamSynchronize(st);
+        for (void *q : p) cudaFree(q);
+    }
+    int get(void **out, size_t bytes)
+    {
+        cudaError_t e = cudaMalloc(out, bytes);
+        if (e != cudaSuccess) return cuda_fail(e, "tw_adjoint_gradient");
+        p.push_back(*out);
+        e = cudaMemsetAsync(*out, 0, bytes, st);
+        return e == cudaSuccess ? TW_OK : cuda_fail(e, "tw_adjoint_gradient");
+    }
+};
+
+template <class C>
+int adjoint_t(tw_solver *s, int nt, const double *obs, int K, double *misfit, double *const *g_grid, double *g_rho,
+              double *g_vp, double *g_vs, double *const *g_state)
+{
+    const size_t fsz[5] = {(size_t)s->rows[0] * s->pitch, (size_t)s->rows[1] * s->pitch, (size_t)s->rows[2] * s->pitch,
+                           (size_t)s->rows[3] * s->pitch, (size_t)s->rows[4] * s->pitch};
+    const int n_ck = (nt + K - 1) / K;
+    const int n_rcv = (int)(s->rcv_tab.size() / 4);
+    DevBuf mem(s->st);
+    int rc;
+    // checkpoints every K steps, the states of one segment, the final state
+    std::vector<std::array<void *, 5>> ck(n_ck), seg(K + 1);
+    std::array<void *, 5> fin{};
+    for (auto *set : {&ck, &seg})
+        for (auto &st_ : *set)
+            for (int k = 0; k < 5; k++)
+                if ((rc = mem.get(&st_[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
+    for (int k = 0; k < 5; k++)
+        if ((rc = mem.get(&fin[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
+    AdjArgs<C> a{};
+    for (int k = 0; k < 5; k++) {
+        if ((rc = mem.get((void **)&a.lam[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
+        if ((rc = mem.get((void **)&a.w[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
+        if ((rc = mem.get((void **)&a.g[k], fsz[k] * sizeof(double))) != TW_OK) return rc;
+        a.coef[k] = (const C *)s->coef[k];
+    }
+    double *d_res = nullptr;
+    if (n_rcv > 0 && (rc = mem.get((void **)&d_res, sizeof(double) * 2 * (size_t)n_rcv * nt)) != TW_OK) return rc;
+    auto cur = [&]() {
+        std::array<void *, 5> c{};
+        for (int k = 0; k < 5; k++) c[k] = cur_f(s, k);
+        return c;
+    };
+
+    // forward sweep, keeping a checkpoint every K steps
+    for (int c = 0; c < n_ck; c++) {
+        if ((rc = copy_state(s, ck[c].data(), cur().data())) != TW_OK) return rc;
+        const int n = std::min(K, nt - c * K);
+        enqueue(s, n, s->st);
+        s->steps_done += n;
+    }
+    if ((rc = copy_state(s, fin.data(), cur().data())) != TW_OK) return rc;
+    TW_CUDA(cudaGetLastError());
+    // residuals and misfit on the host (FP64)
+    std::vector<double> tr(2 * (size_t)n_rcv * nt), res(tr.size());
+    double J = 0.;
+    if (n_rcv > 0) {
+        TW_CUDA(cudaMemcpy2DAsync(tr.data(), sizeof(double) * nt, s->d_traces, sizeof(double) * s->d.max_steps,
+                                  sizeof(double) * nt, 2 * (size_t)n_rcv, cudaMemcpyDeviceToHost, s->st));
+        TW_CUDA(cudaStreamSynchronize(s->st));
+        for (int q = 0; q < n_rcv; q++)
+            for (int f = 0; f < 2; f++) {
+                const bool has = s->rcv_tab[4 * q + f] >= 0;
+                for (int it = 0; it < nt; it++) {
+                    const size_t i = (2 * (size_t)q + f) * nt + it;
+                    res[i] = has ? tr[i] - obs[i] : 0.;
+                    J += 0.5 * res[i] * res[i];
+                }
+            }
+        TW_CUDA(cudaMemcpyAsync(d_res, res.data(), sizeof(double) * res.size(), cudaMemcpyHostToDevice, s->st));
+    }
+    if (misfit) *misfit = J;
+    a.pitch = s->pitch;
+    a.Mx = (int)s->d.Mx;
+    a.My = (int)s->d.My;
+    a.op = make_ops<C>((double)s->d.num_dx / (double)s->d.den_dx, s->d.dt, false);
+    a.rcv = s->d_rcv;
+    a.n_rcv = n_rcv;
+    a.resid = d_res;
+    a.nt = nt;
+
+    // backward sweep: lam_nt = R^T r_{nt-1}; per segment, recompute its states from the
+    // checkpoint, then step the adjoint back through it
+    launch_adjoint_inject<C>(a, nt - 1, s->st);
+    for (int c = n_ck - 1; c >= 0; c--) {
+        const int k0 = c * K, k1 = std::min(nt, k0 + K);
+        if ((rc = copy_state(s, cur().data(), ck[c].data())) != TW_OK) return rc;
+        TW_CUDA(cudaMemcpyAsync(s->d_step, &k0, sizeof(int), cudaMemcpyHostToDevice, s->st));
+        if ((rc = copy_state(s, seg[0].data(), ck[c].data())) != TW_OK) return rc;
+        for (int k = k0; k < k1; k++) {
+            enqueue(s, 1, s->st);
+            if ((rc = copy_state(s, seg[k - k0 + 1].data(), cur().data())) != TW_OK) return rc;
+        }
+        for (int n = k1 - 1; n >= k0; n--) {
+            for (int k = 0; k < 5; k++) {
+                a.u0[k] = (const C *)seg[n - k0][k];
+                a.u1[k] = (const C *)seg[n + 1 - k0][k];
+            }
+            launch_adjoint_step<C>(a, s->st);
+            if (n >= 1) launch_adjoint_inject<C>(a, n - 1, s->st);
+        }
+        TW_CUDA(cudaGetLastError());
+    }
+    // leave the handle as tw_step(nt) would: the final state, the step counter at nt
+    if ((rc = copy_state(s, cur().data(), fin.data())) != TW_OK) return rc;
+    TW_CUDA(cudaMemcpyAsync(s->d_step, &nt, sizeof(int), cudaMemcpyHostToDevice, s->st));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+
+    // gradients with respect to the material on each grid: mu, rho (through 1/rho), lambda, 2mu
+    const long Mx = s->d.Mx;
+    const bool want_model = g_rho || g_vp || g_vs;
+    double *gq[5] = {};
+    for (int k = 0; k < 5; k++) {
+        const size_t n = (size_t)s->rows[k] * s->cols[k];
+        if ((rc = mem.get((void **)&gq[k], sizeof(double) * n)) != TW_OK) return rc;
+        TW_CUDA(cudaMemcpy2DAsync(gq[k], sizeof(double) * s->cols[k], a.g[k], sizeof(double) * s->pitch,
+                                  sizeof(double) * s->cols[k], s->rows[k], cudaMemcpyDeviceToDevice, s->st));
+    }
+    std::vector<double> h, m;
+    for (int k = 0; k < 5; k++) {
+        const size_t n = (size_t)s->rows[k] * s->cols[k];
+        h.resize(n);
+        TW_CUDA(cudaMemcpyAsync(h.data(), gq[k], sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
+        TW_CUDA(cudaStreamSynchronize(s->st));
+        if (k == F_MN || k == F_NM) {   // d(1/rho)/d rho = -1/rho^2 at the interpolated FP64 density
+            m.resize(n);
+            TW_CUDA(cudaMemcpyAsync(m.data(), s->mat[k], sizeof(double) * n, cudaMemcpyDeviceToHost, s->st));
+            TW_CUDA(cudaStreamSynchronize(s->st));
+            for (size_t i = 0; i < n; i++) h[i] = -h[i] / (m[i] * m[i]);
+            if (want_model) TW_CUDA(cudaMemcpyAsync(gq[k], h.data(), sizeof(double) * n, cudaMemcpyHostToDevice, s->st));
+        }
+        if (g_grid && g_grid[k]) memcpy(g_grid[k], h.data(), sizeof(double) * n);
+        TW_CUDA(cudaStreamSynchronize(s->st));
+    }
+    if (g_state)
+        for (int k = 0; k < 5; k++) {
+            if (!g_state[k]) continue;
+            std::vector<C> t((size_t)s->rows[k] * s->cols[k]);
+            TW_CUDA(cudaMemcpy2DAsync(t.data(), sizeof(C) * s->cols[k], a.lam[k], sizeof(C) * s->pitch,
+                                      sizeof(C) * s->cols[k], s->rows[k], cudaMemcpyDeviceToHost, s->st));
+            TW_CUDA(cudaStreamSynchronize(s->st));
+            for (size_t i = 0; i < t.size(); i++) g_state[k][i] = (double)t[i];
+        }
+    if (want_model) {
+        if (!s->model_set) return TW_ERR_STATE;
+        const long Nxp = s->model_Mxp + 1, Nyp = s->model_Myp + 1, P = (Nxp + 1) * (Nyp + 1);
+        double *nd = nullptr;   // node gradients: mu, lambda, 2mu, rho (direct); outputs rho, vp, vs
+        if ((rc = mem.get((void **)&nd, sizeof(double) * 7 * P)) != TW_OK) return rc;
+        double *g_mu = nd, *g_lam = nd + P, *g_m2 = nd + 2 * P, *g_r = nd + 3 * P;
+        struct { int slot, txN, tyN; double *node; } jobs[5] = {
+            {F_NN, 1, 1, g_mu}, {F_MN, 0, 1, g_r}, {F_NM, 1, 0, g_r}, {F_MM0, 0, 0, g_lam}, {F_MM1, 0, 0, g_m2}};
+        for (auto &j : jobs)
+            launch_interp_T(s->rows[j.slot], s->cols[j.slot], j.txN, j.tyN, s->d.num_dx, s->d.den_dx, s->model_ndM,
+                            s->model_ddM, Nxp, Nyp, gq[j.slot], j.node, s->st);
+        launch_model_derive_T(s->model, s->model + P, s->model + 2 * P, P, g_mu, g_lam, g_m2, g_r, nd + 4 * P,
+                              nd + 5 * P, nd + 6 * P, s->st);
+        TW_CUDA(cudaGetLastError());
+        double *outs[3] = {g_rho, g_vp, g_vs};
+        for (int q = 0; q < 3; q++)
+            if (outs[q]) TW_CUDA(cudaMemcpyAsync(outs[q], nd + (4 + q) * P, sizeof(double) * P, cudaMemcpyDeviceToHost, s->st));
+        TW_CUDA(cudaStreamSynchronize(s->st));
+    }
+    (void)Mx;
+    return TW_OK;
+}
+
+}  // namespace
+
+extern "C" int tw_adjoint_gradient(tw_solver *s, int nt, const double *obs, int ckpt_every, double *misfit,
+                                   double *const *g_grid, double *g_rho, double *g_vp, double *g_vs,
+                                   double *const *g_state)
+{
+    if (check(s) || nt < 1 || ckpt_every < 1 || (!obs && !s->rcv_tab.empty())) return TW_ERR_INVALID;
+    if (!s->elastic || s->d.cpst != TW_CPST_00 || (s->d.precision != TW_FP64 && s->d.precision != TW_FP32))
+        return TW_ERR_UNSUPPORTED;
+    if (!s->mat_ready) return TW_ERR_STATE;
+    if (s->steps_done != 0) return TW_ERR_STATE;   // the forward sweep starts at step 0
+    if (nt > s->d.max_steps) return TW_ERR_RECORD_FULL;
+    if ((g_rho || g_vp || g_vs) && !s->model_set) return TW_ERR_STATE;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    const int K = std::min(ckpt_every, nt);
+    return s->d.precision == TW_FP64 ? adjoint_t<double>(s, nt, obs, K, misfit, g_grid, g_rho, g_vp, g_vs, g_state)
+                                     : adjoint_t<float>(s, nt, obs, K, misfit, g_grid, g_rho, g_vp, g_vs, g_state);
+}
 
 // ======================================================================== batched shots
 // Many acoustic handles advanced together: one launch per half-step covers the tiles of every
