@@ -49,6 +49,11 @@ template <class C, class G>
 __device__ __forceinline__ C dxN_T(const Ops<C> &o, int Mx, int r, G w)
 {
     C v = C(0);
+    if (r >= 5 && r <= Mx - 5) {   // read only by interior rows r-2..r+1 (same order as below)
+#pragma unroll
+        for (int t = 3; t >= 0; t--) v = add(v, mul(o.st[t], w(r + 1 - t)));
+        return v;
+    }
     for (int ix = max(0, r - 4); ix <= min(Mx - 1, r + 4); ix++) {
         const C c = cN(o, Mx, ix, r);
         if (c != C(0)) v = add(v, mul(c, w(ix)));
@@ -61,6 +66,11 @@ template <class C, class G>
 __device__ __forceinline__ C dxM_T(const Ops<C> &o, int Mx, int r, G w)
 {
     C v = C(0);
+    if (r >= 5 && r <= Mx - 6) {   // read only by interior rows r-1..r+2
+#pragma unroll
+        for (int t = 3; t >= 0; t--) v = add(v, mul(o.st[t], w(r + 2 - t)));
+        return v;
+    }
     for (int ix = max(0, r - 5); ix <= min(Mx, r + 5); ix++) {
         const C c = cM(o, Mx, ix, r);
         if (c != C(0)) v = add(v, mul(c, w(ix)));
@@ -74,6 +84,11 @@ template <class C, class G>
 __device__ __forceinline__ C dyNfromM_T(const Ops<C> &o, int My, int k, G w)
 {
     C v = C(0);
+    if (k >= 2 && k <= My - 3) {   // no wrap: read by N columns k-1..k+2
+#pragma unroll
+        for (int t = 0; t < 4; t++) v = add(v, mul(o.st[t], w(k + 2 - t)));
+        return v;
+    }
 #pragma unroll
     for (int t = 0; t < 4; t++) {
         const int js[3] = {k, k - My, k + My};
@@ -96,6 +111,11 @@ template <class C, class G>
 __device__ __forceinline__ C dyMfromN_T(const Ops<C> &o, int My, int k, G w)
 {
     C v = C(0);
+    if (k >= 2 && k <= My - 2) {   // no wrap: read by M columns k-2..k+1
+#pragma unroll
+        for (int t = 0; t < 4; t++) v = add(v, mul(o.st[t], w(k + 1 - t)));
+        return v;
+    }
 #pragma unroll
     for (int t = 0; t < 4; t++) {
         // j = c - 1 + t reads N column nread(j): j = k directly, j = -1 -> My - 1, j = My + 1 -> 1

@@ -224,13 +224,12 @@ void enqueue_steps(tw_solver *s, int n, cudaStream_t st)
 void *cur_f(const tw_solver *s, int k) { return s->parity ? s->f2[k] : s->f[k]; }
 void *cur_res(const tw_solver *s, int k) { return s->parity ? s->res2[k] : s->res[k]; }
 
-// one fused elastic step from the current buffers into the other ones
+// one fused elastic step from the buffers fin (rin) into fout (rout)
 template <class S, class C>
-void enqueue_fused_step(tw_solver *s, cudaStream_t st)
+void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *const *rin, void *const *rout,
+                      cudaStream_t st)
 {
     FusedArgs<S, C> a{};
-    void **fin = s->parity ? s->f2 : s->f, **fout = s->parity ? s->f : s->f2;
-    void **rin = s->parity ? s->res2 : s->res, **rout = s->parity ? s->res : s->res2;
     for (int k = 0; k < 5; k++) {
         a.in[k] = (const S *)fin[k];
         a.out[k] = (S *)fout[k];
@@ -263,6 +262,15 @@ void enqueue_fused_step(tw_solver *s, cudaStream_t st)
     a.rcv = s->d_rcv_list;
     a.traces = s->d_traces;
     launch_fused<S, C>(a, s->d.cpst, s->d.energy != 0, st);
+}
+
+// one fused elastic step from the current buffers into the other ones
+template <class S, class C>
+void enqueue_fused_step(tw_solver *s, cudaStream_t st)
+{
+    void **fin = s->parity ? s->f2 : s->f, **fout = s->parity ? s->f : s->f2;
+    void **rin = s->parity ? s->res2 : s->res, **rout = s->parity ? s->res : s->res2;
+    enqueue_fused_io<S, C>(s, fin, fout, rin, rout, st);
     s->parity ^= 1;
 }
 
@@ -1017,22 +1025,40 @@ int copy_state(tw_solver *s, void *const *dst, void *const *src)
     return TW_OK;
 }
 
-struct DevBuf {   // zeroed device allocations of one gradient call, freed on every exit
+// device memory of one gradient call: one allocation carved into 256-byte aligned pieces
+// (sizes are summed on a first pass, then the same calls hand out the pieces), freed on exit
+struct DevBuf {
     cudaStream_t st;
-    std::vector<void *> p;
+    char *base = nullptr;
+    size_t used = 0, size = 0;
+    bool sizing = true;
     explicit DevBuf(cudaStream_t s) : st(s) {}
     ~DevBuf()
     {
         cudaStreamSynchronize(st);
-        for (void *q : p) cudaFree(q);
+        cudaFree(base);
     }
     int get(void **out, size_t bytes)
     {
-        cudaError_t e = cudaMalloc(out, bytes);
+        const size_t b = (bytes + 255) / 256 * 256;
+        if (sizing) {
+            size += b;
+            *out = nullptr;
+            return TW_OK;
+        }
+        if (used + b > size) return TW_ERR_INVALID;
+        *out = base + used;
+        used += b;
+        return TW_OK;
+    }
+    int commit()   // allocate and zero the arena, then hand out pieces in the same order
+    {
+        cudaError_t e = cudaMalloc((void **)&base, size);
+        if (e != cudaSuccess) return e == cudaErrorMemoryAllocation ? TW_ERR_NOMEM : cuda_fail(e, "tw_adjoint_gradient");
+        e = cudaMemsetAsync(base, 0, size, st);
         if (e != cudaSuccess) return cuda_fail(e, "tw_adjoint_gradient");
-        p.push_back(*out);
-        e = cudaMemsetAsync(*out, 0, bytes, st);
-        return e == cudaSuccess ? TW_OK : cuda_fail(e, "tw_adjoint_gradient");
+        sizing = false;
+        return TW_OK;
     }
 };
 
@@ -1049,21 +1075,27 @@ int adjoint_t(tw_solver *s, int nt, const double *obs, int K, double *misfit, do
     // checkpoints every K steps, the states of one segment, the final state
     std::vector<std::array<void *, 5>> ck(n_ck), seg(K + 1);
     std::array<void *, 5> fin{};
-    for (auto *set : {&ck, &seg})
-        for (auto &st_ : *set)
-            for (int k = 0; k < 5; k++)
-                if ((rc = mem.get(&st_[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
-    for (int k = 0; k < 5; k++)
-        if ((rc = mem.get(&fin[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
     AdjArgs<C> a{};
-    for (int k = 0; k < 5; k++) {
-        if ((rc = mem.get((void **)&a.lam[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
-        if ((rc = mem.get((void **)&a.w[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
-        if ((rc = mem.get((void **)&a.g[k], fsz[k] * sizeof(double))) != TW_OK) return rc;
-        a.coef[k] = (const C *)s->coef[k];
+    double *d_res = nullptr, *gq[5] = {}, *nd = nullptr;
+    const bool want_model = g_rho || g_vp || g_vs;
+    const long Pm = want_model ? (s->model_Mxp + 2) * (s->model_Myp + 2) : 0;
+    for (int pass = 0; pass < 2; pass++) {
+        for (auto *set : {&ck, &seg})
+            for (auto &st_ : *set)
+                for (int k = 0; k < 5; k++)
+                    if ((rc = mem.get(&st_[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
+        for (int k = 0; k < 5; k++) {
+            if ((rc = mem.get(&fin[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
+            if ((rc = mem.get((void **)&a.lam[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
+            if ((rc = mem.get((void **)&a.w[k], fsz[k] * sizeof(C))) != TW_OK) return rc;
+            if ((rc = mem.get((void **)&a.g[k], fsz[k] * sizeof(double))) != TW_OK) return rc;
+            if ((rc = mem.get((void **)&gq[k], sizeof(double) * s->rows[k] * s->cols[k])) != TW_OK) return rc;
+        }
+        if (n_rcv > 0 && (rc = mem.get((void **)&d_res, sizeof(double) * 2 * (size_t)n_rcv * nt)) != TW_OK) return rc;
+        if (want_model && (rc = mem.get((void **)&nd, sizeof(double) * 7 * Pm)) != TW_OK) return rc;
+        if (pass == 0 && (rc = mem.commit()) != TW_OK) return rc;
     }
-    double *d_res = nullptr;
-    if (n_rcv > 0 && (rc = mem.get((void **)&d_res, sizeof(double) * 2 * (size_t)n_rcv * nt)) != TW_OK) return rc;
+    for (int k = 0; k < 5; k++) a.coef[k] = (const C *)s->coef[k];
     auto cur = [&]() {
         std::array<void *, 5> c{};
         for (int k = 0; k < 5; k++) c[k] = cur_f(s, k);
@@ -1112,13 +1144,11 @@ int adjoint_t(tw_solver *s, int nt, const double *obs, int K, double *misfit, do
     launch_adjoint_inject<C>(a, nt - 1, s->st);
     for (int c = n_ck - 1; c >= 0; c--) {
         const int k0 = c * K, k1 = std::min(nt, k0 + K);
-        if ((rc = copy_state(s, cur().data(), ck[c].data())) != TW_OK) return rc;
         TW_CUDA(cudaMemcpyAsync(s->d_step, &k0, sizeof(int), cudaMemcpyHostToDevice, s->st));
         if ((rc = copy_state(s, seg[0].data(), ck[c].data())) != TW_OK) return rc;
-        for (int k = k0; k < k1; k++) {
-            enqueue(s, 1, s->st);
-            if ((rc = copy_state(s, seg[k - k0 + 1].data(), cur().data())) != TW_OK) return rc;
-        }
+        void *const none[5] = {};
+        for (int k = k0; k < k1; k++)   // step k: segment state k - k0 -> k - k0 + 1
+            enqueue_fused_io<C, C>(s, seg[k - k0].data(), seg[k - k0 + 1].data(), none, none, s->st);
         for (int n = k1 - 1; n >= k0; n--) {
             for (int k = 0; k < 5; k++) {
                 a.u0[k] = (const C *)seg[n - k0][k];
@@ -1135,12 +1165,7 @@ int adjoint_t(tw_solver *s, int nt, const double *obs, int K, double *misfit, do
     TW_CUDA(cudaStreamSynchronize(s->st));
 
     // gradients with respect to the material on each grid: mu, rho (through 1/rho), lambda, 2mu
-    const long Mx = s->d.Mx;
-    const bool want_model = g_rho || g_vp || g_vs;
-    double *gq[5] = {};
     for (int k = 0; k < 5; k++) {
-        const size_t n = (size_t)s->rows[k] * s->cols[k];
-        if ((rc = mem.get((void **)&gq[k], sizeof(double) * n)) != TW_OK) return rc;
         TW_CUDA(cudaMemcpy2DAsync(gq[k], sizeof(double) * s->cols[k], a.g[k], sizeof(double) * s->pitch,
                                   sizeof(double) * s->cols[k], s->rows[k], cudaMemcpyDeviceToDevice, s->st));
     }
@@ -1172,8 +1197,7 @@ int adjoint_t(tw_solver *s, int nt, const double *obs, int K, double *misfit, do
     if (want_model) {
         if (!s->model_set) return TW_ERR_STATE;
         const long Nxp = s->model_Mxp + 1, Nyp = s->model_Myp + 1, P = (Nxp + 1) * (Nyp + 1);
-        double *nd = nullptr;   // node gradients: mu, lambda, 2mu, rho (direct); outputs rho, vp, vs
-        if ((rc = mem.get((void **)&nd, sizeof(double) * 7 * P)) != TW_OK) return rc;
+        // node gradients nd: mu, lambda, 2mu, rho (direct); then the outputs rho, vp, vs
         double *g_mu = nd, *g_lam = nd + P, *g_m2 = nd + 2 * P, *g_r = nd + 3 * P;
         struct { int slot, txN, tyN; double *node; } jobs[5] = {
             {F_NN, 1, 1, g_mu}, {F_MN, 0, 1, g_r}, {F_NM, 1, 0, g_r}, {F_MM0, 0, 0, g_lam}, {F_MM1, 0, 0, g_m2}};
@@ -1188,7 +1212,6 @@ int adjoint_t(tw_solver *s, int nt, const double *obs, int K, double *misfit, do
             if (outs[q]) TW_CUDA(cudaMemcpyAsync(outs[q], nd + (4 + q) * P, sizeof(double) * P, cudaMemcpyDeviceToHost, s->st));
         TW_CUDA(cudaStreamSynchronize(s->st));
     }
-    (void)Mx;
     return TW_OK;
 }
 
