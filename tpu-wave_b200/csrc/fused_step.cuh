@@ -653,11 +653,12 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, TW_FS_MIN_BLOCKS) k_elastic_fu
     const int cta = blockIdx.x;
     const int rcv_b = a.rcv_off[cta], rcv_e = a.rcv_off[cta + 1];
     EAcc E;
-    const int n_int = a.n_int_seg * a.n_int_x;
-    if (cta < n_int) {   // interior CTA (segment, group of FS_WARPS warp strips)
-        const int seg = cta / a.n_int_x, wstrip = (cta % a.n_int_x) * FS_WARPS + (threadIdx.x >> 5);
-        const int y0 = wstrip * FS_WARP_CORE;
-        if (wstrip < a.n_wstrip) {
+    const int n_int = a.n_int_cta;
+    if (cta < n_int) {   // interior CTA: FS_WARPS consecutive (segment, strip) warps, segment-major
+        const int gw = cta * FS_WARPS + (threadIdx.x >> 5);
+        if (gw < a.n_int_seg * a.n_wstrip) {
+            const int seg = gw / a.n_wstrip, wstrip = gw - seg * a.n_wstrip;
+            const int y0 = wstrip * FS_WARP_CORE;
             if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false>(a, wstrip, seg, it, rcv_b, rcv_e, E);
             else interior_warp<S, C, CPST, ENERGY, true>(a, wstrip, seg, it, rcv_b, rcv_e, E);
         }
@@ -737,7 +738,7 @@ cudaError_t prepare_fused()
 template <class S, class C>
 void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, cudaStream_t st)
 {
-    const dim3 grid(a.n_int_seg * a.n_int_x + a.n_zone * a.n_bstrip), block(FS_THREADS_MAX);
+    const dim3 grid(a.n_int_cta + a.n_zone * a.n_bstrip), block(FS_THREADS_MAX);
     const size_t smem = fused_smem_bytes<S, C>(a.tile_rows);
 #define TW_FUSED_CASE(N)                                                              \
     case N:                                                                           \

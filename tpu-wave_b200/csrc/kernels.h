@@ -90,7 +90,7 @@ struct FusedArgs {
     int n_int_seg, int_rows;  // interior rows [FS_ZONE, Mx - FS_ZONE) = int_rows, in n_int_seg balanced segments
     int n_zone;               // 2 boundary zones, or 1 zone holding the whole grid
     int n_wstrip, n_bstrip;   // interior warp strips, boundary strips
-    int n_int_x;              // interior CTAs per segment (groups of FS_WARPS warp strips)
+    int n_int_cta;            // interior CTAs: the n_int_seg x n_wstrip warps, FS_WARPS per CTA
     int tile_rows;
     const double *src_inc;
     int src_grid, src_ix, src_iy;

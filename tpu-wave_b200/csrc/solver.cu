@@ -72,7 +72,7 @@ struct tw_solver {
     bool fused = false;
     void *f2[5] = {}, *res2[5] = {};
     int parity = 0;                   // which buffer holds the current state (0: f/res, 1: f2/res2)
-    int n_int_seg = 0, int_rows = 0, n_zone = 1, n_wstrip = 0, n_bstrip = 1, n_int_x = 0, tile_rows = 1;
+    int n_int_seg = 0, int_rows = 0, n_zone = 1, n_wstrip = 0, n_bstrip = 1, n_int_cta = 0, tile_rows = 1;
     int *d_done = nullptr, *d_rcv_off = nullptr, *d_rcv_list = nullptr;
     int rcv_list_cap = 0;
     double *w[5] = {}, *mat[5] = {};
@@ -247,7 +247,7 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
     a.n_zone = s->n_zone;
     a.n_wstrip = s->n_wstrip;
     a.n_bstrip = s->n_bstrip;
-    a.n_int_x = s->n_int_x;
+    a.n_int_cta = s->n_int_cta;
     a.tile_rows = s->tile_rows;
     a.src_inc = s->src_inc;
     a.src_grid = s->src_grid;
@@ -395,7 +395,7 @@ int upload_receivers(tw_solver *s)
     if (s->fused) {
         // per-CTA receiver lists: a receiver belongs to the CTA whose segment owns its row and
         // whose strip owns its column (fused_step.cu)
-        const int n_int = s->n_int_seg * s->n_int_x;
+        const int n_int = s->n_int_cta;
         const int nctas = n_int + s->n_zone * s->n_bstrip;
         std::vector<std::vector<int>> per(nctas);
         const int Mx = (int)s->d.Mx;
@@ -409,7 +409,7 @@ int upload_receivers(tw_solver *s)
             } else {
                 int seg = 0;   // the balanced segment holding the row (fused_step.cu)
                 while (FS_ZONE + (int)((long)(seg + 1) * s->int_rows / s->n_int_seg) <= row) seg++;
-                cta = seg * s->n_int_x + col / FS_WARP_CORE / FS_WARPS;
+                cta = (seg * s->n_wstrip + col / FS_WARP_CORE) / FS_WARPS;
             }
             for (int f = 0; f < 2; f++)
                 if (q[f] >= 0) per[cta].insert(per[cta].end(), {q[f], row, col, 2 * r + f});
@@ -613,18 +613,17 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
             s->n_zone = 1;
             s->tile_rows = (int)Mx + 1;
         } else {
-            // interior segments sized for about two 8-warp CTAs per SM of a 148-SM B200, at least
-            // 8 rows each, the last one taking the remainder
+            // balanced interior segments: TW_FS_CTAS_PER_SM CTAs of work for each of the 148 SMs,
+            // the boundary CTAs included, segments of 8 rows or more; the segment x strip warps are
+            // packed FS_WARPS to a CTA
             s->n_zone = 2;
             s->tile_rows = 12;
-            s->n_int_x = (s->n_wstrip + FS_WARPS - 1) / FS_WARPS;
             s->int_rows = (int)Mx - 2 * FS_ZONE;
-            // one wave of TW_FS_CTAS_PER_SM CTAs on each of the 148 SMs, the boundary CTAs
-            // included; segments of 8 rows or more
-            const int target = std::max(1, (148 * TW_FS_CTAS_PER_SM - 2 * s->n_bstrip) / s->n_int_x);
+            const int target = std::max(1, (148 * TW_FS_CTAS_PER_SM - 2 * s->n_bstrip) * FS_WARPS / s->n_wstrip);
             s->n_int_seg = std::max(1, std::min(target, s->int_rows / 8));
+            s->n_int_cta = (s->n_int_seg * s->n_wstrip + FS_WARPS - 1) / FS_WARPS;
         }
-        const int nctas = s->n_int_seg * s->n_int_x + s->n_zone * s->n_bstrip;
+        const int nctas = s->n_int_cta + s->n_zone * s->n_bstrip;
         if ((rc_ = s->alloc((void **)&s->d_done, sizeof(int))) != TW_OK) return fail(rc_);
         cudaMemsetAsync(s->d_done, 0, sizeof(int), s->st);
         if ((rc_ = s->alloc((void **)&s->d_rcv_off, sizeof(int) * (nctas + 1))) != TW_OK) return fail(rc_);
