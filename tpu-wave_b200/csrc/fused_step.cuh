@@ -124,6 +124,43 @@ struct Row {   // global values one interior iteration consumes
     P2<double> wmn, wnm, wnn, wm3, wm4;
 };
 
+// ---- per-lane row staging through shared memory
+// Each interior warp owns a ring of RING_DEPTH row stages in shared memory. A lane copies the
+// values it will need for a row asynchronously (cp.async) into its own slots a few rows ahead and
+// reads them back when the row comes up: the copies need no registers while in flight, and as a
+// lane only ever reads what it copied itself, no warp or block barrier is involved.
+template <class C, bool ENERGY>
+constexpr int ring_depth() { return (sizeof(C) == 8 || ENERGY) ? 2 : TW_FS_RING; }
+
+template <class S, class C, int CPST, bool ENERGY>
+struct RingLayout {
+    static constexpr bool KR = Cpst<CPST>::keep_r, KC = Cpst<CPST>::keep_c, SPLIT = Cpst<CPST>::split;
+    // slots of the storage type: nn, mm0, mm1, vmn, vnm; their lo parts (split); the residuals
+    // rmn, rnm, rnn, rm0, rm1 (R and C codes)
+    static constexpr int NS = 5 + (SPLIT ? 5 : 0) + ((KR || KC) ? 5 : 0);
+    static constexpr int NC = 5;                      // pmn, pnm, mu, lam, m2
+    static constexpr int NE = ENERGY ? 5 : 0;         // wmn, wnm, wnn, wm3, wm4 (double)
+    static constexpr int s_bytes = 32 * 2 * (int)sizeof(S), c_bytes = 32 * 2 * (int)sizeof(C), e_bytes = 32 * 16;
+    static constexpr int stage = NS * s_bytes + NC * c_bytes + NE * e_bytes;
+    static constexpr int warp = stage * ring_depth<C, ENERGY>();
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+// copy `bytes` (4, 8 or 16) from global to shared memory asynchronously; pred false: zero fill
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void *dst, const void *src, bool pred)
+{
+    if constexpr (BYTES == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(smem_u32(dst)), "l"(src), "r"(pred ? 16 : 0) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(smem_u32(dst)), "l"(src), "n"(BYTES), "r"(pred ? BYTES : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 }  // namespace
 
 // ------------------------------------------------------------------------------- interior warp
@@ -131,7 +168,8 @@ struct Row {   // global values one interior iteration consumes
 // physical columns, unowned columns or the seam; otherwise every pair is adjacent, aligned and
 // owned by the core lanes, and loads and stores are single vector accesses
 template <class S, class C, int CPST, bool ENERGY, bool EDGE>
-__device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int it, int rcv_b, int rcv_e, EAcc &E)
+__device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int it, int rcv_b, int rcv_e, EAcc &E,
+                              unsigned char *ring)
 {
     constexpr bool KR = Cpst<CPST>::keep_r, KC = Cpst<CPST>::keep_c, SPLIT = Cpst<CPST>::split;
     const int lane = threadIdx.x & 31;
@@ -177,38 +215,116 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
         }
         return v;
     };
-    auto fetch = [&](int j, Row<C> &in) {
-        in.nn = ld2f(F_NN, j + 2, pN0, pN1);
-        in.mm0 = ld2f(F_MM0, j + 1, pM0, pM1);
-        in.mm1 = ld2f(F_MM1, j, pM0, pM1);
-        in.vmn = ld2f(F_MN, j, pN0, pN1);
-        in.vnm = ld2f(F_NM, j, pM0, pM1);
-        in.pmn = ldg2(a.coef[F_MN] + j * pitch, pN0, pN1);
-        in.pnm = ldg2(a.coef[F_NM] + j * pitch, pM0, pM1);
-        if (KR || KC) {
-            in.rmn = ld2(rowp(a.rin[F_MN], j), pN0, pN1);
-            in.rnm = ld2(rowp(a.rin[F_NM], j), pM0, pM1);
+    // ---- row staging: issue(j, st) copies row j's values into ring stage st, read(st, in)
+    // converts them into `in`
+    using RL = RingLayout<S, C, CPST, ENERGY>;
+    constexpr int D = ring_depth<C, ENERGY>();
+    const int l = lane;
+    auto sslot = [&](int st, int k) { return ring + st * RL::stage + k * RL::s_bytes + l * 2 * (int)sizeof(S); };
+    auto cslot = [&](int st, int k) { return ring + st * RL::stage + RL::NS * RL::s_bytes + k * RL::c_bytes + l * 2 * (int)sizeof(C); };
+    auto eslot = [&](int st, int k) {
+        return ring + st * RL::stage + RL::NS * RL::s_bytes + RL::NC * RL::c_bytes + k * RL::e_bytes + l * 16;
+    };
+    // one pair of T at columns (pa, pb) of `row` into dst
+    auto put2 = [&](unsigned char *dst, const auto *row, int pa, int pb, bool pred) {
+        using T = typename std::remove_cv<typename std::remove_pointer<decltype(row)>::type>::type;
+        if (!EDGE) {
+            cp_async<2 * (int)sizeof(T)>(dst, row + c0, pred);
+        } else if constexpr (sizeof(T) >= 4) {
+            cp_async<(int)sizeof(T)>(dst, row + pa, pred);
+            cp_async<(int)sizeof(T)>(dst + sizeof(T), row + pb, pred);
+        } else {   // 16-bit elements: too small for cp.async, staged through registers
+            T *d = reinterpret_cast<T *>(dst);
+            d[0] = pred ? row[pa] : T(0.f);
+            d[1] = pred ? row[pb] : T(0.f);
+        }
+    };
+    auto issue = [&](int j, int st) {
+        put2(sslot(st, 0), rowp(a.in[F_NN], j + 2), pN0, pN1, true);
+        put2(sslot(st, 1), rowp(a.in[F_MM0], j + 1), pM0, pM1, true);
+        put2(sslot(st, 2), rowp(a.in[F_MM1], j), pM0, pM1, true);
+        put2(sslot(st, 3), rowp(a.in[F_MN], j), pN0, pN1, true);
+        put2(sslot(st, 4), rowp(a.in[F_NM], j), pM0, pM1, true);
+        int k = 5;
+        if constexpr (SPLIT) {
+            put2(sslot(st, 5), rowp(a.rin[F_NN], j + 2), pN0, pN1, true);
+            put2(sslot(st, 6), rowp(a.rin[F_MM0], j + 1), pM0, pM1, true);
+            put2(sslot(st, 7), rowp(a.rin[F_MM1], j), pM0, pM1, true);
+            put2(sslot(st, 8), rowp(a.rin[F_MN], j), pN0, pN1, true);
+            put2(sslot(st, 9), rowp(a.rin[F_NM], j), pM0, pM1, true);
+            k = 10;
         }
         const int i = j - 2;
-        if (core && i >= x0 && i < x1) {
-            in.mu = ldg2(a.coef[F_NN] + i * pitch, pN0, pN1);
-            in.lam = ldg2(a.coef[F_MM0] + i * pitch, pM0, pM1);
-            in.m2 = ldg2(a.coef[F_MM1] + i * pitch, pM0, pM1);
-            if (KR || KC) {
-                in.rnn = ld2(rowp(a.rin[F_NN], i), pN0, pN1);
-                in.rm0 = ld2(rowp(a.rin[F_MM0], i), pM0, pM1);
-                in.rm1 = ld2(rowp(a.rin[F_MM1], i), pM0, pM1);
-            }
-            if (ENERGY) {
-                in.wnn = ldg2(a.w[F_NN] + i * pitch, pN0, pN1);
-                in.wm3 = ldg2(a.w[F_MM0] + i * pitch, pM0, pM1);
-                in.wm4 = ldg2(a.w[F_MM1] + i * pitch, pM0, pM1);
-            }
+        const bool srow = core && i >= x0 && i < x1;
+        if constexpr (KR || KC) {
+            put2(sslot(st, k + 0), rowp(a.rin[F_MN], j), pN0, pN1, true);
+            put2(sslot(st, k + 1), rowp(a.rin[F_NM], j), pM0, pM1, true);
+            put2(sslot(st, k + 2), rowp(a.rin[F_NN], i), pN0, pN1, srow);
+            put2(sslot(st, k + 3), rowp(a.rin[F_MM0], i), pM0, pM1, srow);
+            put2(sslot(st, k + 4), rowp(a.rin[F_MM1], i), pM0, pM1, srow);
         }
-        if (ENERGY && core && j >= x0 && j < x1) {
-            in.wmn = ldg2(a.w[F_MN] + j * pitch, pN0, pN1);
-            in.wnm = ldg2(a.w[F_NM] + j * pitch, pM0, pM1);
+        put2(cslot(st, 0), a.coef[F_MN] + j * pitch, pN0, pN1, true);
+        put2(cslot(st, 1), a.coef[F_NM] + j * pitch, pM0, pM1, true);
+        put2(cslot(st, 2), a.coef[F_NN] + i * pitch, pN0, pN1, srow);
+        put2(cslot(st, 3), a.coef[F_MM0] + i * pitch, pM0, pM1, srow);
+        put2(cslot(st, 4), a.coef[F_MM1] + i * pitch, pM0, pM1, srow);
+        if constexpr (ENERGY) {
+            const bool vrow = core && j >= x0 && j < x1;
+            put2(eslot(st, 0), a.w[F_MN] + j * pitch, pN0, pN1, vrow);
+            put2(eslot(st, 1), a.w[F_NM] + j * pitch, pM0, pM1, vrow);
+            put2(eslot(st, 2), a.w[F_NN] + i * pitch, pN0, pN1, srow);
+            put2(eslot(st, 3), a.w[F_MM0] + i * pitch, pM0, pM1, srow);
+            put2(eslot(st, 4), a.w[F_MM1] + i * pitch, pM0, pM1, srow);
         }
+    };
+    auto rdS = [&](int st, int k) {
+        const typename Vec2<S>::T v = *reinterpret_cast<const typename Vec2<S>::T *>(sslot(st, k));
+        return P2<C>{to_c<C>(v.x), to_c<C>(v.y)};
+    };
+    auto rdC = [&](int st, int k) {
+        const typename Vec2<C>::T v = *reinterpret_cast<const typename Vec2<C>::T *>(cslot(st, k));
+        return P2<C>{v.x, v.y};
+    };
+    auto rdF = [&](int st, int k) {   // a field pair as the stencil reads it
+        P2<C> v = rdS(st, k);
+        if constexpr (SPLIT) {
+            const P2<C> lo = rdS(st, k + 5);
+            v.a = add(v.a, lo.a);
+            v.b = add(v.b, lo.b);
+        }
+        return v;
+    };
+    auto read = [&](int st, int j, Row<C> &in) {
+        in.nn = rdF(st, 0);
+        in.mm0 = rdF(st, 1);
+        in.mm1 = rdF(st, 2);
+        in.vmn = rdF(st, 3);
+        in.vnm = rdF(st, 4);
+        if constexpr (KR || KC) {
+            constexpr int k = SPLIT ? 10 : 5;
+            in.rmn = rdS(st, k + 0);
+            in.rnm = rdS(st, k + 1);
+            in.rnn = rdS(st, k + 2);
+            in.rm0 = rdS(st, k + 3);
+            in.rm1 = rdS(st, k + 4);
+        }
+        in.pmn = rdC(st, 0);
+        in.pnm = rdC(st, 1);
+        in.mu = rdC(st, 2);
+        in.lam = rdC(st, 3);
+        in.m2 = rdC(st, 4);
+        if constexpr (ENERGY) {
+            auto rdE = [&](int k) {
+                const double2 v = *reinterpret_cast<const double2 *>(eslot(st, k));
+                return P2<double>{v.x, v.y};
+            };
+            in.wmn = rdE(0);
+            in.wnm = rdE(1);
+            in.wnn = rdE(2);
+            in.wm3 = rdE(3);
+            in.wm4 = rdE(4);
+        }
+        (void)j;
     };
 
     // this lane's receivers (at most RC of them in registers; more fall back to the CTA list)
@@ -288,11 +404,20 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
     for (int q = 0; q < 3; q++) M0w[q] = ld2f(F_MM0, jb - 2 + q, pM0, pM1);
 #pragma unroll
     for (int q = 0; q < 2; q++) M1w[q] = ld2f(F_MM1, jb - 2 + q, pM0, pM1);
-    Row<C> cur, nxt;
-    fetch(jb, nxt);
+    Row<C> cur;
+#pragma unroll
+    for (int q = 0; q < D - 1; q++) {   // the first D - 1 rows in flight
+        if (jb + q <= je) issue(jb + q, q);
+        cp_async_commit();
+    }
+    int sr = 0;   // ring stage of row j
     for (int j = jb; j <= je; j++) {
-        cur = nxt;
-        if (j < je) fetch(j + 1, nxt);
+        // row j + D - 1 goes into the stage row j - 1 used (read in the previous iteration)
+        if (j + D - 1 <= je) issue(j + D - 1, sr == 0 ? D - 1 : sr - 1);
+        cp_async_commit();
+        cp_async_wait<D - 1>();   // row j has landed
+        read(sr, j, cur);
+        sr = sr + 1 == D ? 0 : sr + 1;
         NNw[4] = cur.nn;
         M0w[3] = cur.mm0;
         M1w[2] = cur.mm1;
@@ -474,6 +599,7 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
 #pragma unroll
         for (int q = 0; q < 3; q++) NMw[q] = NMw[q + 1];
     }
+    cp_async_wait_all();
 }
 
 // ------------------------------------------------------------------------------- boundary CTA
@@ -646,7 +772,7 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
 
 // ------------------------------------------------------------------------------- the launch
 template <class S, class C, int CPST, bool ENERGY>
-__global__ void __launch_bounds__(FS_THREADS_MAX, TW_FS_MIN_BLOCKS) k_elastic_fused(FusedArgs<S, C> a)
+__global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 4 : TW_FS_MIN_BLOCKS) k_elastic_fused(FusedArgs<S, C> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int it = *a.step;
@@ -659,8 +785,9 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, TW_FS_MIN_BLOCKS) k_elastic_fu
         if (gw < a.n_int_seg * a.n_wstrip) {
             const int seg = gw / a.n_wstrip, wstrip = gw - seg * a.n_wstrip;
             const int y0 = wstrip * FS_WARP_CORE;
-            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false>(a, wstrip, seg, it, rcv_b, rcv_e, E);
-            else interior_warp<S, C, CPST, ENERGY, true>(a, wstrip, seg, it, rcv_b, rcv_e, E);
+            unsigned char *ring = smem_raw + (threadIdx.x >> 5) * RingLayout<S, C, CPST, ENERGY>::warp;
+            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
+            else interior_warp<S, C, CPST, ENERGY, true>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
         }
     } else {             // boundary CTA (zone, strip)
         const int b = cta - n_int;
@@ -698,28 +825,34 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, TW_FS_MIN_BLOCKS) k_elastic_fu
 }
 
 // ------------------------------------------------------------------------------- launcher
+// dynamic shared memory: the boundary CTAs' velocity tile or the interior warps' rings
+template <class S, class C, int CPST, bool ENERGY>
+size_t fused_smem_bytes(int tile_rows)
+{
+    const size_t tile = sizeof(C) * 2 * (size_t)tile_rows * FS_BND_W;
+    const size_t rings = (size_t)FS_WARPS * RingLayout<S, C, CPST, ENERGY>::warp;
+    return tile > rings ? tile : rings;
+}
+
 namespace {
 template <class S, class C, int N>
-cudaError_t set_attr(int smem)
+cudaError_t set_attr(int)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)fused_smem_bytes<S, C, N, true>(FS_SMALL_MX + 1));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_elastic_fused<S, C, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    return cudaFuncSetAttribute(k_elastic_fused<S, C, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)fused_smem_bytes<S, C, N, false>(FS_SMALL_MX + 1));
 }
 }  // namespace
 
-template <class S, class C>
-size_t fused_smem_bytes(int tile_rows)
-{
-    return sizeof(C) * 2 * (size_t)tile_rows * FS_BND_W;
-}
 
 // shared-memory opt-in for every variant at the largest tile; called at handle creation,
 // outside any stream capture
 template <class S, class C>
 cudaError_t prepare_fused()
 {
-    const int smem = (int)fused_smem_bytes<S, C>(FS_SMALL_MX + 1);
+    const int smem = 0;
     cudaError_t e;
     if constexpr (sizeof(S) < sizeof(C)) {   // 16-bit storage: plain or split
         if ((e = set_attr<S, C, 0>(smem)) != cudaSuccess) return e;
@@ -739,11 +872,10 @@ template <class S, class C>
 void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, cudaStream_t st)
 {
     const dim3 grid(a.n_int_cta + a.n_zone * a.n_bstrip), block(FS_THREADS_MAX);
-    const size_t smem = fused_smem_bytes<S, C>(a.tile_rows);
-#define TW_FUSED_CASE(N)                                                              \
-    case N:                                                                           \
-        if (energy) k_elastic_fused<S, C, N, true><<<grid, block, smem, st>>>(a);    \
-        else k_elastic_fused<S, C, N, false><<<grid, block, smem, st>>>(a);          \
+#define TW_FUSED_CASE(N)                                                                                  \
+    case N:                                                                                               \
+        if (energy) k_elastic_fused<S, C, N, true><<<grid, block, fused_smem_bytes<S, C, N, true>(a.tile_rows), st>>>(a); \
+        else k_elastic_fused<S, C, N, false><<<grid, block, fused_smem_bytes<S, C, N, false>(a.tile_rows), st>>>(a);     \
         break;
     if constexpr (sizeof(S) < sizeof(C)) {
         switch (cpst) {

@@ -62,10 +62,13 @@ void launch_energy(const EnergyArgs<S, C> &e, cudaStream_t st);
 #define TW_FS_WARPS 4                 // warps per interior CTA
 #endif
 #ifndef TW_FS_MIN_BLOCKS
-#define TW_FS_MIN_BLOCKS 4            // CTAs per SM the register allocation is sized for
+#define TW_FS_MIN_BLOCKS 5            // CTAs per SM the register allocation is sized for
 #endif
 #ifndef TW_FS_CTAS_PER_SM
-#define TW_FS_CTAS_PER_SM 8           // CTAs per SM the row segmentation aims at (two waves)
+#define TW_FS_CTAS_PER_SM 15          // CTAs per SM the row segmentation aims at (three waves)
+#endif
+#ifndef TW_FS_RING
+#define TW_FS_RING 3                  // rows staged ahead per interior warp (FP64: 2)
 #endif
 constexpr int FS_WARP_CORE = 56;      // 28 core lanes x 2 columns; 2 halo lanes on each side
 constexpr int FS_WARPS = TW_FS_WARPS;
