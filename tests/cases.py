@@ -125,12 +125,13 @@ def product_elastic(case, precision, acoustic=False, fields0=None, resid0=None, 
         s.close()
 
 
-def product_acoustic_periodic(case, precision, fields0=None, resid0=None):
+def product_acoustic_periodic(case, precision, fields0=None, resid0=None, energy=True):
+    """energy=False runs the fused one-launch step (the energy records need the two-launch path)."""
     tw = load_twave()
     cp = {"0": "00", "3": "3R", "6": "6R"}[case.cpst]
     s = tw.Solver(case.Nx, case.Ny, 1, max(case.Nx, case.Ny), case.dt, physics=tw.ACOUSTIC, bc_x=tw.PERIODIC,
                   precision=precision, cpst=cp, central_f=case.central_f, time_delay=case.time_delay,
-                  max_steps=max(case.Nt, 1))
+                  max_steps=max(case.Nt, 1), energy=energy)
     try:
         # Vx (N in x) is the NM grid, Vy (N in y) the MN grid
         s.set_material_grid(tw.NM, 0, case.rho_vx)
@@ -150,7 +151,10 @@ def product_acoustic_periodic(case, precision, fields0=None, resid0=None):
         s.run(case.Nt)
         out = {"fields": {"Vx": s.read_field(tw.NM), "Vy": s.read_field(tw.MN), "P": s.read_field(tw.MM)},
                "traces": s.read_receivers()[:, 0, :]}
-        out["E_k"], out["E_p0"], out["E_p1"] = s.read_energy()
+        if energy:
+            out["E_k"], out["E_p0"], out["E_p1"] = s.read_energy()
+        if resid0 is not None:
+            out["resid"] = [s.read_resid(g) for g in slots]
         return out
     finally:
         s.close()

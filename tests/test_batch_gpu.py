@@ -68,13 +68,15 @@ def test_batch_equals_each_shot_alone_and_the_oracle(cpst, prec):
 
 @pytest.mark.parametrize("shape", [(32, 8, 1, 0), (64, 4, 2, 0), (128, 2, 4, 3), (256, 1, 1, 1), (32, 1, 3, 7)])
 def test_every_launch_shape_gives_the_same_result(shape):
+    """Free-surface shots use the tiled per-point kernels, whose launch shape is free."""
     tw = load_twave()
     cases = [acoustic_periodic_case(nx, ny, seed=7 + k, cpst="6", Nt=20) for k, (nx, ny) in enumerate(SIZES)]
-    ref_shots = [make_shot(tw, c, "f32") for c in cases]
-    b0 = tw.Batch(ref_shots)
-    b0.run(20)
+    ref_shots = [make_shot(tw, c, "f32", bc_x=tw.SAT_FREE) for c in cases]
+    for s in ref_shots:
+        s.run(20)
     ref = [state(tw, s) for s in ref_shots]
-    shots = [make_shot(tw, c, "f32") for c in cases]
+    b0 = None
+    shots = [make_shot(tw, c, "f32", bc_x=tw.SAT_FREE) for c in cases]
     b = tw.Batch(shots)
     b.set_shape(*shape)
     assert b.shape() == shape[:3] + ((shape[3] or b.shape()[3]),)
@@ -86,7 +88,34 @@ def test_every_launch_shape_gives_the_same_result(shape):
         for a, w in zip(f, r[0]):
             assert np.array_equal(a, w)
         assert np.array_equal(t, r[1])
-    for h in [b, b0] + shots + ref_shots:
+    for h in [b] + shots + ref_shots:
+        h.close()
+
+
+@pytest.mark.parametrize("per_sm", [1, 3, 15, 40])
+def test_fused_batch_segmentation_gives_the_same_result(per_sm):
+    """Periodic shots step with the fused kernel; its segmentation target changes nothing."""
+    tw = load_twave()
+    cases = [acoustic_periodic_case(nx, ny, seed=17 + k, cpst="3", Nt=21) for k, (nx, ny) in enumerate(SIZES)]
+    ref = []
+    for c in cases:
+        s = make_shot(tw, c, "f32")
+        s.run(21)
+        ref.append(state(tw, s))
+        s.close()
+    shots = [make_shot(tw, c, "f32") for c in cases]
+    b = tw.Batch(shots)
+    b.set_shape(0, 0, 0, per_sm)
+    assert b.shape()[2] == per_sm
+    b.step(16)
+    b.step(5)
+    b.sync()
+    for s, r in zip(shots, ref):
+        f, t = state(tw, s)
+        for a, w in zip(f, r[0]):
+            assert np.array_equal(a, w)
+        assert np.array_equal(t, r[1])
+    for h in [b] + shots:
         h.close()
 
 

@@ -110,6 +110,34 @@ struct FusedArgs {
 };
 template <class S, class C>
 void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, cudaStream_t st);
+
+// fused periodic acoustic step (acoustic_fused.cu): one shot, or a batch of shots in one launch
+template <class S, class C>
+struct AcShot {
+    const S *in[5];           // state before the step (slots F_MN Vy, F_NM Vx, F_MM0 pressure)
+    S *out[5];                // state after the step
+    const S *rin[5];          // residual arrays ('3' / '6' codes)
+    S *rout[5];
+    const C *coef[5];         // 1/rho of Vy and Vx, kappa
+    long pitch;
+    int Mx, My;
+    Ops<C> op;
+    int n_seg, n_wstrip;      // the shot's warps: n_seg row segments x n_wstrip column strips,
+    int warp_off;             // numbered from warp_off within the launch
+    const double *src_inc;
+    int src_grid, src_ix, src_iy;
+    int *step;
+    int *flags;
+    int max_steps;
+    const int *rcv;           // [n_rcv][4]: field slot, row, column, trace row
+    int n_rcv;
+    double *traces;
+};
+template <class S, class C>
+void launch_acoustic_fused(const AcShot<S, C> &a, int cpst, int *done, cudaStream_t st);
+template <class S, class C>
+void launch_acoustic_fused_batch(const AcShot<S, C> *shots, int n_shots, int n_warps, int cpst, int *done,
+                                 cudaStream_t st);
 template <class S, class C>
 cudaError_t prepare_fused();
 

@@ -70,6 +70,10 @@ struct tw_solver {
     void *f[5] = {}, *res[5] = {}, *coef[5] = {};
     // fused elastic path: double-buffered state, strip x segment geometry, per-CTA receivers
     bool fused = false;
+    // fused periodic acoustic path (energy off): double-buffered state, n_int_seg x n_wstrip
+    // warps, receivers as one flat list in d_rcv_list
+    bool afused = false;
+    int n_rcv_list = 0;
     void *f2[5] = {}, *res2[5] = {};
     int parity = 0;                   // which buffer holds the current state (0: f/res, 1: f2/res2)
     int n_int_seg = 0, int_rows = 0, n_zone = 1, n_wstrip = 0, n_bstrip = 1, n_int_cta = 0, tile_rows = 1;
@@ -224,6 +228,40 @@ void enqueue_steps(tw_solver *s, int n, cudaStream_t st)
 void *cur_f(const tw_solver *s, int k) { return s->parity ? s->f2[k] : s->f[k]; }
 void *cur_res(const tw_solver *s, int k) { return s->parity ? s->res2[k] : s->res[k]; }
 
+// arguments of one fused acoustic step of shot s whose state is in buffer `parity`
+template <class S, class C>
+AcShot<S, C> acoustic_shot(const tw_solver *s, int parity)
+{
+    AcShot<S, C> a{};
+    void *const *fin = parity ? s->f2 : s->f, *const *fout = parity ? s->f : s->f2;
+    void *const *rin = parity ? s->res2 : s->res, *const *rout = parity ? s->res : s->res2;
+    for (int k = 0; k < 5; k++) {
+        a.in[k] = (const S *)fin[k];
+        a.out[k] = (S *)fout[k];
+        a.rin[k] = (const S *)rin[k];
+        a.rout[k] = (S *)rout[k];
+        a.coef[k] = (const C *)s->coef[k];
+    }
+    a.pitch = s->pitch;
+    a.Mx = (int)s->d.Mx;
+    a.My = (int)s->d.My;
+    a.op = make_ops<C>((double)s->d.num_dx / (double)s->d.den_dx, s->d.dt, true);
+    a.n_seg = s->n_int_seg;
+    a.n_wstrip = s->n_wstrip;
+    a.warp_off = 0;
+    a.src_inc = s->src_inc;
+    a.src_grid = s->src_grid;
+    a.src_ix = (int)s->src_ix;
+    a.src_iy = (int)s->src_iy;
+    a.step = s->d_step;
+    a.flags = s->d_flags;
+    a.max_steps = s->d.max_steps;
+    a.rcv = s->d_rcv_list;
+    a.n_rcv = s->n_rcv_list;
+    a.traces = s->d_traces;
+    return a;
+}
+
 // one fused elastic step from the buffers fin (rin) into fout (rout)
 template <class S, class C>
 void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *const *rin, void *const *rout,
@@ -301,6 +339,14 @@ void enqueue_phase(tw_solver *s, int ph, cudaStream_t st)
 
 void enqueue(tw_solver *s, int n, cudaStream_t st)
 {
+    if (s->afused) {
+        for (int k = 0; k < n; k++) {
+            if (s->d.precision == TW_FP64) launch_acoustic_fused<double, double>(acoustic_shot<double, double>(s, s->parity), s->d.cpst, s->d_done, st);
+            else launch_acoustic_fused<float, float>(acoustic_shot<float, float>(s, s->parity), s->d.cpst, s->d_done, st);
+            s->parity ^= 1;
+        }
+        return;
+    }
     if (s->fused) {
         for (int k = 0; k < n; k++) {
             switch (s->d.precision) {
@@ -430,6 +476,25 @@ int upload_receivers(tw_solver *s)
         TW_CUDA(cudaMemcpyAsync(s->d_rcv_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, s->st));
         if (!list.empty())
             TW_CUDA(cudaMemcpyAsync(s->d_rcv_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, s->st));
+    }
+    if (s->afused) {   // (field slot, row, column, trace row) per recorded field
+        std::vector<int> list;
+        for (int r = 0; r < n; r++) {
+            const int *q = &s->rcv_tab[4 * r];
+            for (int f = 0; f < 2; f++)
+                if (q[f] >= 0) list.insert(list.end(), {q[f], q[2], q[3], 2 * r + f});
+        }
+        if ((int)list.size() > s->rcv_list_cap) {
+            cudaFree(s->d_rcv_list);
+            s->d_rcv_list = nullptr;
+            int cap = 64;
+            while (cap < (int)list.size()) cap *= 2;
+            if (s->alloc((void **)&s->d_rcv_list, sizeof(int) * cap) != TW_OK) return TW_ERR_NOMEM;
+            s->rcv_list_cap = cap;
+        }
+        if (!list.empty())
+            TW_CUDA(cudaMemcpyAsync(s->d_rcv_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, s->st));
+        s->n_rcv_list = (int)list.size() / 4;
     }
     TW_CUDA(cudaStreamSynchronize(s->st));
     s->drop_graph();
@@ -628,6 +693,26 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
         cudaMemsetAsync(s->d_done, 0, sizeof(int), s->st);
         if ((rc_ = s->alloc((void **)&s->d_rcv_off, sizeof(int) * (nctas + 1))) != TW_OK) return fail(rc_);
         cudaMemsetAsync(s->d_rcv_off, 0, sizeof(int) * (nctas + 1), s->st);
+    }
+    if (!s->elastic && s->periodic && !d.energy) {
+        // fused periodic acoustic path: a second copy of the state; segments of 8 rows or more,
+        // TW_FS_CTAS_PER_SM CTAs of work per SM of a 148-SM B200
+        s->afused = true;
+        for (int k = 0; k < 5; k++) {
+            if (!s->has_slot(k)) continue;
+            const size_t n = (size_t)s->rows[k] * s->pitch;
+            if ((rc_ = s->alloc(&s->f2[k], n * s->esz)) != TW_OK) return fail(rc_);
+            cudaMemsetAsync(s->f2[k], 0, n * s->esz, s->st);
+            if (cp) {
+                if ((rc_ = s->alloc(&s->res2[k], n * s->esz)) != TW_OK) return fail(rc_);
+                cudaMemsetAsync(s->res2[k], 0, n * s->esz, s->st);
+            }
+        }
+        s->n_wstrip = (int)((My + 1 + FS_WARP_CORE - 1) / FS_WARP_CORE);
+        const int target = std::max(1, 148 * TW_FS_CTAS_PER_SM * FS_WARPS / s->n_wstrip);
+        s->n_int_seg = std::max(1, std::min(target, (int)Mx / 8));
+        if ((rc_ = s->alloc((void **)&s->d_done, sizeof(int))) != TW_OK) return fail(rc_);
+        cudaMemsetAsync(s->d_done, 0, sizeof(int), s->st);
     }
     if ((rc_ = s->alloc((void **)&s->src_inc, sizeof(double) * d.max_steps)) != TW_OK) return fail(rc_);
     if ((rc_ = s->alloc((void **)&s->d_energy, sizeof(double) * 3 * d.max_steps)) != TW_OK) return fail(rc_);
@@ -836,7 +921,7 @@ int tw_step(tw_solver *s, int n)
     // a graph of G steps captured once and replayed; leftover steps are launched directly
     const int G = 16;
     int left = n;
-    if (s->fused && s->parity && left > 0 && n >= G) {
+    if ((s->fused || s->afused) && s->parity && left > 0 && n >= G) {
         enqueue(s, 1, s->st);   // captured graphs start from the first buffer
         left--;
     }
@@ -972,7 +1057,7 @@ int tw_profile(tw_solver *s, int n, double *ms)
     for (int k = 0; k < n; k++)
         for (int ph = 0; ph < 4; ph++) {
             cudaEventRecord(ev[(size_t)8 * k + 2 * ph], s->st);
-            if (s->fused) {
+            if (s->fused || s->afused) {
                 if (ph == 0) enqueue(s, 1, s->st);   // the whole step is one launch
             } else if (ph != 2 || s->d.energy) {
                 if (f64) enqueue_phase<double, double>(s, ph, s->st);
@@ -991,7 +1076,7 @@ int tw_profile(tw_solver *s, int n, double *ms)
     for (auto &x : ev) cudaEventDestroy(x);
     if (e != cudaSuccess) return cuda_fail(e, "tw_profile");
     for (int ph = 0; ph < 4; ph++) ms[ph] = acc[ph] / n;
-    if (s->fused) ms[1] = ms[2] = ms[3] = 0.;   // the fused step launches nothing else
+    if (s->fused || s->afused) ms[1] = ms[2] = ms[3] = 0.;   // the fused step launches nothing else
     s->steps_done += n;
     return TW_OK;
 }
@@ -1240,6 +1325,12 @@ extern "C" int tw_adjoint_gradient(tw_solver *s, int nt, const double *obs, int 
 struct tw_batch {
     std::vector<tw_solver *> shots;
     int precision = TW_FP32, cpst = 0, periodic = 0, device = 0;
+    // periodic shots step with the fused acoustic kernel: per-shot arguments for both relative
+    // parities (d_ac: 2 x n), the launch's warps, its CTA counter, and the CTAs-per-SM target
+    bool fused = false;
+    void *d_ac = nullptr;
+    int *d_done = nullptr;
+    int n_warps = 0, per_sm = TW_FS_CTAS_PER_SM;
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
     void *d_shots = nullptr, *d_gather = nullptr;
@@ -1258,7 +1349,7 @@ struct tw_batch {
     ~tw_batch()
     {
         drop_graph();
-        cudaFree(d_shots); cudaFree(d_gather); cudaFree(d_tile_shot);
+        cudaFree(d_shots); cudaFree(d_gather); cudaFree(d_tile_shot); cudaFree(d_ac); cudaFree(d_done);
         if (done) cudaEventDestroy(done);
         if (st) cudaStreamDestroy(st);
     }
@@ -1320,6 +1411,47 @@ int batch_layout_t(tw_batch *b, const BatchShape &shape)
     return TW_OK;
 }
 
+// fused batches: segments of about the same height in every shot, sized for per_sm CTAs of work
+// on each of 148 SMs (8 rows or more); arguments for both relative parities from each shot's
+// current buffer
+template <class S, class C>
+int batch_fused_layout_t(tw_batch *b, int per_sm)
+{
+    const int n = (int)b->shots.size();
+    double work = 0.;   // strip x row units of all shots
+    for (tw_solver *s : b->shots) work += (double)((s->d.My + 1 + FS_WARP_CORE - 1) / FS_WARP_CORE) * s->d.Mx;
+    const double rows = std::max(8.0, work / (148.0 * per_sm * FS_WARPS));
+    std::vector<AcShot<S, C>> ac(2 * (size_t)n);
+    int off = 0;
+    for (int k = 0; k < n; k++) {
+        tw_solver *s = b->shots[k];
+        for (int p = 0; p < 2; p++) {
+            AcShot<S, C> a = acoustic_shot<S, C>(s, s->parity ^ p);
+            a.n_seg = std::max(1, std::min((int)s->d.Mx / 8, (int)std::lround(s->d.Mx / rows)));
+            a.warp_off = off;
+            ac[(size_t)p * n + k] = a;
+        }
+        off += ac[k].n_seg * ac[k].n_wstrip;
+    }
+    if (!b->d_ac) TW_CUDA(cudaMalloc(&b->d_ac, sizeof(AcShot<S, C>) * 2 * n));
+    if (!b->d_done) {
+        TW_CUDA(cudaMalloc((void **)&b->d_done, sizeof(int)));
+        TW_CUDA(cudaMemsetAsync(b->d_done, 0, sizeof(int), b->st));
+    }
+    TW_CUDA(cudaMemcpyAsync(b->d_ac, ac.data(), sizeof(AcShot<S, C>) * ac.size(), cudaMemcpyHostToDevice, b->st));
+    TW_CUDA(cudaStreamSynchronize(b->st));
+    if (off != b->n_warps || per_sm != b->per_sm) b->drop_graph();
+    b->n_warps = off;
+    b->per_sm = per_sm;
+    return TW_OK;
+}
+
+int batch_fused_layout(tw_batch *b, int per_sm)
+{
+    return b->precision == TW_FP64 ? batch_fused_layout_t<double, double>(b, per_sm)
+                                   : batch_fused_layout_t<float, float>(b, per_sm);
+}
+
 int batch_layout(tw_batch *b, const BatchShape &shape)
 {
     return b->precision == TW_FP64 ? batch_layout_t<double, double>(b, shape) : batch_layout_t<float, float>(b, shape);
@@ -1338,6 +1470,18 @@ void enqueue_batch_t(tw_batch *b, int n, cudaStream_t st)
 
 void enqueue_batch(tw_batch *b, int n, cudaStream_t st)
 {
+    if (b->fused) {   // step k uses the arguments of relative parity k & 1
+        const int ns = (int)b->shots.size();
+        for (int k = 0; k < n; k++) {
+            if (b->precision == TW_FP64)
+                launch_acoustic_fused_batch<double, double>((const AcShot<double, double> *)b->d_ac + (size_t)(k & 1) * ns, ns,
+                                                            b->n_warps, b->cpst, b->d_done, st);
+            else
+                launch_acoustic_fused_batch<float, float>((const AcShot<float, float> *)b->d_ac + (size_t)(k & 1) * ns, ns,
+                                                          b->n_warps, b->cpst, b->d_done, st);
+        }
+        return;
+    }
     if (b->precision == TW_FP64) enqueue_batch_t<double, double>(b, n, st);
     else enqueue_batch_t<float, float>(b, n, st);
 }
@@ -1376,7 +1520,9 @@ int tw_batch_create(tw_batch **out, tw_solver *const *shots, int n)
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
     if (e != cudaSuccess) return fail(cuda_fail(e, "tw_batch_create"));
-    const int rc = batch_layout(b, BatchShape{32, 8, 1, 0});
+    b->fused = true;
+    for (tw_solver *s : b->shots) b->fused = b->fused && s->afused;
+    const int rc = b->fused ? batch_fused_layout(b, TW_FS_CTAS_PER_SM) : batch_layout(b, BatchShape{32, 8, 1, 0});
     if (rc != TW_OK) return fail(rc);
     *out = b;
     return TW_OK;
@@ -1394,14 +1540,25 @@ int tw_batch_set_shape(tw_batch *b, int tx, int ty, int rows_per_thread, int cta
 {
     if (!b) return TW_ERR_INVALID;
     const BatchShape sh{tx, ty, rows_per_thread, ctas};
-    if (!shape_ok(sh)) return TW_ERR_INVALID;
     TW_CUDA(cudaSetDevice(b->device));
+    if (b->fused) {   // fused batches: `ctas` is the CTAs-per-SM target of the segmentation
+        if (ctas < 1) return TW_ERR_INVALID;
+        return batch_fused_layout(b, ctas);
+    }
+    if (!shape_ok(sh)) return TW_ERR_INVALID;
     return batch_layout(b, sh);
 }
 
 int tw_batch_get_shape(tw_batch *b, int *shape4)
 {
     if (!b || !shape4) return TW_ERR_INVALID;
+    if (b->fused) {   // warps of FS_WARP_CORE columns, FS_WARPS per CTA, the per-SM target, the warps
+        shape4[0] = FS_WARP_CORE;
+        shape4[1] = FS_WARPS;
+        shape4[2] = b->per_sm;
+        shape4[3] = b->n_warps;
+        return TW_OK;
+    }
     shape4[0] = b->shape.tx;
     shape4[1] = b->shape.ty;
     shape4[2] = b->shape.rpt;
@@ -1415,15 +1572,19 @@ int tw_batch_tune(tw_batch *b, int steps, double *best_ms)
     TW_CUDA(cudaSetDevice(b->device));
     for (tw_solver *s : b->shots) {
         TW_CUDA(cudaStreamSynchronize(s->st));
-        if (steps + 1 > s->d.max_steps) steps = s->d.max_steps - 1;
+        if (steps + 3 > s->d.max_steps) steps = s->d.max_steps - 3;
     }
     if (steps < 1) return TW_ERR_RECORD_FULL;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     std::vector<BatchShape> cand;
-    for (int tx : {32, 64, 128, 256})
-        for (int rpt : {1, 2, 4})
-            for (int per_sm : {0, 4, 8, 16}) cand.push_back(BatchShape{tx, 256 / tx, rpt, per_sm * sms});
+    if (b->fused) {   // fused batches: the CTAs-per-SM target of the segmentation
+        for (int per_sm : {2, 4, 8, 15, 24, 32}) cand.push_back(BatchShape{0, 0, 0, per_sm});
+    } else {
+        for (int tx : {32, 64, 128, 256})
+            for (int rpt : {1, 2, 4})
+                for (int per_sm : {0, 4, 8, 16}) cand.push_back(BatchShape{tx, 256 / tx, rpt, per_sm * sms});
+    }
     cudaEvent_t e0, e1;
     TW_CUDA(cudaEventCreate(&e0));
     TW_CUDA(cudaEventCreate(&e1));
@@ -1431,11 +1592,11 @@ int tw_batch_tune(tw_batch *b, int steps, double *best_ms)
     BatchShape pick = b->shape;
     int rc = TW_OK;
     for (const BatchShape &c : cand) {
-        if ((rc = batch_layout(b, c)) != TW_OK) break;
+        if ((rc = b->fused ? batch_fused_layout(b, c.ctas) : batch_layout(b, c)) != TW_OK) break;
         for (tw_solver *s : b->shots) cudaMemsetAsync(s->d_step, 0, sizeof(int), b->st);
-        enqueue_batch(b, 1, b->st);
+        enqueue_batch(b, 2, b->st);   // (an even count: the relative parity returns to 0)
         cudaEventRecord(e0, b->st);
-        enqueue_batch(b, steps, b->st);
+        enqueue_batch(b, steps + (steps & 1), b->st);
         cudaEventRecord(e1, b->st);
         cudaError_t e = cudaEventSynchronize(e1);
         if (e != cudaSuccess) { rc = cuda_fail(e, "tw_batch_tune"); break; }
@@ -1446,9 +1607,9 @@ int tw_batch_tune(tw_batch *b, int steps, double *best_ms)
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc != TW_OK) return rc;
-    if ((rc = batch_layout(b, pick)) != TW_OK) return rc;
     for (tw_solver *s : b->shots)
         if ((rc = tw_reset(s)) != TW_OK) return rc;
+    if ((rc = b->fused ? batch_fused_layout(b, pick.ctas) : batch_layout(b, pick)) != TW_OK) return rc;
     if (best_ms) *best_ms = best;
     return TW_OK;
 }
@@ -1461,6 +1622,10 @@ int tw_batch_step(tw_batch *b, int n)
     if (n == 0) return TW_OK;
     TW_CUDA(cudaSetDevice(b->device));
     for (tw_solver *s : b->shots) TW_CUDA(cudaStreamSynchronize(s->st));   // queued single-shot work first
+    if (b->fused) {   // each shot's current buffer may have changed since the last call
+        const int rc = batch_fused_layout(b, b->per_sm);
+        if (rc != TW_OK) return rc;
+    }
     const int G = 16;
     int left = n;
     if (left >= G) {
@@ -1487,6 +1652,7 @@ int tw_batch_step(tw_batch *b, int n)
     for (tw_solver *s : b->shots) {
         TW_CUDA(cudaStreamWaitEvent(s->st, b->done, 0));
         s->steps_done += n;
+        if (b->fused) s->parity ^= n & 1;
     }
     return TW_OK;
 }
