@@ -43,7 +43,8 @@ enum {
     TW_ERR_NONFINITE = -9,      /* a NaN/Inf appeared in a field (sticky, reported by tw_sync) */
     TW_ERR_UNSUPPORTED = -10,   /* combination not implemented (e.g. elastic with periodic x) */
     TW_ERR_MODEL_BOUNDS = -11,  /* interpolation stepped out of the model (grid_parameter.cpp:54-56) */
-    TW_ERR_TOO_LARGE = -12      /* model larger than the no-allocation scratch (TW_NOALLOC_MAX_MODEL_POINTS) */
+    TW_ERR_TOO_LARGE = -12,     /* model larger than the no-allocation scratch (TW_NOALLOC_MAX_MODEL_POINTS) */
+    TW_ERR_IO = -13             /* a file could not be opened, read or written, or is malformed */
 };
 
 /* ---- enums ------------------------------------------------------------------------------ */
@@ -235,6 +236,47 @@ TW_API int tw_batch_tune(tw_batch *b, int steps, double *best_ms);
 TW_API int tw_batch_step(tw_batch *b, int n);
 /* Wait for the batch; returns the first sticky error of any shot. */
 TW_API int tw_batch_sync(tw_batch *b);
+
+/* ---- the reference's files --------------------------------------------------------------
+ * Readers and writers of the reference's own input and output files, so that workflows built
+ * around its executables (InputFile.txt, SrcRcv.txt, model files, Signal / Energy / Snapshot
+ * text outputs) can use this library unchanged. */
+typedef struct {
+    long Mx_prmt, My_prmt;      /* model_<X>_<Y>: model cells along data x, data y */
+    long Mx, My;                /* grids_<X>_<Y>: simulation cells */
+    int num_dxM, den_dxM;       /* dxM_<num>_<den>: model spacing */
+    int num_dx, den_dx;         /* dxS_<num>_<den>: simulation spacing */
+    char bdry[4];               /* bdry_<xL><xR><yL><yR>, upper case; zeros when absent */
+    long Nt;
+    double dt_max, cfl, dt;     /* MAXdt, CFL and dt = MAXdt * CFL (main_host_FDM_2D.tpp:57) */
+    double central_f, time_delay;
+    int device;
+} tw_io_input;
+/* InputFile.txt (input_processing.cpp:11-137); missing entries keep the reference's defaults. */
+TW_API int tw_io_read_input(const char *path, tw_io_input *out);
+
+typedef struct {
+    long src_index;             /* the source's index (for a receiver: the source it belongs to) */
+    long rcv_index;             /* the receiver's index; -1 for a source */
+    char type_x, type_y;        /* 'N' or 'M' along data x, data y */
+    long num_x, den_x, num_y, den_y;   /* location num/den along data x, data y */
+} tw_io_point;
+/* SrcRcv.txt (inverse.cpp:133-322): the Src and Rcv lines in file order. Writes at most cap
+ * points; *n is the count in the file (cap 0 with pts NULL asks for it). A receiver listed
+ * before its source is TW_ERR_IO, as the reference stops there. */
+TW_API int tw_io_read_srcrcv(const char *path, tw_io_point *pts, int cap, int *n);
+/* A model file (inverse.cpp:6-130): (Mx_prmt+1) x (My_prmt+1) native doubles, x outer, into the
+ * padded (Mx_prmt+2) x (My_prmt+2) layout of tw_set_material_model (zeros in the padding). */
+TW_API int tw_io_read_model(const char *path, long Mx_prmt, long My_prmt, double *padded);
+/* Output files of the handle's records in the reference's text formats (forward.cpp:215-325,
+ * nvcc_device_FDM_2D.cu:786-819), into `folder`:
+ *   Signal_src_<s>_<src grid>_<iy>_<ix>_rcv_<r>_<rcv grid>_<iy>_<ix>.txt per receiver:
+ *     "% 6d  " step, then "% 16.15e  " per field of the grid;
+ *   Energy_src_<s>_<src grid>_<iy>_<ix>.txt (energy on): "%16.15e" of E_k + (E_p0 + E_p1) / 2;
+ *   with snapshots != 0, Snapshot_<grid>_<name>_<field>.txt: the current field, row-major.
+ * Grid strings list the data-y type first, as the reference writes them; values are multiplied
+ * by source_scaling (the energy by its square). rcv_index: one index per receiver (NULL: 0, 1, ...). */
+TW_API int tw_io_write_records(tw_solver *s, const char *folder, int src_index, const int *rcv_index, int snapshots);
 
 TW_API const char *tw_strerror(int status);
 TW_API const char *tw_last_cuda_error(void);

@@ -30,7 +30,7 @@ PRECISION = {"f64": FP64, "f32": FP32, "bf16": BF16, "fp16": FP16}
 
 ERRORS = {0: "TW_OK", -1: "TW_ERR_INVALID", -2: "TW_ERR_CUDA", -3: "TW_ERR_NOMEM", -4: "TW_ERR_STATE",
           -5: "TW_ERR_LOCATION", -6: "TW_ERR_OUTSIDE", -7: "TW_ERR_WEAK_BOUNDARY", -8: "TW_ERR_RECORD_FULL",
-          -9: "TW_ERR_NONFINITE", -10: "TW_ERR_UNSUPPORTED", -11: "TW_ERR_MODEL_BOUNDS", -12: "TW_ERR_TOO_LARGE"}
+          -9: "TW_ERR_NONFINITE", -10: "TW_ERR_UNSUPPORTED", -11: "TW_ERR_MODEL_BOUNDS", -12: "TW_ERR_TOO_LARGE", -13: "TW_ERR_IO"}
 
 
 class TwError(RuntimeError):
@@ -57,6 +57,18 @@ _lib = None
 
 def library_path() -> str:
     return LIB_PATH
+
+
+class IoInput(C.Structure):
+    _fields_ = [("Mx_prmt", C.c_long), ("My_prmt", C.c_long), ("Mx", C.c_long), ("My", C.c_long),
+                ("num_dxM", C.c_int), ("den_dxM", C.c_int), ("num_dx", C.c_int), ("den_dx", C.c_int),
+                ("bdry", C.c_char * 4), ("Nt", C.c_long), ("dt_max", C.c_double), ("cfl", C.c_double),
+                ("dt", C.c_double), ("central_f", C.c_double), ("time_delay", C.c_double), ("device", C.c_int)]
+
+
+class IoPoint(C.Structure):
+    _fields_ = [("src_index", C.c_long), ("rcv_index", C.c_long), ("type_x", C.c_char), ("type_y", C.c_char),
+                ("num_x", C.c_long), ("den_x", C.c_long), ("num_y", C.c_long), ("den_y", C.c_long)]
 
 
 def lib() -> C.CDLL:
@@ -91,6 +103,10 @@ def lib() -> C.CDLL:
                                               C.c_int, C.c_int, vp, vp, vp, vp, vp, vp]
         L.tw_location_to_index.argtypes = [C.c_char, C.c_long, C.c_long, C.c_int, C.c_int, lp]
         L.tw_adjoint_gradient.argtypes = [vp, C.c_int, dp, C.c_int, dp, C.POINTER(dp), dp, dp, dp, C.POINTER(dp)]
+        L.tw_io_read_input.argtypes = [C.c_char_p, C.POINTER(IoInput)]
+        L.tw_io_read_srcrcv.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+        L.tw_io_read_model.argtypes = [C.c_char_p, C.c_long, C.c_long, dp]
+        L.tw_io_write_records.argtypes = [vp, C.c_char_p, C.c_int, C.POINTER(C.c_int), C.c_int]
         L.tw_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
         L.tw_batch_destroy.argtypes = [vp]
         L.tw_batch_destroy.restype = None
@@ -123,6 +139,29 @@ def _ok(code: int, what: str):
         if code == -2:
             what = f"{what} ({lib().tw_last_cuda_error().decode()})"
         raise TwError(code, what)
+
+
+def io_read_input(path: str) -> IoInput:
+    """The reference's InputFile.txt (tw_io_read_input)."""
+    out = IoInput()
+    _ok(lib().tw_io_read_input(path.encode(), C.byref(out)), "tw_io_read_input")
+    return out
+
+
+def io_read_srcrcv(path: str) -> list:
+    """The Src and Rcv lines of the reference's SrcRcv.txt, in file order (tw_io_read_srcrcv)."""
+    n = C.c_int()
+    _ok(lib().tw_io_read_srcrcv(path.encode(), None, 0, C.byref(n)), "tw_io_read_srcrcv")
+    arr = (IoPoint * max(n.value, 1))()
+    _ok(lib().tw_io_read_srcrcv(path.encode(), arr, n.value, C.byref(n)), "tw_io_read_srcrcv")
+    return [arr[i] for i in range(n.value)]
+
+
+def io_read_model(path: str, Mx_prmt: int, My_prmt: int) -> np.ndarray:
+    """A model file in the padded (Mx_prmt+2) x (My_prmt+2) layout (tw_io_read_model)."""
+    out = np.zeros((Mx_prmt + 2, My_prmt + 2))
+    _ok(lib().tw_io_read_model(path.encode(), Mx_prmt, My_prmt, _dp(out)), "tw_io_read_model")
+    return out
 
 
 def location_to_index(gtype: str, num: int, den: int, num_dx: int, den_dx: int) -> int:
@@ -299,6 +338,13 @@ class Solver:
         if state:
             out["state"] = dict(zip(("NN", "MN", "NM", "MM0", "MM1"), st))
         return out
+
+    def write_records(self, folder: str, src_index: int = 0, rcv_index=None, snapshots: bool = False):
+        """The reference's Signal / Energy / Snapshot text files (tw_io_write_records)."""
+        ri = None
+        if rcv_index is not None:
+            ri = (C.c_int * len(rcv_index))(*rcv_index)
+        _ok(lib().tw_io_write_records(self.h, folder.encode(), src_index, ri, int(snapshots)), "tw_io_write_records")
 
     def stream(self) -> int:
         p = C.c_void_p()

@@ -584,6 +584,7 @@ const char *tw_strerror(int status)
     case TW_ERR_UNSUPPORTED: return "unsupported configuration";
     case TW_ERR_MODEL_BOUNDS: return "material interpolation outside the model";
     case TW_ERR_TOO_LARGE: return "model larger than the no-allocation scratch (TW_NOALLOC_MAX_MODEL_POINTS)";
+    case TW_ERR_IO: return "file missing, unreadable, unwritable or malformed";
     }
     return "unknown status";
 }
@@ -1027,6 +1028,67 @@ int tw_read_energy(tw_solver *s, double *E_k, double *E_p0, double *E_p1)
         if (E_k) E_k[it] = k[it];
         if (E_p1) E_p1[it] = p1[it];
         if (E_p0) E_p0[it] = s->periodic ? (it > 0 ? p1[it - 1] : 0.) : p0[it];
+    }
+    return TW_OK;
+}
+
+int tw_io_write_records(tw_solver *s, const char *folder, int src_index, const int *rcv_index, int snapshots)
+{
+    if (check(s) || !folder) return TW_ERR_INVALID;
+    const int n = (int)(s->rcv_tab.size() / 4), nt = s->steps_done;
+    const double sc = s->d.source_scaling;
+    static const char *gname[4] = {"Sxy", "Vx", "Vy", "SMM"};       // grid.hpp:155-159
+    auto gstr = [](int grid) {   // data-y type first (forward.cpp:251)
+        const char tx = (grid == TW_NN || grid == TW_NM) ? 'N' : 'M', ty = (grid == TW_NN || grid == TW_MN) ? 'N' : 'M';
+        return std::string(1, ty) + std::string(1, tx);
+    };
+    auto grid_of_slot = [](int slot) { return slot == F_NN ? TW_NN : slot == F_MN ? TW_MN : slot == F_NM ? TW_NM : TW_MM; };
+    const std::string src = s->src_grid >= 0
+        ? "src_" + std::to_string(src_index) + "_" + gstr(s->src_grid) + "_" + std::to_string(s->src_iy) + "_" + std::to_string(s->src_ix)
+        : "src_" + std::to_string(src_index) + "_none";
+    if (n > 0 && nt > 0) {
+        std::vector<double> tr(2 * (size_t)n * nt);
+        const int rc = tw_read_receivers(s, tr.data());
+        if (rc != TW_OK) return rc;
+        for (int r = 0; r < n; r++) {
+            const int *q = &s->rcv_tab[4 * r];
+            const int g = grid_of_slot(q[0]), nf = q[1] >= 0 ? 2 : 1;
+            const std::string name = std::string(folder) + "/Signal_" + src + "_rcv_" + std::to_string(rcv_index ? rcv_index[r] : r) +
+                                     "_" + gstr(g) + "_" + std::to_string(q[3]) + "_" + std::to_string(q[2]) + ".txt";
+            FILE *fp = fopen(name.c_str(), "w");
+            if (!fp) return TW_ERR_IO;
+            for (int it = 0; it < nt; it++) {
+                fprintf(fp, "% 6d  ", it);
+                for (int f = 0; f < nf; f++) fprintf(fp, "% 16.15e  ", sc * tr[(2 * (size_t)r + f) * nt + it]);
+                fprintf(fp, "\n");
+            }
+            if (fclose(fp) != 0) return TW_ERR_IO;
+        }
+    }
+    if (s->d.energy && nt > 0) {
+        std::vector<double> k(nt), p0(nt), p1(nt);
+        const int rc = tw_read_energy(s, k.data(), p0.data(), p1.data());
+        if (rc != TW_OK) return rc;
+        FILE *fp = fopen((std::string(folder) + "/Energy_" + src + ".txt").c_str(), "w");
+        if (!fp) return TW_ERR_IO;
+        for (int it = 0; it < nt; it++) fprintf(fp, "%16.15e\n", sc * sc * (k[it] + (p0[it] + p1[it]) / 2.));
+        if (fclose(fp) != 0) return TW_ERR_IO;
+    }
+    if (snapshots) {
+        for (int g = 0; g < 4; g++)
+            for (int f = 0; f < 2; f++) {
+                const int slot = slot_of(s, g, f);
+                if (slot < 0) continue;
+                const long R = s->ref_rows[g], Cn = s->ref_cols[g];
+                std::vector<double> v((size_t)R * Cn);
+                const int rc = tw_read_field(s, g, f, v.data(), Cn);
+                if (rc != TW_OK) return rc;
+                const std::string name = std::string(folder) + "/Snapshot_" + gstr(g) + "_" + gname[g] + "_" + std::to_string(f) + ".txt";
+                FILE *fp = fopen(name.c_str(), "w");
+                if (!fp) return TW_ERR_IO;
+                for (double x : v) fprintf(fp, "% 16.15e\n", sc * x);
+                if (fclose(fp) != 0) return TW_ERR_IO;
+            }
     }
     return TW_OK;
 }
