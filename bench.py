@@ -27,6 +27,12 @@ of each against the FP64 run of the same scheme.
 one batched launch per half-step (launch shape from the autotuner) against the same 64 handles
 solved one after another; the traces of the two must agree bit for bit.
 
+`--workload acoustic512` measures the plain-method acoustic configuration: 512 x 512 on [0,1]^2,
+c = 1, rho = 1, FP32, CFL 0.5, Ricker f0 = 10 at the centre, 1000 steps, 16 receivers, in the
+periodic and the free-surface mode (both two launches per step at this size), with
+the reference's single-core solver on a sample of the same run for the CPU baseline and a
+bit-for-bit trace comparison.
+
 `--workload adjoint` measures the adjoint gradient: elastic 1024 x 1024 FP32, 2000 steps, 8
 shots along row 16, 256 receivers on NM row 4; observed traces from the layered medium with a 5 %
 Gaussian anomaly, gradient of the misfit with respect to rho, vp, vs of the layered medium,
@@ -536,6 +542,63 @@ def run_batch(args):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- plain acoustic 512^2
+def run_acoustic512(args):
+    import torch
+    from oracle import refrun
+    tw = load_twave()
+    torch.cuda.set_device(0)
+    n, K = 512, args.steps
+    dx = 1.0 / n
+    dt = 0.5 * dx / np.sqrt(2.0)
+    rcv_ix, rcv_iy = np.full(16, 128), 16 + 32 * np.arange(16)
+    out = {}
+    for mode, bc in (("periodic", tw.PERIODIC), ("free_surface", tw.SAT_FREE)):
+        s = tw.Solver(n, n, 1, n, dt, physics=tw.ACOUSTIC, bc_x=bc, precision="f32", cpst="00", central_f=10.0,
+                      time_delay=0.25, max_steps=K + 64, energy=False)
+        s.set_material_grid(tw.NM, 0, np.ones((n + 1, n)))
+        s.set_material_grid(tw.MN, 0, np.ones((n, n + 1)))
+        s.set_material_grid(tw.MM, 0, np.ones((n, n)))
+        s.set_source(tw.MM, n // 2, n // 2)
+        s.add_receivers(tw.MM, rcv_ix, rcv_iy)
+        s.run(32)
+        s.reset()
+        stream = torch.cuda.ExternalStream(s.stream())
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.step(K)
+        e1.record(stream)
+        s.sync()
+        ms = e0.elapsed_time(e1)
+        out[mode] = {"gpts": n * n * K / (ms / 1e3) / 1e9, "ms_per_step": ms / K,
+                     "hbm_frac_at_36B": n * n * K / (ms / 1e3) * 36 / 1e9 / measured_peaks()[0],
+                     "traces": s.read_receivers()[:, 0, :]}
+        s.close()
+    # the reference's single-core solver (periodic) on the first steps of the same run
+    cs = min(K, args.cpu_steps * 10)
+    case = refrun.AcousticCase(Nx=n, Ny=n, dx=dx, dt=dt, coef_vx=np.ones((n + 1, n)), coef_vy=np.ones((n, n + 1)),
+                               coef_p=np.ones((n, n)), src=(n // 2, n // 2),
+                               rcvs=[(2, int(a), int(b)) for a, b in zip(rcv_ix, rcv_iy)], Nt=cs, cpst="0",
+                               central_f=10.0, time_delay=0.25)
+    ref = refrun.run_acoustic(case, "f32", perf=True)   # timing build (the reference's -O3 flags)
+    cpu = {"value": n * n * cs / ref.loop_seconds / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
+           "sample": f"the first {cs} steps of this run, periodic mode, the reference's single-core acoustic FP32 solver"}
+    case.Nt = 100                                         # parity build: traces bit for bit
+    par = refrun.run_acoustic(case, "f32", perf=False)
+    same = bool(np.array_equal(par.traces, out["periodic"]["traces"][:, :100]))
+    for v in out.values():
+        v.pop("traces")
+    line = {"metric": METRIC, "value": out["periodic"]["gpts"], "unit": UNIT, "n_gpus": 1, "steps": K, "warmup": 32,
+            "ms_per_step": out["periodic"]["ms_per_step"], "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "plain acoustic 512x512 on [0,1]^2, c=1, rho=1, FP32, CFL 0.5, Ricker f0=10 at the "
+                                   "centre, 16 receivers on P row 128; value: periodic mode (at this size the handle runs the "
+                                   "two-launch step, faster than the fused one below 2^20 points)",
+                       "l2": "grid far smaller than L2 (fields and coefficients 6 MB)"},
+            "modes": out, "cpu_baseline": cpu, "traces_identical_to_reference_on_sample": same}
+    print(json.dumps(line), flush=True)
+
+
 # ---------------------------------------------------------------- adjoint workload
 ADJ_N = 1024
 ADJ_SEED = 20261203 + 5
@@ -681,7 +744,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["elastic2048", "mixed", "batch", "adjoint"], default="elastic2048")
+    ap.add_argument("--workload", choices=["elastic2048", "acoustic512", "mixed", "batch", "adjoint"],
+                    default="elastic2048")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be at least 3")
@@ -689,9 +753,10 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args, dist)
         return
-    if args.workload in ("mixed", "batch", "adjoint"):
+    if args.workload in ("acoustic512", "mixed", "batch", "adjoint"):
         if dist.rank == 0:
-            {"mixed": run_mixed, "batch": run_batch, "adjoint": run_adjoint}[args.workload](args)
+            {"acoustic512": run_acoustic512, "mixed": run_mixed, "batch": run_batch,
+             "adjoint": run_adjoint}[args.workload](args)
         return
     run_ours(args, dist)
 

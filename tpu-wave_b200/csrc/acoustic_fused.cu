@@ -71,15 +71,28 @@ __device__ void acoustic_warp(const AcShot<S, C> &a, int wstrip, int seg)
         }
     };
 
-    // receivers of this lane's columns (at most RC kept in registers; more: scan the shot's list)
+    // receivers of this lane's columns (at most RC kept in registers; more: scan the shot's list).
+    // The warp reads the list 32 entries at a time, one per lane, and keeps those in its strip and
+    // rows, so a long list costs no chain of dependent loads.
     constexpr int RC = 2;
     int rq[RC], nr = 0;
     bool rmany = false;
-    for (int q = 0; q < a.n_rcv; q++) {
-        const int col = a.rcv[4 * q + 2];
-        if (core && (col == c0 || col == c1)) {
-            if (nr < RC) rq[nr++] = q;
-            else rmany = true;
+    for (int base = 0; base < a.n_rcv; base += 32) {
+        const int q = base + lane;
+        int col = -1, row = -1;
+        if (q < a.n_rcv) {
+            row = a.rcv[4 * q + 1];
+            col = a.rcv[4 * q + 2];
+        }
+        unsigned m = __ballot_sync(FULL, col >= y0 && col < y0 + FS_WARP_CORE + 2 && row >= x0 && row <= x1);
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            const int cc = __shfl_sync(FULL, col, b);
+            if (core && (cc == c0 || cc == c1)) {
+                if (nr < RC) rq[nr++] = base + b;
+                else rmany = true;
+            }
         }
     }
     auto record = [&](int slot, int row, int col, double v) {

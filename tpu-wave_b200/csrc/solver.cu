@@ -73,6 +73,7 @@ struct tw_solver {
     // fused periodic acoustic path (energy off): double-buffered state, n_int_seg x n_wstrip
     // warps, receivers as one flat list in d_rcv_list
     bool afused = false;
+    bool pfuse = false;               // double-buffered periodic acoustic: may join a fused batch
     int n_rcv_list = 0;
     void *f2[5] = {}, *res2[5] = {};
     int parity = 0;                   // which buffer holds the current state (0: f/res, 1: f2/res2)
@@ -144,13 +145,18 @@ int slot_of(const tw_solver *s, int grid, int field)
     return -1;
 }
 
+// the buffers holding the current state (the second copy after an odd number of fused steps)
+void *cur_f(const tw_solver *s, int k) { return s->parity ? s->f2[k] : s->f[k]; }
+void *cur_res(const tw_solver *s, int k) { return s->parity ? s->res2[k] : s->res[k]; }
+
+// arguments of the in-place per-point kernels, on the current buffers
 template <class S, class C>
 StepArgs<S, C> step_args(const tw_solver *s)
 {
     StepArgs<S, C> a{};
     for (int k = 0; k < 5; k++) {
-        a.f[k] = (S *)s->f[k];
-        a.res[k] = (S *)s->res[k];
+        a.f[k] = (S *)cur_f(s, k);
+        a.res[k] = (S *)cur_res(s, k);
         a.coef[k] = (const C *)s->coef[k];
     }
     a.pitch = s->pitch;
@@ -180,8 +186,8 @@ void energy_phase(const tw_solver *s, int phase, cudaStream_t st)
     e.scale = s->periodic ? 1.0 : 0.5;
     auto term = [&](int a, int b, int wslot, int pslot) {
         const int t = e.nterms++;
-        e.a[t] = (const S *)s->f[a];
-        e.b[t] = (const S *)s->f[b];
+        e.a[t] = (const S *)cur_f(s, a);
+        e.b[t] = (const S *)cur_f(s, b);
         e.w[t] = s->w[wslot];
         e.p[t] = (const C *)s->coef[pslot];
         e.rows[t] = s->rows[a];
@@ -206,7 +212,7 @@ void enqueue_steps(tw_solver *s, int n, cudaStream_t st)
 {
     const StepArgs<S, C> a = step_args<S, C>(s);
     GatherArgs<S> g{};
-    for (int k = 0; k < 5; k++) g.f[k] = (const S *)s->f[k];
+    for (int k = 0; k < 5; k++) g.f[k] = (const S *)cur_f(s, k);
     g.rcv = s->d_rcv;
     g.n_rcv = (int)(s->rcv_tab.size() / 4);
     g.pitch = s->pitch;
@@ -224,9 +230,6 @@ void enqueue_steps(tw_solver *s, int n, cudaStream_t st)
         launch_gather<S>(g, st);
     }
 }
-
-void *cur_f(const tw_solver *s, int k) { return s->parity ? s->f2[k] : s->f[k]; }
-void *cur_res(const tw_solver *s, int k) { return s->parity ? s->res2[k] : s->res[k]; }
 
 // arguments of one fused acoustic step of shot s whose state is in buffer `parity`
 template <class S, class C>
@@ -325,7 +328,7 @@ void enqueue_phase(tw_solver *s, int ph, cudaStream_t st)
         energy_phase<S, C>(s, 2, st);
     } else {
         GatherArgs<S> g{};
-        for (int k = 0; k < 5; k++) g.f[k] = (const S *)s->f[k];
+        for (int k = 0; k < 5; k++) g.f[k] = (const S *)cur_f(s, k);
         g.rcv = s->d_rcv;
         g.n_rcv = (int)(s->rcv_tab.size() / 4);
         g.pitch = s->pitch;
@@ -477,7 +480,7 @@ int upload_receivers(tw_solver *s)
         if (!list.empty())
             TW_CUDA(cudaMemcpyAsync(s->d_rcv_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, s->st));
     }
-    if (s->afused) {   // (field slot, row, column, trace row) per recorded field
+    if (s->pfuse) {   // (field slot, row, column, trace row) per recorded field, for the fused steps
         std::vector<int> list;
         for (int r = 0; r < n; r++) {
             const int *q = &s->rcv_tab[4 * r];
@@ -696,9 +699,12 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
         cudaMemsetAsync(s->d_rcv_off, 0, sizeof(int) * (nctas + 1), s->st);
     }
     if (!s->elastic && s->periodic && !d.energy) {
-        // fused periodic acoustic path: a second copy of the state; segments of 8 rows or more,
-        // TW_FS_CTAS_PER_SM CTAs of work per SM of a 148-SM B200
-        s->afused = true;
+        // periodic acoustic with energy off: a second copy of the state, for the fused step of a
+        // batch and, on grids of 2^20 points or more, of the handle alone (below that the
+        // two-launch kernels are faster: a warp's short row segment is latency-bound); segments
+        // of 8 rows or more, TW_FS_CTAS_PER_SM CTAs of work per SM of a 148-SM B200
+        s->pfuse = true;
+        s->afused = Mx * My >= (1L << 20);
         for (int k = 0; k < 5; k++) {
             if (!s->has_slot(k)) continue;
             const size_t n = (size_t)s->rows[k] * s->pitch;
@@ -1443,7 +1449,7 @@ int batch_layout_t(tw_batch *b, const BatchShape &shape)
         sh[k].tile_off = (int)tile_shot.size();
         tile_shot.insert(tile_shot.end(), (size_t)(tx * ty), k);
         GatherArgs<S> &g = ga[k];
-        for (int q = 0; q < 5; q++) g.f[q] = (const S *)s->f[q];
+        for (int q = 0; q < 5; q++) g.f[q] = (const S *)cur_f(s, q);
         g.rcv = s->d_rcv;
         g.n_rcv = (int)(s->rcv_tab.size() / 4);
         g.pitch = s->pitch;
@@ -1583,7 +1589,7 @@ int tw_batch_create(tw_batch **out, tw_solver *const *shots, int n)
     if (e == cudaSuccess) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
     if (e != cudaSuccess) return fail(cuda_fail(e, "tw_batch_create"));
     b->fused = true;
-    for (tw_solver *s : b->shots) b->fused = b->fused && s->afused;
+    for (tw_solver *s : b->shots) b->fused = b->fused && s->pfuse;
     const int rc = b->fused ? batch_fused_layout(b, TW_FS_CTAS_PER_SM) : batch_layout(b, BatchShape{32, 8, 1, 0});
     if (rc != TW_OK) return fail(rc);
     *out = b;
