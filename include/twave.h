@@ -82,6 +82,9 @@ typedef struct {
     int max_steps;          /* capacity of the trace and energy records */
     int energy;             /* 1: discrete energy every step (reference default, main_host_FDM_2D.tpp:34); 0: off */
     int device;             /* CUDA device ordinal (ns_input::device_number) */
+    int coef_fp16;          /* 1: store the stepping coefficients in FP16 (elastic, FP32 arithmetic; no
+                               reference counterpart): 10 B less per update; the medium is quantised to
+                               FP16, and coefficients outside its normal range are TW_ERR_UNSUPPORTED */
 } tw_grid_desc;
 
 typedef struct {

@@ -91,12 +91,13 @@ def acoustic_periodic_case(Nx, Ny, seed=0, cpst="0", Nt=40, cfl=0.5, central_f=1
 ELASTIC_KEYS = ("NN", "MN", "NM", "MM0", "MM1")
 
 
-def product_elastic(case, precision, acoustic=False, fields0=None, resid0=None, energy=True):
+def product_elastic(case, precision, acoustic=False, fields0=None, resid0=None, energy=True, coef_fp16=False):
     """Run `case` through the C ABI; returns dict(fields, traces, E_k, E_p0, E_p1, resid)."""
     tw = load_twave()
     s = tw.Solver(case.Mx, case.My, case.num_dx, case.den_dx, case.dt,
                   physics=tw.ACOUSTIC if acoustic else tw.ELASTIC, precision=precision, cpst=case.cpst,
-                  central_f=case.central_f, time_delay=case.time_delay, max_steps=max(case.Nt, 1), energy=energy)
+                  central_f=case.central_f, time_delay=case.time_delay, max_steps=max(case.Nt, 1), energy=energy,
+                  coef_fp16=coef_fp16)
     try:
         Mx, My = case.Mx, case.My
         shp = (Mx + 2, My + 2)

@@ -44,7 +44,8 @@ class GridDesc(C.Structure):
     _fields_ = [("physics", C.c_int), ("bc_x", C.c_int), ("precision", C.c_int), ("cpst", C.c_int),
                 ("Mx", C.c_long), ("My", C.c_long), ("num_dx", C.c_int), ("den_dx", C.c_int),
                 ("dt", C.c_double), ("central_f", C.c_double), ("time_delay", C.c_double),
-                ("source_scaling", C.c_double), ("max_steps", C.c_int), ("energy", C.c_int), ("device", C.c_int)]
+                ("source_scaling", C.c_double), ("max_steps", C.c_int), ("energy", C.c_int), ("device", C.c_int),
+                ("coef_fp16", C.c_int)]
 
 
 class Info(C.Structure):
@@ -177,9 +178,10 @@ class Solver:
     def __init__(self, Mx: int, My: int, num_dx: int, den_dx: int, dt: float, *, physics: int = ELASTIC,
                  bc_x: int = SAT_FREE, precision: str = "f32", cpst: str = "00", central_f: float = 5.0,
                  time_delay: float = 0.25, source_scaling: float = 1.0, max_steps: int = 1000,
-                 energy: bool = True, device: int = 0):
+                 energy: bool = True, device: int = 0, coef_fp16: bool = False):
         self.desc = GridDesc(physics, bc_x, PRECISION[precision], CPST[cpst], Mx, My, num_dx, den_dx, dt,
-                             central_f, time_delay, source_scaling, max_steps, 1 if energy else 0, device)
+                             central_f, time_delay, source_scaling, max_steps, 1 if energy else 0, device,
+                             1 if coef_fp16 else 0)
         self.h = C.c_void_p()
         _ok(lib().tw_create(C.byref(self.h), C.byref(self.desc)), "tw_create")
         self.Mx, self.My, self.physics, self.bc_x = Mx, My, physics, bc_x

@@ -72,14 +72,32 @@ __device__ __forceinline__ double norm_x(const MaterialArgs &m, int txN, int row
     return m.dx;
 }
 
-template <class C>
+// a stepping coefficient as stored: the compute type, or FP16 (range checked: the medium must
+// lie in the normal FP16 range, else bit 2 of *err)
+template <class C, class K>
+__device__ __forceinline__ K store_coef(C v, int *err)
+{
+    if constexpr (sizeof(K) == 2) {
+        const float a = fabsf((float)v);
+        if (a > 65504.f || (a != 0.f && a < 6.103515625e-05f)) atomicOr(err, 2);
+        return __float2half_rn((float)v);
+    } else {
+        return v;
+    }
+}
+template <class K>
+__device__ __forceinline__ double kval(K v) { return (double)to_c<float>(v); }
+template <>
+__device__ __forceinline__ double kval<double>(double v) { return v; }
+
+template <class C, class K>
 __global__ void k_material_finalize(MaterialArgs m)
 {
     const int iy = blockIdx.x * blockDim.x + threadIdx.x;
     const int ix = blockIdx.y * blockDim.y + threadIdx.y;
     const double dx = m.dx;
     const bool elastic = m.physics == 0;
-    C **coef = (C **)m.coef;
+    K **coef = (K **)m.coef;
     // y factor of the norm (grid_energy.cpp:123-152): dx everywhere, then 1 on the first and 0 on
     // the last (duplicate) point of an N-type-y grid
     auto y_factor = [&](int g, double w) {
@@ -97,9 +115,9 @@ __global__ void k_material_finalize(MaterialArgs m)
     // NN (elastic only): mu, weight 1/mu
     if (elastic && ix < m.rows[F_NN] && iy < m.cols[F_NN]) {
         const long i = (long)ix * m.cols[F_NN] + iy, o = (long)ix * m.pitch + iy;
-        const C mu = (C)m.mat[F_NN][i];
+        const K mu = store_coef<C, K>((C)m.mat[F_NN][i], m.err);
         coef[F_NN][o] = mu;
-        double w = __ddiv_rn(1., (double)mu);
+        double w = __ddiv_rn(1., kval(mu));
         w = mul(w, norm_x(m, 1, m.rows[F_NN], ix));
         m.w[F_NN][o] = y_factor(F_NN, w);
     }
@@ -108,24 +126,24 @@ __global__ void k_material_finalize(MaterialArgs m)
         if (ix >= m.rows[g] || iy >= m.cols[g]) continue;
         const long i = (long)ix * m.cols[g] + iy, o = (long)ix * m.pitch + iy;
         const double rho = m.mat[g][i];
-        coef[g][o] = (C)__ddiv_rn(1., rho);
+        coef[g][o] = store_coef<C, K>((C)__ddiv_rn(1., rho), m.err);
         if (m.periodic) {
             m.w[g][o] = sc_weight(g);
         } else {
-            double w = (double)(C)rho;
+            double w = sizeof(K) == 2 ? kval(store_coef<C, K>((C)rho, m.err)) : (double)(C)rho;
             w = mul(w, norm_x(m, g == F_NM, m.rows[g], ix));
             m.w[g][o] = y_factor(g, w);
         }
     }
     if (ix < m.rows[F_MM0] && iy < m.cols[F_MM0]) {
         const long i = (long)ix * m.cols[F_MM0] + iy, o = (long)ix * m.pitch + iy;
-        const C lam = (C)m.mat[F_MM0][i];
+        const K lam = store_coef<C, K>((C)m.mat[F_MM0][i], m.err);
         coef[F_MM0][o] = lam;
         const double fx = m.periodic ? 0. : norm_x(m, 0, m.rows[F_MM0], ix);
         if (elastic) {
-            const C m2 = (C)m.mat[F_MM1][i];
+            const K m2 = store_coef<C, K>((C)m.mat[F_MM1][i], m.err);
             coef[F_MM1][o] = m2;
-            const double l = (double)lam, t = (double)m2;
+            const double l = kval(lam), t = kval(m2);
             const double den = mul(t, add(mul(2., l), t));
             const double w1 = __ddiv_rn(add(l, t), den);
             const double w2 = -__ddiv_rn(mul(l, 2.), den);
@@ -135,19 +153,20 @@ __global__ void k_material_finalize(MaterialArgs m)
             m.w[F_MM0][o] = sc_weight(F_MM0);
         } else {
             // acoustic free surface: the mu -> 0 limit of the elastic weights, (2 P1 + P2) -> 1/kappa
-            m.w[F_MM0][o] = y_factor(F_MM0, mul(__ddiv_rn(1., (double)lam), fx));
+            m.w[F_MM0][o] = y_factor(F_MM0, mul(__ddiv_rn(1., kval(lam)), fx));
         }
     }
 }
 
-template <class C>
+template <class C, class K>
 void launch_material_finalize(const MaterialArgs &m, cudaStream_t st)
 {
     const dim3 b(32, 8), g((m.My + 1 + 31) / 32, (m.Mx + 1 + 7) / 8);
-    k_material_finalize<C><<<g, b, 0, st>>>(m);
+    k_material_finalize<C, K><<<g, b, 0, st>>>(m);
 }
-template void launch_material_finalize<double>(const MaterialArgs &, cudaStream_t);
-template void launch_material_finalize<float>(const MaterialArgs &, cudaStream_t);
+template void launch_material_finalize<double, double>(const MaterialArgs &, cudaStream_t);
+template void launch_material_finalize<float, float>(const MaterialArgs &, cudaStream_t);
+template void launch_material_finalize<float, __half>(const MaterialArgs &, cudaStream_t);
 
 // ---------------------------------------------------------------- discrete energy (FP64)
 __device__ __forceinline__ double warp_sum(double v)

@@ -3,5 +3,5 @@
 
 namespace tw {
 template cudaError_t prepare_fused<__nv_bfloat16, float>();
-template void launch_fused<__nv_bfloat16, float>(const FusedArgs<__nv_bfloat16, float> &, int, bool, cudaStream_t);
+template void launch_fused<__nv_bfloat16, float>(const FusedArgs<__nv_bfloat16, float> &, int, bool, bool, cudaStream_t);
 }  // namespace tw

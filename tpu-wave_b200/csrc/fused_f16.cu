@@ -3,5 +3,5 @@
 
 namespace tw {
 template cudaError_t prepare_fused<__half, float>();
-template void launch_fused<__half, float>(const FusedArgs<__half, float> &, int, bool, cudaStream_t);
+template void launch_fused<__half, float>(const FusedArgs<__half, float> &, int, bool, bool, cudaStream_t);
 }  // namespace tw

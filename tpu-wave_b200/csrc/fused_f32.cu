@@ -3,5 +3,5 @@
 
 namespace tw {
 template cudaError_t prepare_fused<float, float>();
-template void launch_fused<float, float>(const FusedArgs<float, float> &, int, bool, cudaStream_t);
+template void launch_fused<float, float>(const FusedArgs<float, float> &, int, bool, bool, cudaStream_t);
 }  // namespace tw

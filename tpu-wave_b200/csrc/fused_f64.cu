@@ -3,5 +3,5 @@
 
 namespace tw {
 template cudaError_t prepare_fused<double, double>();
-template void launch_fused<double, double>(const FusedArgs<double, double> &, int, bool, cudaStream_t);
+template void launch_fused<double, double>(const FusedArgs<double, double> &, int, bool, bool, cudaStream_t);
 }  // namespace tw

@@ -132,15 +132,15 @@ struct Row {   // global values one interior iteration consumes
 template <class C, bool ENERGY>
 constexpr int ring_depth() { return (sizeof(C) == 8 || ENERGY) ? 2 : TW_FS_RING; }
 
-template <class S, class C, int CPST, bool ENERGY>
+template <class S, class C, int CPST, bool ENERGY, class K = C>
 struct RingLayout {
     static constexpr bool KR = Cpst<CPST>::keep_r, KC = Cpst<CPST>::keep_c, SPLIT = Cpst<CPST>::split;
     // slots of the storage type: nn, mm0, mm1, vmn, vnm; their lo parts (split); the residuals
     // rmn, rnm, rnn, rm0, rm1 (R and C codes)
     static constexpr int NS = 5 + (SPLIT ? 5 : 0) + ((KR || KC) ? 5 : 0);
-    static constexpr int NC = 5;                      // pmn, pnm, mu, lam, m2
+    static constexpr int NC = 5;                      // pmn, pnm, mu, lam, m2 (coefficient type K)
     static constexpr int NE = ENERGY ? 5 : 0;         // wmn, wnm, wnn, wm3, wm4 (double)
-    static constexpr int s_bytes = 32 * 2 * (int)sizeof(S), c_bytes = 32 * 2 * (int)sizeof(C), e_bytes = 32 * 16;
+    static constexpr int s_bytes = 32 * 2 * (int)sizeof(S), c_bytes = 32 * 2 * (int)sizeof(K), e_bytes = 32 * 16;
     static constexpr int stage = NS * s_bytes + NC * c_bytes + NE * e_bytes;
     static constexpr int warp = stage * ring_depth<C, ENERGY>();
 };
@@ -167,7 +167,7 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // EDGE: the strip touches the periodic wrap or the end of a row, so lanes may have non-adjacent
 // physical columns, unowned columns or the seam; otherwise every pair is adjacent, aligned and
 // owned by the core lanes, and loads and stores are single vector accesses
-template <class S, class C, int CPST, bool ENERGY, bool EDGE>
+template <class S, class C, int CPST, bool ENERGY, bool EDGE, class K>
 __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int it, int rcv_b, int rcv_e, EAcc &E,
                               unsigned char *ring)
 {
@@ -217,11 +217,12 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
     };
     // ---- row staging: issue(j, st) copies row j's values into ring stage st, read(st, in)
     // converts them into `in`
-    using RL = RingLayout<S, C, CPST, ENERGY>;
+    using RL = RingLayout<S, C, CPST, ENERGY, K>;
     constexpr int D = ring_depth<C, ENERGY>();
     const int l = lane;
     auto sslot = [&](int st, int k) { return ring + st * RL::stage + k * RL::s_bytes + l * 2 * (int)sizeof(S); };
-    auto cslot = [&](int st, int k) { return ring + st * RL::stage + RL::NS * RL::s_bytes + k * RL::c_bytes + l * 2 * (int)sizeof(C); };
+    auto cslot = [&](int st, int k) { return ring + st * RL::stage + RL::NS * RL::s_bytes + k * RL::c_bytes + l * 2 * (int)sizeof(K); };
+    auto coef = [&](int f) { return reinterpret_cast<const K *>(a.coef[f]); };
     auto eslot = [&](int st, int k) {
         return ring + st * RL::stage + RL::NS * RL::s_bytes + RL::NC * RL::c_bytes + k * RL::e_bytes + l * 16;
     };
@@ -263,11 +264,11 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
             put2(sslot(st, k + 3), rowp(a.rin[F_MM0], i), pM0, pM1, srow);
             put2(sslot(st, k + 4), rowp(a.rin[F_MM1], i), pM0, pM1, srow);
         }
-        put2(cslot(st, 0), a.coef[F_MN] + j * pitch, pN0, pN1, true);
-        put2(cslot(st, 1), a.coef[F_NM] + j * pitch, pM0, pM1, true);
-        put2(cslot(st, 2), a.coef[F_NN] + i * pitch, pN0, pN1, srow);
-        put2(cslot(st, 3), a.coef[F_MM0] + i * pitch, pM0, pM1, srow);
-        put2(cslot(st, 4), a.coef[F_MM1] + i * pitch, pM0, pM1, srow);
+        put2(cslot(st, 0), coef(F_MN) + j * pitch, pN0, pN1, true);
+        put2(cslot(st, 1), coef(F_NM) + j * pitch, pM0, pM1, true);
+        put2(cslot(st, 2), coef(F_NN) + i * pitch, pN0, pN1, srow);
+        put2(cslot(st, 3), coef(F_MM0) + i * pitch, pM0, pM1, srow);
+        put2(cslot(st, 4), coef(F_MM1) + i * pitch, pM0, pM1, srow);
         if constexpr (ENERGY) {
             const bool vrow = core && j >= x0 && j < x1;
             put2(eslot(st, 0), a.w[F_MN] + j * pitch, pN0, pN1, vrow);
@@ -282,8 +283,8 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
         return P2<C>{to_c<C>(v.x), to_c<C>(v.y)};
     };
     auto rdC = [&](int st, int k) {
-        const typename Vec2<C>::T v = *reinterpret_cast<const typename Vec2<C>::T *>(cslot(st, k));
-        return P2<C>{v.x, v.y};
+        const typename Vec2<K>::T v = *reinterpret_cast<const typename Vec2<K>::T *>(cslot(st, k));
+        return P2<C>{to_c<C>(v.x), to_c<C>(v.y)};
     };
     auto rdF = [&](int st, int k) {   // a field pair as the stencil reads it
         P2<C> v = rdS(st, k);
@@ -603,7 +604,7 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
 }
 
 // ------------------------------------------------------------------------------- boundary CTA
-template <class S, class C, int CPST, bool ENERGY>
+template <class S, class C, int CPST, bool ENERGY, class K>
 __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int it, int rcv_b, int rcv_e, C *tile,
                              EAcc &E)
 {
@@ -662,7 +663,7 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
             if (j < Mx) {   // MN
                 C r, cc;
                 ldr(F_MN, j, pN, r, cc);
-                const C P = __ldg(a.coef[F_MN] + (long)j * pitch + pN);
+                const C P = ld<C>(reinterpret_cast<const K *>(a.coef[F_MN]), (long)j * pitch + pN);
                 C v = dx_from_N<C>(a.op, FA(F_NN), pitch, Mx, j, pN);
                 r = add(r, mul(v, P));
                 if (sat_MN<C>(a.op, FA(F_NN), pitch, Mx, j, pN, v)) r = add(r, mul(v, P));
@@ -682,7 +683,7 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
             {   // NM
                 C r, cc;
                 ldr(F_NM, j, pM, r, cc);
-                const C P = __ldg(a.coef[F_NM] + (long)j * pitch + pM);
+                const C P = ld<C>(reinterpret_cast<const K *>(a.coef[F_NM]), (long)j * pitch + pM);
                 C v = dx_from_M<C>(a.op, FA(F_MM0), pitch, Mx, j, pM);
                 r = add(r, mul(v, P));
                 if (sat_NM<C>(a.op, FA(F_MM0), pitch, Mx, j, pM, v)) r = add(r, mul(v, P));
@@ -709,7 +710,7 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
             if (ownN) {   // NN
                 C r, cc;
                 ldr(F_NN, i, c, r, cc);
-                const C P = __ldg(a.coef[F_NN] + o);
+                const C P = ld<C>(reinterpret_cast<const K *>(a.coef[F_NN]), o);
                 C v = dxM<C>(a.op, Mx, i, [&](int rr) { return tMN[(rr - vr0) * NT + t]; });
                 r = add(r, mul(v, P));
                 v = C(0);
@@ -733,7 +734,8 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
                 C r0, k0, r1, k1;
                 ldr(F_MM0, i, c, r0, k0);
                 ldr(F_MM1, i, c, r1, k1);
-                const C L = __ldg(a.coef[F_MM0] + o), M2 = __ldg(a.coef[F_MM1] + o);
+                const C L = ld<C>(reinterpret_cast<const K *>(a.coef[F_MM0]), o),
+                        M2 = ld<C>(reinterpret_cast<const K *>(a.coef[F_MM1]), o);
                 C v = dxN<C>(a.op, Mx, i, [&](int rr) { return tNM[(rr - vr0) * NT + t]; });
                 r0 = add(r0, mul(v, L));
                 r1 = add(r1, mul(v, L));
@@ -771,7 +773,7 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
 }
 
 // ------------------------------------------------------------------------------- the launch
-template <class S, class C, int CPST, bool ENERGY>
+template <class S, class C, int CPST, bool ENERGY, class K>
 __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 4 : TW_FS_MIN_BLOCKS) k_elastic_fused(FusedArgs<S, C> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -785,13 +787,13 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 4 : TW_FS_MIN_BLOCKS)
         if (gw < a.n_int_seg * a.n_wstrip) {
             const int seg = gw / a.n_wstrip, wstrip = gw - seg * a.n_wstrip;
             const int y0 = wstrip * FS_WARP_CORE;
-            unsigned char *ring = smem_raw + (threadIdx.x >> 5) * RingLayout<S, C, CPST, ENERGY>::warp;
-            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
-            else interior_warp<S, C, CPST, ENERGY, true>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
+            unsigned char *ring = smem_raw + (threadIdx.x >> 5) * RingLayout<S, C, CPST, ENERGY, K>::warp;
+            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false, K>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
+            else interior_warp<S, C, CPST, ENERGY, true, K>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
         }
     } else {             // boundary CTA (zone, strip)
         const int b = cta - n_int;
-        boundary_cta<S, C, CPST, ENERGY>(a, b % a.n_bstrip, b / a.n_bstrip, it, rcv_b, rcv_e,
+        boundary_cta<S, C, CPST, ENERGY, K>(a, b % a.n_bstrip, b / a.n_bstrip, it, rcv_b, rcv_e,
                                          reinterpret_cast<C *>(smem_raw), E);
     }
     if (ENERGY) {
@@ -826,23 +828,23 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 4 : TW_FS_MIN_BLOCKS)
 
 // ------------------------------------------------------------------------------- launcher
 // dynamic shared memory: the boundary CTAs' velocity tile or the interior warps' rings
-template <class S, class C, int CPST, bool ENERGY>
+template <class S, class C, int CPST, bool ENERGY, class K = C>
 size_t fused_smem_bytes(int tile_rows)
 {
     const size_t tile = sizeof(C) * 2 * (size_t)tile_rows * FS_BND_W;
-    const size_t rings = (size_t)FS_WARPS * RingLayout<S, C, CPST, ENERGY>::warp;
+    const size_t rings = (size_t)FS_WARPS * RingLayout<S, C, CPST, ENERGY, K>::warp;
     return tile > rings ? tile : rings;
 }
 
 namespace {
-template <class S, class C, int N>
+template <class S, class C, int N, class K = C>
 cudaError_t set_attr(int)
 {
-    cudaError_t e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)fused_smem_bytes<S, C, N, true>(FS_SMALL_MX + 1));
+    cudaError_t e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, true, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)fused_smem_bytes<S, C, N, true, K>(FS_SMALL_MX + 1));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_elastic_fused<S, C, N, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)fused_smem_bytes<S, C, N, false>(FS_SMALL_MX + 1));
+    return cudaFuncSetAttribute(k_elastic_fused<S, C, N, false, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)fused_smem_bytes<S, C, N, false, K>(FS_SMALL_MX + 1));
 }
 }  // namespace
 
@@ -854,10 +856,14 @@ cudaError_t prepare_fused()
 {
     const int smem = 0;
     cudaError_t e;
-    if constexpr (sizeof(S) < sizeof(C)) {   // 16-bit storage: plain or split
+    if constexpr (sizeof(S) < sizeof(C)) {   // 16-bit storage: plain or split; FP32 or FP16 coefficients
         if ((e = set_attr<S, C, 0>(smem)) != cudaSuccess) return e;
+        if ((e = set_attr<S, C, 0, __half>(smem)) != cudaSuccess) return e;
+        if ((e = set_attr<S, C, 7, __half>(smem)) != cudaSuccess) return e;
         return set_attr<S, C, 7>(smem);
     } else {
+        if constexpr (sizeof(C) == 4)        // FP32: FP16 coefficients with the plain update
+            if ((e = set_attr<S, C, 0, __half>(smem)) != cudaSuccess) return e;
         if ((e = set_attr<S, C, 0>(smem)) != cudaSuccess) return e;
         if ((e = set_attr<S, C, 1>(smem)) != cudaSuccess) return e;
         if ((e = set_attr<S, C, 2>(smem)) != cudaSuccess) return e;
@@ -869,13 +875,32 @@ cudaError_t prepare_fused()
 }
 
 template <class S, class C>
-void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, cudaStream_t st)
+void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, bool coef16, cudaStream_t st)
 {
     const dim3 grid(a.n_int_cta + a.n_zone * a.n_bstrip), block(FS_THREADS_MAX);
+    if constexpr (sizeof(C) == 4) {
+        if (coef16) {   // FP16 coefficients: plain update (and the split pair for 16-bit fields)
+#define TW_FUSED_CASE16(N)                                                                                                   \
+    case N:                                                                                                                  \
+        if (energy) k_elastic_fused<S, C, N, true, __half><<<grid, block, fused_smem_bytes<S, C, N, true, __half>(a.tile_rows), st>>>(a); \
+        else k_elastic_fused<S, C, N, false, __half><<<grid, block, fused_smem_bytes<S, C, N, false, __half>(a.tile_rows), st>>>(a);     \
+        break;
+            if constexpr (sizeof(S) < sizeof(C)) {
+                switch (cpst) {
+                    TW_FUSED_CASE16(0)
+                    TW_FUSED_CASE16(7)
+                }
+            } else {
+                switch (cpst) { TW_FUSED_CASE16(0) }
+            }
+#undef TW_FUSED_CASE16
+            return;
+        }
+    }
 #define TW_FUSED_CASE(N)                                                                                  \
     case N:                                                                                               \
-        if (energy) k_elastic_fused<S, C, N, true><<<grid, block, fused_smem_bytes<S, C, N, true>(a.tile_rows), st>>>(a); \
-        else k_elastic_fused<S, C, N, false><<<grid, block, fused_smem_bytes<S, C, N, false>(a.tile_rows), st>>>(a);     \
+        if (energy) k_elastic_fused<S, C, N, true, C><<<grid, block, fused_smem_bytes<S, C, N, true>(a.tile_rows), st>>>(a); \
+        else k_elastic_fused<S, C, N, false, C><<<grid, block, fused_smem_bytes<S, C, N, false>(a.tile_rows), st>>>(a);     \
         break;
     if constexpr (sizeof(S) < sizeof(C)) {
         switch (cpst) {

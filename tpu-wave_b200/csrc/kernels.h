@@ -29,10 +29,11 @@ struct MaterialArgs {
     double dx;
     double nxN[8], nxM[6];    // A_diag * dx rounded to the storage type: N-type L[4] R[4], M-type L[3] R[3]
     int physics, periodic;
+    int *err;                 // bit 2 set: a coefficient outside the normal range of the FP16 storage
 };
-// define the stepping coefficients and energy weights (make_density_reciprocal,
+// define the stepping coefficients (stored as K) and energy weights (make_density_reciprocal,
 // define_parameters_energy, adjust_parameters_energy_periodic)
-template <class C>
+template <class C, class K = C>
 void launch_material_finalize(const MaterialArgs &m, cudaStream_t st);
 
 template <class S, class C>
@@ -86,7 +87,7 @@ struct FusedArgs {
     S *out[5];                // state after the step
     const S *rin[5];          // compensation arrays before / after
     S *rout[5];
-    const C *coef[5];
+    const void *coef[5];     // stepping coefficients: the compute type, or FP16
     long pitch;
     int Mx, My;
     Ops<C> op;
@@ -109,7 +110,7 @@ struct FusedArgs {
     double *traces;
 };
 template <class S, class C>
-void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, cudaStream_t st);
+void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, bool coef16, cudaStream_t st);
 
 // fused periodic acoustic step (acoustic_fused.cu): one shot, or a batch of shots in one launch
 template <class S, class C>

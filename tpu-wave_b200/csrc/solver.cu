@@ -276,7 +276,7 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
         a.out[k] = (S *)fout[k];
         a.rin[k] = (const S *)rin[k];
         a.rout[k] = (S *)rout[k];
-        a.coef[k] = (const C *)s->coef[k];
+        a.coef[k] = s->coef[k];
         a.w[k] = s->w[k];
     }
     a.pitch = s->pitch;
@@ -302,7 +302,7 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
     a.rcv_off = s->d_rcv_off;
     a.rcv = s->d_rcv_list;
     a.traces = s->d_traces;
-    launch_fused<S, C>(a, s->d.cpst, s->d.energy != 0, st);
+    launch_fused<S, C>(a, s->d.cpst, s->d.energy != 0, s->d.coef_fp16 != 0, st);
 }
 
 // one fused elastic step from the current buffers into the other ones
@@ -395,9 +395,16 @@ int finalize_material(tw_solver *s)
         m.nxM[i] = f64 ? l : (double)(float)l;
         m.nxM[3 + i] = f64 ? r : (double)(float)r;
     }
-    if (f64) launch_material_finalize<double>(m, s->st);
-    else launch_material_finalize<float>(m, s->st);
+    m.err = s->d_err;
+    TW_CUDA(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->st));
+    if (f64) launch_material_finalize<double, double>(m, s->st);
+    else if (s->d.coef_fp16) launch_material_finalize<float, __half>(m, s->st);
+    else launch_material_finalize<float, float>(m, s->st);
     TW_CUDA(cudaGetLastError());
+    int herr = 0;
+    TW_CUDA(cudaMemcpyAsync(&herr, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    if (herr & 2) return TW_ERR_UNSUPPORTED;   // a coefficient outside the normal FP16 range
     s->mat_dirty = false;
     s->mat_ready = true;
     return TW_OK;
@@ -609,6 +616,11 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
     // storage type narrower than the FP32 compute type
     if (narrow && (d.physics != TW_ELASTIC || (d.cpst != TW_CPST_00 && d.cpst != TW_CPST_SPLIT))) return TW_ERR_UNSUPPORTED;
     if (!narrow && d.cpst == TW_CPST_SPLIT) return TW_ERR_UNSUPPORTED;
+    if (d.coef_fp16 != 0 && d.coef_fp16 != 1) return TW_ERR_INVALID;
+    // FP16 coefficients: elastic with FP32 arithmetic, plain update (or the split pair)
+    if (d.coef_fp16 && (d.physics != TW_ELASTIC || d.precision == TW_FP64 ||
+                        (d.cpst != TW_CPST_00 && d.cpst != TW_CPST_SPLIT)))
+        return TW_ERR_UNSUPPORTED;
     if (d.bc_x == TW_BC_PERIODIC && d.cpst != TW_CPST_00 && d.cpst != TW_CPST_3R && d.cpst != TW_CPST_6R)
         return TW_ERR_UNSUPPORTED;   // the single-core tree offers '0', '3', '6' (namespaces.hpp:665-667)
     if (d.Mx < 8 || d.My < 4 || d.Mx > (1L << 30) / 2 || d.My > (1L << 30) / 2) return TW_ERR_INVALID;
@@ -641,7 +653,7 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaSetDevice"));
     e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreate"));
-    const size_t csz = d.precision == TW_FP64 ? 8 : 4;
+    const size_t csz = d.precision == TW_FP64 ? 8 : (d.coef_fp16 ? 2 : 4);
     const bool cp = d.cpst != TW_CPST_00;
     for (int k = 0; k < 5; k++) {
         if (!s->has_slot(k)) continue;
@@ -1107,7 +1119,7 @@ int tw_get_info(tw_solver *s, tw_info *info)
     info->steps_done = s->steps_done;
     info->n_rcv = (int)(s->rcv_tab.size() / 4);
     const int nf = s->elastic ? 5 : 3;
-    const double csz = s->d.precision == TW_FP64 ? 8 : 4;
+    const double csz = s->d.precision == TW_FP64 ? 8 : (s->d.coef_fp16 ? 2 : 4);
     info->bytes_per_update = nf * (2.0 * s->esz + (s->d.cpst != TW_CPST_00 ? 2.0 * s->esz : 0.0)) + nf * csz;
     info->device_bytes = s->dev_bytes;
     return TW_OK;
@@ -1374,7 +1386,8 @@ extern "C" int tw_adjoint_gradient(tw_solver *s, int nt, const double *obs, int 
                                    double *const *g_state)
 {
     if (check(s) || nt < 1 || ckpt_every < 1 || (!obs && !s->rcv_tab.empty())) return TW_ERR_INVALID;
-    if (!s->elastic || s->d.cpst != TW_CPST_00 || (s->d.precision != TW_FP64 && s->d.precision != TW_FP32))
+    if (!s->elastic || s->d.cpst != TW_CPST_00 || (s->d.precision != TW_FP64 && s->d.precision != TW_FP32) ||
+        s->d.coef_fp16)
         return TW_ERR_UNSUPPORTED;
     if (!s->mat_ready) return TW_ERR_STATE;
     if (s->steps_done != 0) return TW_ERR_STATE;   // the forward sweep starts at step 0
