@@ -212,6 +212,11 @@ TW_API int tw_adjoint_gradient(tw_solver *s, int nt, const double *obs, int ckpt
                                double *const *g_grid, double *g_rho, double *g_vp, double *g_vs,
                                double *const *g_state);
 
+/* Data misfit of the recorded traces against observed ones: calculate_data_misfit
+ * (forward.cpp:414-445), sum over steps and fields of (trace - obs)^2 per receiver (no factor
+ * 1/2: twice tw_adjoint_gradient's J). obs: [n_rcv][2][steps_done]; per_rcv may be NULL. */
+TW_API int tw_data_misfit(tw_solver *s, const double *obs, double *total, double *per_rcv);
+
 /* ---- batched shots ---------------------------------------------------------------------
  * No counterpart in the reference, which runs one shot per process. A batch advances many
  * acoustic handles (the shots: independent grids of any sizes) together: each half-step is ONE

@@ -108,6 +108,7 @@ def lib() -> C.CDLL:
         L.tw_io_read_srcrcv.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.tw_io_read_model.argtypes = [C.c_char_p, C.c_long, C.c_long, dp]
         L.tw_io_write_records.argtypes = [vp, C.c_char_p, C.c_int, C.POINTER(C.c_int), C.c_int]
+        L.tw_data_misfit.argtypes = [vp, dp, dp, dp]
         L.tw_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
         L.tw_batch_destroy.argtypes = [vp]
         L.tw_batch_destroy.restype = None
@@ -340,6 +341,14 @@ class Solver:
         if state:
             out["state"] = dict(zip(("NN", "MN", "NM", "MM0", "MM1"), st))
         return out
+
+    def data_misfit(self, obs):
+        """(total, per receiver) sum of squared trace residuals (tw_data_misfit)."""
+        n = self.info().steps_done
+        o = np.ascontiguousarray(np.asarray(obs, np.float64).reshape(self.n_rcv, 2, n))
+        tot, per = C.c_double(), np.zeros(max(self.n_rcv, 1))
+        _ok(lib().tw_data_misfit(self.h, _dp(o), C.byref(tot), _dp(per)), "tw_data_misfit")
+        return tot.value, per[:self.n_rcv]
 
     def write_records(self, folder: str, src_index: int = 0, rcv_index=None, snapshots: bool = False):
         """The reference's Signal / Energy / Snapshot text files (tw_io_write_records)."""

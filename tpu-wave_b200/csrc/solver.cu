@@ -1050,6 +1050,31 @@ int tw_read_energy(tw_solver *s, double *E_k, double *E_p0, double *E_p1)
     return TW_OK;
 }
 
+int tw_data_misfit(tw_solver *s, const double *obs, double *total, double *per_rcv)
+{
+    if (check(s) || !obs) return TW_ERR_INVALID;
+    const int n = (int)(s->rcv_tab.size() / 4), nt = s->steps_done;
+    std::vector<double> tr(2 * (size_t)n * std::max(nt, 1));
+    if (n > 0 && nt > 0) {
+        const int rc = tw_read_receivers(s, tr.data());
+        if (rc != TW_OK) return rc;
+    }
+    double J = 0.;
+    for (int r = 0; r < n; r++) {
+        double Jr = 0.;   // sum over steps and the grid's fields, in the reference's order
+        const int nf = s->rcv_tab[4 * r + 1] >= 0 ? 2 : 1;
+        for (int it = 0; it < nt; it++)
+            for (int f = 0; f < nf; f++) {
+                const size_t i = (2 * (size_t)r + f) * nt + it;
+                Jr += (tr[i] - obs[i]) * (tr[i] - obs[i]);
+            }
+        if (per_rcv) per_rcv[r] = Jr;
+        J += Jr;
+    }
+    if (total) *total = J;
+    return TW_OK;
+}
+
 int tw_io_write_records(tw_solver *s, const char *folder, int src_index, const int *rcv_index, int snapshots)
 {
     if (check(s) || !folder) return TW_ERR_INVALID;
