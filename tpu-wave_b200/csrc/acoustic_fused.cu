@@ -26,10 +26,22 @@ struct ARow {   // global values one iteration consumes
 
 __device__ __forceinline__ int prow(int r, int Mx) { return r < 0 ? r + Mx : (r >= Mx ? r - Mx : r); }
 
+// per-lane row staging (as in the elastic step): slots of the storage type p1, vx, vy and the
+// residuals rx, ry, rp (R codes); slots of the compute type cx, cy, kap
+template <class S, class C, int CPST>
+struct ARing {
+    static constexpr bool KR = Cpst<CPST>::keep_r;
+    static constexpr int NS = 3 + (KR ? 3 : 0), NC = 3;
+    static constexpr int s_bytes = 32 * 2 * (int)sizeof(S), c_bytes = 32 * 2 * (int)sizeof(C);
+    static constexpr int stage = NS * s_bytes + NC * c_bytes;
+    static constexpr int depth = sizeof(C) == 8 ? 2 : TW_FS_RING;
+    static constexpr int warp = stage * depth;
+};
+
 }  // namespace
 
 template <class S, class C, int CPST, bool EDGE>
-__device__ void acoustic_warp(const AcShot<S, C> &a, int wstrip, int seg)
+__device__ void acoustic_warp(const AcShot<S, C> &a, int wstrip, int seg, unsigned char *ring)
 {
     constexpr bool KR = Cpst<CPST>::keep_r;
     const int lane = threadIdx.x & 31;
@@ -53,22 +65,59 @@ __device__ void acoustic_warp(const AcShot<S, C> &a, int wstrip, int seg)
         return ld2_any<C>(row, pa, pb);
     };
     auto rowp = [&](const auto *base, int r) { return base + (long)r * pitch; };
-    auto fetch = [&](int j, ARow<C> &in) {
-        in.p1 = ld2(rowp(a.in[F_MM0], prow(j + 1, Mx)), pM0, pM1);
+    using RG = ARing<S, C, CPST>;
+    constexpr int D = RG::depth;
+    auto sslot = [&](int st, int k) { return ring + st * RG::stage + k * RG::s_bytes + lane * 2 * (int)sizeof(S); };
+    auto cslot = [&](int st, int k) { return ring + st * RG::stage + RG::NS * RG::s_bytes + k * RG::c_bytes + lane * 2 * (int)sizeof(C); };
+    auto put2 = [&](unsigned char *dst, const auto *row, int pa, int pb, bool pred) {
+        using T = typename std::remove_cv<typename std::remove_pointer<decltype(row)>::type>::type;
+        if (!EDGE) {
+            cp_async<2 * (int)sizeof(T)>(dst, row + c0, pred);
+        } else {
+            cp_async<(int)sizeof(T)>(dst, row + pa, pred);
+            cp_async<(int)sizeof(T)>(dst + sizeof(T), row + pb, pred);
+        }
+    };
+    // row j's values into ring stage st (rows outside the segment's use are zero-filled, their
+    // addresses clamped into the grid)
+    auto issue = [&](int j, int st) {
         const int jn = nread(j, Mx);
-        in.vx = ld2(rowp(a.in[F_NM], jn), pM0, pM1);
-        in.cx = ld2(rowp(a.coef[F_NM], jn), pM0, pM1);
-        if (KR) in.rx = ld2(rowp(a.rin[F_NM], jn), pM0, pM1);
-        if (j >= x0 && j < x1) {
-            in.vy = ld2(rowp(a.in[F_MN], j), pN0, pN1);
-            in.cy = ld2(rowp(a.coef[F_MN], j), pN0, pN1);
-            if (KR) in.ry = ld2(rowp(a.rin[F_MN], j), pN0, pN1);
+        const bool vrow = j >= x0 && j < x1;
+        const int jv = vrow ? j : x0, i = j - 2;
+        const bool prw = i >= x0 && i < x1;
+        const int ip = prw ? i : x0;
+        put2(sslot(st, 0), rowp(a.in[F_MM0], prow(j + 1, Mx)), pM0, pM1, true);
+        put2(sslot(st, 1), rowp(a.in[F_NM], jn), pM0, pM1, true);
+        put2(sslot(st, 2), rowp(a.in[F_MN], jv), pN0, pN1, vrow);
+        if constexpr (KR) {
+            put2(sslot(st, 3), rowp(a.rin[F_NM], jn), pM0, pM1, true);
+            put2(sslot(st, 4), rowp(a.rin[F_MN], jv), pN0, pN1, vrow);
+            put2(sslot(st, 5), rowp(a.rin[F_MM0], ip), pM0, pM1, prw);
         }
-        const int i = j - 2;
-        if (i >= x0 && i < x1) {
-            in.kap = ld2(rowp(a.coef[F_MM0], i), pM0, pM1);
-            if (KR) in.rp = ld2(rowp(a.rin[F_MM0], i), pM0, pM1);
+        put2(cslot(st, 0), rowp(a.coef[F_NM], jn), pM0, pM1, true);
+        put2(cslot(st, 1), rowp(a.coef[F_MN], jv), pN0, pN1, vrow);
+        put2(cslot(st, 2), rowp(a.coef[F_MM0], ip), pM0, pM1, prw);
+    };
+    auto read = [&](int st, ARow<C> &in) {
+        auto rS = [&](int k) {
+            const typename Vec2<S>::T v = *reinterpret_cast<const typename Vec2<S>::T *>(sslot(st, k));
+            return P2<C>{to_c<C>(v.x), to_c<C>(v.y)};
+        };
+        auto rC = [&](int k) {
+            const typename Vec2<C>::T v = *reinterpret_cast<const typename Vec2<C>::T *>(cslot(st, k));
+            return P2<C>{v.x, v.y};
+        };
+        in.p1 = rS(0);
+        in.vx = rS(1);
+        in.vy = rS(2);
+        if constexpr (KR) {
+            in.rx = rS(3);
+            in.ry = rS(4);
+            in.rp = rS(5);
         }
+        in.cx = rC(0);
+        in.cy = rC(1);
+        in.kap = rC(2);
     };
 
     // receivers of this lane's columns (at most RC kept in registers; more: scan the shot's list).
@@ -139,11 +188,20 @@ __device__ void acoustic_warp(const AcShot<S, C> &a, int wstrip, int seg)
     const int jb = x0 - 1, je = x1 + 1;
 #pragma unroll
     for (int q = 0; q < 3; q++) Pw[q] = ld2(rowp(a.in[F_MM0], prow(jb - 2 + q, Mx)), pM0, pM1);
-    ARow<C> cur, nxt;
-    fetch(jb, nxt);
+    ARow<C> cur;
+#pragma unroll
+    for (int q = 0; q < D - 1; q++) {   // the first D - 1 rows in flight
+        if (jb + q <= je) issue(jb + q, q);
+        cp_async_commit();
+    }
+    int sr = 0;   // ring stage of row j
     for (int j = jb; j <= je; j++) {
-        cur = nxt;
-        if (j < je) fetch(j + 1, nxt);
+        // row j + D - 1 into the stage row j - 1 used (read in the previous iteration)
+        if (j + D - 1 <= je) issue(j + D - 1, sr == 0 ? D - 1 : sr - 1);
+        cp_async_commit();
+        cp_async_wait<D - 1>();
+        read(sr, cur);
+        sr = sr + 1 == D ? 0 : sr + 1;
         Pw[3] = cur.p1;
         {   // Vx (NM) row j: x derivative of the pressure rows j-2..j+1 (dx_periodic<false>)
             P2<C> v{C(0), C(0)};
@@ -207,12 +265,15 @@ __device__ void acoustic_warp(const AcShot<S, C> &a, int wstrip, int seg)
 #pragma unroll
         for (int q = 0; q < 2; q++) Yw[q] = Yw[q + 1];
     }
+    cp_async_wait_all();
 }
 
 // warp gw of the launch -> (shot, segment, strip); the last CTA advances every shot's step
 template <class S, class C, int CPST>
 __device__ __forceinline__ void acoustic_fused_body(const AcShot<S, C> *shots, int n_shots, int n_warps, int *done)
 {
+    extern __shared__ __align__(16) unsigned char smem_ac[];
+    unsigned char *ring = smem_ac + (threadIdx.x >> 5) * ARing<S, C, CPST>::warp;
     const int gw = blockIdx.x * FS_WARPS + (threadIdx.x >> 5);
     if (gw < n_warps) {
         int lo = 0, hi = n_shots - 1;   // the shot whose warp range holds gw
@@ -224,8 +285,8 @@ __device__ __forceinline__ void acoustic_fused_body(const AcShot<S, C> *shots, i
         const AcShot<S, C> &a = shots[lo];
         const int local = gw - a.warp_off, seg = local / a.n_wstrip, wstrip = local - seg * a.n_wstrip;
         const int y0 = wstrip * FS_WARP_CORE;
-        if (y0 >= 4 && y0 + 60 <= a.My) acoustic_warp<S, C, CPST, false>(a, wstrip, seg);
-        else acoustic_warp<S, C, CPST, true>(a, wstrip, seg);
+        if (y0 >= 4 && y0 + 60 <= a.My) acoustic_warp<S, C, CPST, false>(a, wstrip, seg, ring);
+        else acoustic_warp<S, C, CPST, true>(a, wstrip, seg, ring);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -252,14 +313,17 @@ __global__ void __launch_bounds__(FS_THREADS_MAX) k_acoustic_fused_batch(const A
     acoustic_fused_body<S, C, CPST>(shots, n_shots, n_warps, done);
 }
 
+template <class S, class C, int CPST>
+constexpr size_t ac_smem() { return (size_t)FS_WARPS * ARing<S, C, CPST>::warp; }
+
 template <class S, class C>
 void launch_acoustic_fused(const AcShot<S, C> &a, int cpst, int *done, cudaStream_t st)
 {
     const int warps = a.n_seg * a.n_wstrip;
     const dim3 grid((warps + FS_WARPS - 1) / FS_WARPS), block(FS_THREADS_MAX);
-    if (cpst == 0) k_acoustic_fused_one<S, C, 0><<<grid, block, 0, st>>>(a, done);
-    else if (cpst == 4) k_acoustic_fused_one<S, C, 4><<<grid, block, 0, st>>>(a, done);
-    else k_acoustic_fused_one<S, C, 6><<<grid, block, 0, st>>>(a, done);
+    if (cpst == 0) k_acoustic_fused_one<S, C, 0><<<grid, block, ac_smem<S, C, 0>(), st>>>(a, done);
+    else if (cpst == 4) k_acoustic_fused_one<S, C, 4><<<grid, block, ac_smem<S, C, 4>(), st>>>(a, done);
+    else k_acoustic_fused_one<S, C, 6><<<grid, block, ac_smem<S, C, 6>(), st>>>(a, done);
 }
 
 template <class S, class C>
@@ -267,9 +331,9 @@ void launch_acoustic_fused_batch(const AcShot<S, C> *shots, int n_shots, int n_w
                                  cudaStream_t st)
 {
     const dim3 grid((n_warps + FS_WARPS - 1) / FS_WARPS), block(FS_THREADS_MAX);
-    if (cpst == 0) k_acoustic_fused_batch<S, C, 0><<<grid, block, 0, st>>>(shots, n_shots, n_warps, done);
-    else if (cpst == 4) k_acoustic_fused_batch<S, C, 4><<<grid, block, 0, st>>>(shots, n_shots, n_warps, done);
-    else k_acoustic_fused_batch<S, C, 6><<<grid, block, 0, st>>>(shots, n_shots, n_warps, done);
+    if (cpst == 0) k_acoustic_fused_batch<S, C, 0><<<grid, block, ac_smem<S, C, 0>(), st>>>(shots, n_shots, n_warps, done);
+    else if (cpst == 4) k_acoustic_fused_batch<S, C, 4><<<grid, block, ac_smem<S, C, 4>(), st>>>(shots, n_shots, n_warps, done);
+    else k_acoustic_fused_batch<S, C, 6><<<grid, block, ac_smem<S, C, 6>(), st>>>(shots, n_shots, n_warps, done);
 }
 
 template void launch_acoustic_fused<double, double>(const AcShot<double, double> &, int, int *, cudaStream_t);
