@@ -94,6 +94,9 @@ typedef struct {
     int n_rcv;
     double bytes_per_update;       /* compulsory HBM bytes per cell-update of one step */
     double device_bytes;           /* device memory held by the handle */
+    long row_off;                  /* a slab: global row of its local row 0 (0 otherwise) */
+    long own_rows[2];              /* a slab: the global rows [own_rows[0], own_rows[1]) it owns */
+    long Mx_glob;                  /* cells along x of the whole grid */
 } tw_info;
 
 typedef struct tw_solver tw_solver;
@@ -190,6 +193,33 @@ TW_API int tw_material_map_noalloc(const double *d_rho, const double *d_vp, cons
                                    long My_prmt, int num_dxM, int den_dxM, long Mx, long My, int num_dx,
                                    int den_dx, double *d_NN_mu, double *d_MN_rho, double *d_NM_rho,
                                    double *d_MM_lambda, double *d_MM_2mu, void *stream);
+
+/* ---- slab decomposition ------------------------------------------------------------------
+ * One elastic grid split along x (data rows) into slabs, each a handle of its own (its own GPU,
+ * or all on one). SURVEY-style row decomposition as the reference's MPI tree exchanges halo strips
+ * (mpi/src/cpp/namespaces.hpp:611-635), here four rows wide once per step, since a fused step
+ * reaches four rows of the old state. tw_create_slab makes the handle of global rows
+ * [row0, row1) of the grid `desc` describes (desc->Mx is the whole grid's): its arrays hold those
+ * rows plus four halo rows at each edge that is not a free surface; the free-surface closures and
+ * SAT terms apply only at the whole grid's top and bottom. Slabs need at least 16 rows, and at
+ * least 16 rows from an inner cut to a free surface. Set-up takes the whole grid's terms: the model,
+ * tw_set_material_grid arrays, source and receiver indices are global; a slab keeps the source
+ * and the receivers in its own rows (the others record zeros, so traces and energies of all slabs
+ * add up to the whole grid's). Field readback and writes are the slab's local arrays (halo rows
+ * included; tw_get_info gives the offset and the owned rows). Step every slab, then exchange. */
+TW_API int tw_create_slab(tw_solver **out, const tw_grid_desc *desc, long row0, long row1);
+/* Refresh the halo rows of two vertically adjacent slabs (upper owns the rows just above lower's)
+ * from each other's current state: device-to-device copies, any devices (peer or staged). Waits for
+ * both handles' queued work first. A multi-GPU driver may instead move the same rows with NCCL,
+ * through tw_slab_halo. */
+TW_API int tw_slab_exchange(tw_solver *upper, tw_solver *lower);
+/* The rows a slab sends or receives at one edge, for a caller's own transport (NCCL send/recv):
+ * side 0 top, 1 bottom; recv 0: the owned rows the neighbour needs, 1: the halo rows to fill.
+ * For field slot f (0 NN, 1 MN, 2 NM, 3 sxx, 4 syy; 5-9 their compensation arrays when present):
+ * device pointer of the first row, row count, row length and row pitch in bytes, of the current
+ * buffers (they alternate between steps). */
+TW_API int tw_slab_halo(tw_solver *s, int side, int recv, int f, void **ptr, long *rows, long *row_bytes,
+                        long *pitch_bytes);
 
 /* ---- adjoint gradient ---------------------------------------------------------------------
  * No counterpart in the reference (it has no adjoint). Full-waveform gradient of the misfit

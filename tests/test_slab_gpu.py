@@ -1,0 +1,91 @@
+"""Slab decomposition of one elastic grid (tw_create_slab / tw_slab_exchange), on one GPU: the
+grid cut into slabs along x, every slab stepped and the halos exchanged after each step, must
+give the whole grid's fields on every owned row and its traces bit for bit, and its energies to
+1e-12 (sums in another order). Covers the free-surface zones of the first and last slab, open
+inner edges, compensation arrays in the halo, sources and receivers in any slab."""
+import numpy as np
+import pytest
+
+from cases import elastic_case, load_twave
+
+pytestmark = pytest.mark.gpu
+SLOTS = None
+
+
+def run(tw, case, prec, cuts, f0, r0, Nt, slab=True):
+    shp = (case.Mx + 2, case.My + 2)
+    kw = dict(precision=prec, cpst=case.cpst, central_f=case.central_f, time_delay=case.time_delay, max_steps=Nt)
+    slots = [(tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)]
+    if slab:
+        hs = [tw.Solver.slab(case.Mx, case.My, 1, case.den_dx, case.dt, a, b, **kw) for a, b in zip(cuts[:-1], cuts[1:])]
+    else:
+        hs = [tw.Solver(case.Mx, case.My, 1, case.den_dx, case.dt, **kw)]
+    for h in hs:
+        h.set_material_model(case.rho.reshape(shp), case.vp.reshape(shp), case.vs.reshape(shp))
+        h.set_source_location(*case.src)
+        for r in case.rcvs:
+            h.add_receiver_location(*r)
+        off = h.row_off if slab else 0
+        for (g, f), a in zip(slots, f0):
+            h.write_field(g, f, a[off:off + h.shape(g)[0]])
+        if r0 is not None:
+            for (g, f), a in zip(slots, r0):
+                h.write_resid(g, f, a[off:off + h.shape(g)[0]])
+    for _ in range(Nt):
+        for h in hs:
+            h.step(1)
+        for up, lo in zip(hs[:-1], hs[1:]):
+            up.exchange(lo)
+    for h in hs:
+        h.sync()
+    fields = [np.zeros_like(a) for a in f0]
+    for h in hs:
+        off = h.row_off if slab else 0
+        own = h.own if slab else (0, case.Mx)
+        for k, (g, f) in enumerate(slots):
+            loc = h.read_field(g, f)
+            hi = own[1] + (1 if (g in (tw.NN, tw.NM) and own[1] == case.Mx) else 0)
+            fields[k][own[0]:hi] = loc[own[0] - off:hi - off]
+    traces = sum(h.read_receivers() for h in hs)
+    energy = [sum(h.read_energy()[i] for h in hs) for i in range(3)]
+    for h in hs:
+        h.close()
+    return fields, traces, energy
+
+
+@pytest.mark.parametrize("prec,cpst", [("f32", "00"), ("f64", "6R"), ("f32", "3C")])
+@pytest.mark.parametrize("cuts", [(0, 24, 48, 72), (0, 40, 72), (0, 16, 56, 72)])
+def test_slabs_equal_the_whole_grid(prec, cpst, cuts):
+    tw = load_twave()
+    Mx, My, den, Nt = 72, 60, 72, 9
+    rcvs = [("N", "M", 2, den, 7, 2 * den), ("M", "M", 2 * 23 + 1, 2 * den, 2 * 9 + 1, 2 * den),
+            ("N", "N", 24, den, 31, den), ("M", "N", 2 * 40 + 1, 2 * den, 0, 1), ("N", "M", Mx, den, 2 * 59 + 1, 2 * den),
+            ("N", "N", 56, den, My, den)]
+    case = elastic_case(Mx, My, seed=5, cpst=cpst, Nt=Nt, den_dx=den, rcvs=rcvs,
+                        src=("M", "M", 2 * 47 + 1, 2 * den, 2 * 20 + 1, 2 * den))
+    rng = np.random.default_rng(4)
+    T = np.float64 if prec == "f64" else np.float32
+    shapes = [(Mx + 1, My + 1), (Mx, My + 1), (Mx + 1, My), (Mx, My), (Mx, My)]
+    f0 = [(rng.standard_normal(s) * 1e-2).astype(T).astype(np.float64) for s in shapes]
+    r0 = None if cpst == "00" else [(rng.standard_normal(s) * 1e-9).astype(T).astype(np.float64) for s in shapes]
+    want = run(tw, case, prec, None, f0, r0, Nt, slab=False)
+    got = run(tw, case, prec, cuts, f0, r0, Nt)
+    for k in range(5):
+        assert np.array_equal(got[0][k], want[0][k]), k
+    assert np.array_equal(got[1], want[1])
+    for a, b in zip(got[2], want[2]):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+def test_slab_arguments():
+    tw = load_twave()
+    with pytest.raises(tw.TwError):
+        tw.Solver.slab(72, 60, 1, 72, 1e-3, 0, 10)      # fewer than 16 rows
+    with pytest.raises(tw.TwError):
+        tw.Solver.slab(72, 60, 1, 72, 1e-3, 8, 40)      # an inner cut 8 rows from the free surface
+    a = tw.Solver.slab(72, 60, 1, 72, 1e-3, 0, 40)
+    b = tw.Solver.slab(72, 60, 1, 72, 1e-3, 48, 72)
+    with pytest.raises(tw.TwError):
+        a.exchange(b)                                     # not adjacent
+    a.close()
+    b.close()

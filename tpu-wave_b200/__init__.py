@@ -50,7 +50,8 @@ class GridDesc(C.Structure):
 
 class Info(C.Structure):
     _fields_ = [("rows", C.c_long * 4), ("cols", C.c_long * 4), ("pitch", C.c_long), ("steps_done", C.c_int),
-                ("n_rcv", C.c_int), ("bytes_per_update", C.c_double), ("device_bytes", C.c_double)]
+                ("n_rcv", C.c_int), ("bytes_per_update", C.c_double), ("device_bytes", C.c_double),
+                ("row_off", C.c_long), ("own_rows", C.c_long * 2), ("Mx_glob", C.c_long)]
 
 
 _lib = None
@@ -109,6 +110,9 @@ def lib() -> C.CDLL:
         L.tw_io_read_model.argtypes = [C.c_char_p, C.c_long, C.c_long, dp]
         L.tw_io_write_records.argtypes = [vp, C.c_char_p, C.c_int, C.POINTER(C.c_int), C.c_int]
         L.tw_data_misfit.argtypes = [vp, dp, dp, dp]
+        L.tw_create_slab.argtypes = [C.POINTER(vp), C.POINTER(GridDesc), C.c_long, C.c_long]
+        L.tw_slab_exchange.argtypes = [vp, vp]
+        L.tw_slab_halo.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(vp), lp, lp, lp]
         L.tw_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
         L.tw_batch_destroy.argtypes = [vp]
         L.tw_batch_destroy.restype = None
@@ -188,6 +192,30 @@ class Solver:
         self.Mx, self.My, self.physics, self.bc_x = Mx, My, physics, bc_x
         self.n_rcv = 0
 
+    @classmethod
+    def slab(cls, Mx: int, My: int, num_dx: int, den_dx: int, dt: float, row0: int, row1: int, **kw):
+        """The handle of global rows [row0, row1) of an Mx x My elastic grid (tw_create_slab)."""
+        self = cls.__new__(cls)
+        energy = kw.pop("energy", True)
+        self.desc = GridDesc(ELASTIC, SAT_FREE, PRECISION[kw.pop("precision", "f32")], CPST[kw.pop("cpst", "00")], Mx, My,
+                             num_dx, den_dx, dt, kw.pop("central_f", 5.0), kw.pop("time_delay", 0.25),
+                             kw.pop("source_scaling", 1.0), kw.pop("max_steps", 1000), 1 if energy else 0,
+                             kw.pop("device", 0), 1 if kw.pop("coef_fp16", False) else 0)
+        if kw:
+            raise TypeError(f"unexpected arguments {sorted(kw)}")
+        self.h = C.c_void_p()
+        _ok(lib().tw_create_slab(C.byref(self.h), C.byref(self.desc), row0, row1), "tw_create_slab")
+        inf = self.info()
+        self.Mx, self.My, self.physics, self.bc_x = int(inf.rows[3]), My, ELASTIC, SAT_FREE   # local cells
+        self.n_rcv = 0
+        self.Mx_glob = Mx
+        self.row_off, self.own = int(inf.row_off), (int(inf.own_rows[0]), int(inf.own_rows[1]))
+        return self
+
+    def exchange(self, lower: "Solver"):
+        """Refresh the halo rows shared with the slab just below (tw_slab_exchange)."""
+        _ok(lib().tw_slab_exchange(self.h, lower.h), "tw_slab_exchange")
+
     def close(self):
         if self.h:
             lib().tw_destroy(self.h)
@@ -212,7 +240,7 @@ class Solver:
 
     # ---- material
     def set_material_model(self, rho, vp, vs=None, Mx_prmt=None, My_prmt=None, num_dxM=None, den_dxM=None):
-        Mxp = self.Mx if Mx_prmt is None else Mx_prmt
+        Mxp = getattr(self, "Mx_glob", self.Mx) if Mx_prmt is None else Mx_prmt   # a slab: the whole grid's
         Myp = self.My if My_prmt is None else My_prmt
         nd = self.desc.num_dx if num_dxM is None else num_dxM
         dd = self.desc.den_dx if den_dxM is None else den_dxM

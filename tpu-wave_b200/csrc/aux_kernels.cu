@@ -28,11 +28,12 @@ void launch_model_derive(const double *rho, const double *vp, const double *vs, 
 // in units of the model spacing is num/den; its integer part indexes the padded model, the
 // remainder (computed in double) weights the four corners.
 __global__ void k_interp(int rows, int cols, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
-                         long Nxp, long Nyp, const double *in, double *out, int *err)
+                         long Nxp, long Nyp, const double *in, double *out, int *err, int row_off)
 {
     const int iy = blockIdx.x * blockDim.x + threadIdx.x;
-    const int ix = blockIdx.y * blockDim.y + threadIdx.y;
-    if (iy >= cols || ix >= rows) return;
+    const int il = blockIdx.y * blockDim.y + threadIdx.y;
+    if (iy >= cols || il >= rows) return;
+    const int ix = il + row_off;   // global row (a slab's local row il)
     long nx, dxl, ny, dyl;
     if (txN) { nx = (long)ix * num_dx; dxl = den_dx; } else { nx = (2L * ix + 1) * num_dx; dxl = 2L * den_dx; }
     if (tyN) { ny = (long)iy * num_dx; dyl = den_dx; } else { ny = (2L * iy + 1) * num_dx; dyl = 2L * den_dx; }
@@ -47,21 +48,25 @@ __global__ void k_interp(int rows, int cols, int txN, int tyN, int num_dx, int d
     v = add(v, mul(mul(a, eta), in[ixM * PS + iyM + 1]));
     v = add(v, mul(mul(xi, b), in[(ixM + 1) * PS + iyM]));
     v = add(v, mul(mul(xi, eta), in[(ixM + 1) * PS + iyM + 1]));
-    out[(long)ix * cols + iy] = v;
+    out[(long)il * cols + iy] = v;
 }
 
 void launch_interp(int rows, int cols, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
-                   long Nx_prmt, long Ny_prmt, const double *in, double *out, int *err, cudaStream_t st)
+                   long Nx_prmt, long Ny_prmt, const double *in, double *out, int *err, cudaStream_t st, int row_off)
 {
     const dim3 b(32, 8), g((cols + 31) / 32, (rows + 7) / 8);
-    k_interp<<<g, b, 0, st>>>(rows, cols, txN, tyN, num_dx, den_dx, num_dxM, den_dxM, Nx_prmt, Ny_prmt, in, out, err);
+    k_interp<<<g, b, 0, st>>>(rows, cols, txN, tyN, num_dx, den_dx, num_dxM, den_dxM, Nx_prmt, Ny_prmt, in, out, err,
+                              row_off);
 }
 
 // x factor of the energy norm for row ix of a grid with `rows` rows (adjust_parameters_energy_periodic,
 // grid_energy.cpp:69-119): A_diag * dx rounded to the storage type on the SAT boundary rows (the
 // host precomputes them into nxN / nxM), dx inside
-__device__ __forceinline__ double norm_x(const MaterialArgs &m, int txN, int rows, int ix)
+__device__ __forceinline__ double norm_x(const MaterialArgs &m, int txN, int rows_local, int il)
 {
+    // a slab's rows are global rows il + row_off of a grid of Mx_glob cells
+    (void)rows_local;
+    const int ix = il + m.row_off, rows = m.Mx_glob + (txN ? 1 : 0);
     if (txN) {
         if (ix < 4) return m.nxN[ix];
         if (ix >= rows - 4) return m.nxN[4 + ix - (rows - 4)];

@@ -181,9 +181,9 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
     const bool core = lane >= 2 && lane < 30;
     const bool oN0 = core && (!EDGE || c0 <= My), oN1 = core && (!EDGE || c1 <= My);
     const bool oM0 = core && (!EDGE || c0 < My), oM1 = core && (!EDGE || c1 < My);
-    // balanced segments of the interior rows [FS_ZONE, Mx - FS_ZONE)
-    const int x0 = FS_ZONE + (int)((long)seg * a.int_rows / a.n_int_seg);
-    const int x1 = FS_ZONE + (int)((long)(seg + 1) * a.int_rows / a.n_int_seg);   // rows [x0, x1)
+    // balanced segments of the interior rows [ir0, ir0 + int_rows)
+    const int x0 = a.ir0 + (int)((long)seg * a.int_rows / a.n_int_seg);
+    const int x1 = a.ir0 + (int)((long)(seg + 1) * a.int_rows / a.n_int_seg);   // rows [x0, x1)
     // NM columns next to the periodic seam read NN by the physical rule (column My and column 0
     // of an N-type-y grid are distinct points)
     const bool seam0 = EDGE && (c0 == -2 || c0 == -1 || c0 == My || c0 == My + 1);
@@ -620,8 +620,9 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
     const bool ownN = core && c <= My, ownM = core && c < My;
     const bool velT = t >= 2 && t < NT - 2;
     int zr0, zr1;   // zone rows (N-type grids up to zr1, M-type up to min(zr1, Mx - 1))
-    if (a.n_zone == 1) { zr0 = 0; zr1 = Mx; }
-    else if (zone == 0) { zr0 = 0; zr1 = FS_ZONE - 1; }
+    const int kind = a.zone_kind[zone];
+    if (kind == 2) { zr0 = 0; zr1 = Mx; }
+    else if (kind == 0) { zr0 = 0; zr1 = FS_ZONE - 1; }
     else { zr0 = Mx - FS_ZONE; zr1 = Mx; }
     const int vr0 = max(zr0 - 2, 0), vr1 = min(zr1 + 2, Mx);
     C *tMN = tile, *tNM = tile + a.tile_rows * NT;

@@ -17,7 +17,8 @@ void launch_model_derive(const double *rho, const double *vp, const double *vs, 
 // bilinear interpolation onto one grid (grid_parameter.cpp:7-60); out: rows x cols, compact.
 // err: set to 1 on an out-of-bounds model access.
 void launch_interp(int rows, int cols, int txN, int tyN, int num_dx, int den_dx, int num_dxM, int den_dxM,
-                   long Nx_prmt, long Ny_prmt, const double *in, double *out, int *err, cudaStream_t st);
+                   long Nx_prmt, long Ny_prmt, const double *in, double *out, int *err, cudaStream_t st,
+                   int row_off = 0);
 
 struct MaterialArgs {
     const double *mat[5];     // FP64 NN mu, MN rho, NM rho, MM lambda (kappa), MM 2mu; rows x cols
@@ -29,6 +30,7 @@ struct MaterialArgs {
     double dx;
     double nxN[8], nxM[6];    // A_diag * dx rounded to the storage type: N-type L[4] R[4], M-type L[3] R[3]
     int physics, periodic;
+    int row_off, Mx_glob;     // a slab: its local row 0 is global row row_off of a grid of Mx_glob cells
     int *err;                 // bit 2 set: a coefficient outside the normal range of the FP16 storage
 };
 // define the stepping coefficients (stored as K) and energy weights (make_density_reciprocal,
@@ -91,8 +93,10 @@ struct FusedArgs {
     long pitch;
     int Mx, My;
     Ops<C> op;
-    int n_int_seg, int_rows;  // interior rows [FS_ZONE, Mx - FS_ZONE) = int_rows, in n_int_seg balanced segments
-    int n_zone;               // 2 boundary zones, or 1 zone holding the whole grid
+    int n_int_seg, int_rows;  // interior rows [ir0, ir0 + int_rows), in n_int_seg balanced segments
+    int ir0;                  // FS_ZONE below a free surface; the halo depth below an open slab edge
+    int n_zone;               // boundary zones: 0, 1 or 2, of the kinds zone_kind[]
+    int zone_kind[2];         // 0: the FS_ZONE rows at the top free surface, 1: at the bottom, 2: the whole grid
     int n_wstrip, n_bstrip;   // interior warp strips, boundary strips
     int n_int_cta;            // interior CTAs: the n_int_seg x n_wstrip warps, FS_WARPS per CTA
     int tile_rows;

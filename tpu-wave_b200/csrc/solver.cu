@@ -78,6 +78,12 @@ struct tw_solver {
     void *f2[5] = {}, *res2[5] = {};
     int parity = 0;                   // which buffer holds the current state (0: f/res, 1: f2/res2)
     int n_int_seg = 0, int_rows = 0, n_zone = 1, n_wstrip = 0, n_bstrip = 1, n_int_cta = 0, tile_rows = 1;
+    int ir0 = FS_ZONE, zone_kind[2] = {0, 1};
+    // a slab of a larger grid (slab decomposition along x): local row r is global row r + row_off
+    // of a grid of Mx_glob cells; it owns global rows [own0, own1) of every grid (plus the last
+    // N-type row when it reaches the bottom); the rows beyond are halo, refreshed by tw_slab_exchange
+    bool slab = false;
+    long row_off = 0, Mx_glob = 0, own0 = 0, own1 = 0;
     int *d_done = nullptr, *d_rcv_off = nullptr, *d_rcv_list = nullptr;
     int rcv_list_cap = 0;
     double *w[5] = {}, *mat[5] = {};
@@ -150,6 +156,15 @@ void *cur_f(const tw_solver *s, int k) { return s->parity ? s->f2[k] : s->f[k]; 
 void *cur_res(const tw_solver *s, int k) { return s->parity ? s->res2[k] : s->res[k]; }
 
 // arguments of the in-place per-point kernels, on the current buffers
+// a slab's local row of global row gx of grid `grid`, or -1 when another slab owns it
+long owned_row(const tw_solver *s, int grid, long gx)
+{
+    if (!s->slab) return gx;
+    const bool Nx = grid == TW_NN || grid == TW_NM;
+    const bool own = (gx >= s->own0 && gx < s->own1) || (Nx && gx == s->Mx_glob && s->own1 == s->Mx_glob);
+    return own ? gx - s->row_off : -1;
+}
+
 template <class S, class C>
 StepArgs<S, C> step_args(const tw_solver *s)
 {
@@ -285,7 +300,10 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
     a.op = make_ops<C>((double)s->d.num_dx / (double)s->d.den_dx, s->d.dt, false);
     a.n_int_seg = s->n_int_seg;
     a.int_rows = s->int_rows;
+    a.ir0 = s->ir0;
     a.n_zone = s->n_zone;
+    a.zone_kind[0] = s->zone_kind[0];
+    a.zone_kind[1] = s->zone_kind[1];
     a.n_wstrip = s->n_wstrip;
     a.n_bstrip = s->n_bstrip;
     a.n_int_cta = s->n_int_cta;
@@ -384,6 +402,8 @@ int finalize_material(tw_solver *s)
     m.dx = (double)s->d.num_dx / (double)s->d.den_dx;
     m.physics = s->elastic ? 0 : 1;
     m.periodic = s->periodic;
+    m.row_off = (int)s->row_off;
+    m.Mx_glob = (int)s->Mx_glob;
     const bool f64 = s->d.precision == TW_FP64;
     for (int i = 0; i < 4; i++) {
         const double l = SbpTables::A_N_L[i] * m.dx, r = SbpTables::A_N_R[i] * m.dx;
@@ -457,14 +477,19 @@ int upload_receivers(tw_solver *s)
         const int Mx = (int)s->d.Mx;
         for (int r = 0; r < n; r++) {
             const int *q = &s->rcv_tab[4 * r];
+            if (q[0] < 0) continue;   // a receiver of another slab
             const int row = q[2], col = q[3];
+            int zone = -1;            // the boundary zone holding the row, if any
+            for (int z = 0; z < s->n_zone; z++) {
+                const int k = s->zone_kind[z];
+                if (k == 2 || (k == 0 && row < FS_ZONE) || (k == 1 && row >= Mx - FS_ZONE)) zone = z;
+            }
             int cta;
-            if (s->n_zone == 1 || row < FS_ZONE || row >= Mx - FS_ZONE) {
-                const int zone = (s->n_zone == 1 || row < FS_ZONE) ? 0 : 1;
+            if (zone >= 0) {
                 cta = n_int + zone * s->n_bstrip + col / FS_BND_TY;
             } else {
-                int seg = 0;   // the balanced segment holding the row (fused_step.cu)
-                while (FS_ZONE + (int)((long)(seg + 1) * s->int_rows / s->n_int_seg) <= row) seg++;
+                int seg = 0;   // the balanced segment holding the row (fused_step.cuh)
+                while (s->ir0 + (int)((long)(seg + 1) * s->int_rows / s->n_int_seg) <= row) seg++;
                 cta = (seg * s->n_wstrip + col / FS_WARP_CORE) / FS_WARPS;
             }
             for (int f = 0; f < 2; f++)
@@ -601,7 +626,42 @@ const char *tw_strerror(int status)
 
 const char *tw_last_cuda_error(void) { return g_cuda_error.c_str(); }
 
+namespace {
+struct SlabSpec {
+    bool on = false;
+    long row_off = 0, Mx_glob = 0, own0 = 0, own1 = 0;
+};
+int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl);
+}  // namespace
+
 int tw_create(tw_solver **out, const tw_grid_desc *desc)
+{
+    return create_impl(out, desc, SlabSpec{});
+}
+
+int tw_create_slab(tw_solver **out, const tw_grid_desc *desc, long row0, long row1)
+{
+    if (!out || !desc) return TW_ERR_INVALID;
+    *out = nullptr;
+    const tw_grid_desc &g = *desc;
+    if (g.physics != TW_ELASTIC || g.bc_x != TW_BC_SAT_FREE) return TW_ERR_UNSUPPORTED;
+    constexpr long H = 4;   // halo rows: the step's x stencils reach four rows of the old state
+    if (row0 < 0 || row1 > g.Mx || row1 - row0 < 2 * FS_ZONE || (row0 > 0 && row0 < 2 * FS_ZONE) ||
+        (row1 < g.Mx && g.Mx - row1 < 2 * FS_ZONE))
+        return TW_ERR_INVALID;
+    SlabSpec sl;
+    sl.on = true;
+    sl.Mx_glob = g.Mx;
+    sl.row_off = row0 > 0 ? row0 - H : 0;
+    sl.own0 = row0;
+    sl.own1 = row1;
+    tw_grid_desc d = g;
+    d.Mx = (row1 < g.Mx ? row1 + H : g.Mx) - sl.row_off;   // local cells
+    return create_impl(out, &d, sl);
+}
+
+namespace {
+int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
 {
     if (!out || !desc) return TW_ERR_INVALID;
     *out = nullptr;
@@ -630,6 +690,11 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
     tw_solver *s = new (std::nothrow) tw_solver();
     if (!s) return TW_ERR_NOMEM;
     s->d = d;
+    s->slab = sl.on;
+    s->row_off = sl.row_off;
+    s->Mx_glob = sl.on ? sl.Mx_glob : d.Mx;
+    s->own0 = sl.on ? sl.own0 : 0;
+    s->own1 = sl.on ? sl.own1 : d.Mx;
     s->elastic = d.physics == TW_ELASTIC;
     s->periodic = d.bc_x == TW_BC_PERIODIC;
     s->esz = d.precision == TW_FP64 ? 8 : (d.precision == TW_FP32 ? 4 : 2);
@@ -689,18 +754,25 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
         }
         s->n_bstrip = (int)((My + 1 + FS_BND_TY - 1) / FS_BND_TY);
         s->n_wstrip = (int)((My + 1 + FS_WARP_CORE - 1) / FS_WARP_CORE);
-        if (Mx < FS_SMALL_MX) {
+        if (!s->slab && Mx < FS_SMALL_MX) {
             s->n_int_seg = 0;
             s->n_zone = 1;
+            s->zone_kind[0] = 2;
             s->tile_rows = (int)Mx + 1;
         } else {
             // balanced interior segments: TW_FS_CTAS_PER_SM CTAs of work for each of the 148 SMs,
             // the boundary CTAs included, segments of 8 rows or more; the segment x strip warps are
-            // packed FS_WARPS to a CTA
-            s->n_zone = 2;
+            // packed FS_WARPS to a CTA. A slab has a free-surface zone only at a global boundary;
+            // at an open edge its interior reaches the four halo rows.
+            const bool top = s->row_off == 0, bot = s->row_off + Mx == s->Mx_glob;
+            s->n_zone = 0;
+            if (top) s->zone_kind[s->n_zone++] = 0;
+            if (bot) s->zone_kind[s->n_zone++] = 1;
             s->tile_rows = 12;
-            s->int_rows = (int)Mx - 2 * FS_ZONE;
-            const int target = std::max(1, (148 * TW_FS_CTAS_PER_SM - 2 * s->n_bstrip) * FS_WARPS / s->n_wstrip);
+            s->ir0 = top ? FS_ZONE : 4;
+            s->int_rows = (int)Mx - (bot ? FS_ZONE : 4) - s->ir0;
+            if (s->int_rows < 8) return fail(TW_ERR_INVALID);
+            const int target = std::max(1, (148 * TW_FS_CTAS_PER_SM - s->n_zone * s->n_bstrip) * FS_WARPS / s->n_wstrip);
             s->n_int_seg = std::max(1, std::min(target, s->int_rows / 8));
             s->n_int_cta = (s->n_int_seg * s->n_wstrip + FS_WARPS - 1) / FS_WARPS;
         }
@@ -748,6 +820,7 @@ int tw_create(tw_solver **out, const tw_grid_desc *desc)
     *out = s;
     return TW_OK;
 }
+}  // namespace
 
 void tw_destroy(tw_solver *s)
 {
@@ -764,7 +837,7 @@ int tw_set_material_model(tw_solver *s, const double *rho, const double *vp, con
     if (Mx_prmt < 1 || My_prmt < 1 || num_dxM <= 0 || den_dxM <= 0) return TW_ERR_INVALID;
     // the model must span the simulation region (input_processing.cpp:203-211)
     for (int dir = 0; dir < 2; dir++) {
-        const long pm = dir == 0 ? Mx_prmt : My_prmt, sm = dir == 0 ? s->d.Mx : s->d.My;
+        const long pm = dir == 0 ? Mx_prmt : My_prmt, sm = dir == 0 ? s->Mx_glob : s->d.My;
         if (pm * num_dxM * (long)s->d.den_dx != sm * (long)s->d.num_dx * den_dxM) return TW_ERR_INVALID;
     }
     TW_CUDA(cudaSetDevice(s->d.device));
@@ -788,7 +861,7 @@ int tw_set_material_model(tw_solver *s, const double *rho, const double *vp, con
     for (auto &j : jobs) {
         if (!s->has_slot(j.slot)) continue;
         launch_interp(s->rows[j.slot], s->cols[j.slot], j.txN, j.tyN, s->d.num_dx, s->d.den_dx, num_dxM, den_dxM, Nxp, Nyp, j.src,
-                      s->mat[j.slot], s->d_err, s->st);
+                      s->mat[j.slot], s->d_err, s->st, (int)s->row_off);
         s->mat_set[j.slot] = true;
     }
     int herr = 0;
@@ -826,8 +899,8 @@ int tw_set_material_grid(tw_solver *s, int grid, int idx, const double *coef, lo
     TW_CUDA(cudaSetDevice(s->d.device));
     const long R = s->rows[slot], Cn = s->cols[slot];
     std::vector<double> tmp((size_t)R * Cn);
-    for (long ix = 0; ix < R; ix++)
-        for (long iy = 0; iy < Cn; iy++) tmp[ix * Cn + iy] = coef[ix * ld + iy];
+    for (long ix = 0; ix < R; ix++)   // a slab: its rows of the global grid's array
+        for (long iy = 0; iy < Cn; iy++) tmp[ix * Cn + iy] = coef[(ix + s->row_off) * ld + iy];
     TW_CUDA(cudaMemcpyAsync(s->mat[slot], tmp.data(), sizeof(double) * tmp.size(), cudaMemcpyHostToDevice, s->st));
     TW_CUDA(cudaStreamSynchronize(s->st));
     s->mat_set[slot] = true;
@@ -847,13 +920,15 @@ int tw_set_source(tw_solver *s, int grid, long ix, long iy)
 {
     if (check(s) || grid < 0 || grid > 3) return TW_ERR_INVALID;
     if (!s->elastic && grid == TW_NN) return TW_ERR_INVALID;
-    if (ix < 0 || iy < 0 || ix >= s->ref_rows[grid] || iy >= s->ref_cols[grid]) return TW_ERR_OUTSIDE;
+    const long rows_g = s->ref_rows[grid] + (s->Mx_glob - s->d.Mx);   // global rows of the grid
+    if (ix < 0 || iy < 0 || ix >= rows_g || iy >= s->ref_cols[grid]) return TW_ERR_OUTSIDE;
     const bool Nx = grid == TW_NN || grid == TW_NM;
     // the reference stops on a source on the free-surface node rows (forward.cpp:95-96); on the
     // periodic seam it only warns (:97-98) and so does nothing here
-    if (!s->periodic && Nx && (ix == 0 || ix == s->d.Mx)) return TW_ERR_WEAK_BOUNDARY;
-    s->src_grid = grid;
-    s->src_ix = ix;
+    if (!s->periodic && Nx && (ix == 0 || ix == s->Mx_glob)) return TW_ERR_WEAK_BOUNDARY;
+    const long lx = owned_row(s, grid, ix);   // a slab injects only a source in its own rows
+    s->src_grid = lx >= 0 ? grid : -1;
+    s->src_ix = lx;
     s->src_iy = iy;
     TW_CUDA(cudaSetDevice(s->d.device));
     return rebuild_source_table(s);
@@ -887,8 +962,13 @@ int tw_add_receivers(tw_solver *s, int grid, const long *ix, const long *iy, int
     for (int k = 0; k < n; k++) {
         // the reference accepts indices up to and including the grid size (forward.cpp:154-155);
         // only points of the grid are accepted here
-        if (ix[k] < 0 || iy[k] < 0 || ix[k] >= s->ref_rows[grid] || iy[k] >= s->ref_cols[grid]) return TW_ERR_OUTSIDE;
-        add.insert(add.end(), {s0, s1, (int)ix[k], (int)iy[k]});
+        const long rows_g = s->ref_rows[grid] + (s->Mx_glob - s->d.Mx);
+        if (ix[k] < 0 || iy[k] < 0 || ix[k] >= rows_g || iy[k] >= s->ref_cols[grid]) return TW_ERR_OUTSIDE;
+        // a slab records only the receivers in its own rows; the others keep zero traces, so the
+        // traces of all slabs add up to the whole grid's
+        const long lx = owned_row(s, grid, ix[k]);
+        if (lx >= 0) add.insert(add.end(), {s0, s1, (int)lx, (int)iy[k]});
+        else add.insert(add.end(), {-1, -1, (int)ix[k], (int)iy[k]});
     }
     s->rcv_tab.insert(s->rcv_tab.end(), add.begin(), add.end());
     TW_CUDA(cudaSetDevice(s->d.device));
@@ -1050,6 +1130,64 @@ int tw_read_energy(tw_solver *s, double *E_k, double *E_p0, double *E_p1)
     return TW_OK;
 }
 
+// halo geometry of slot f (5..9: compensation arrays) at one edge of a slab
+int slab_rows(tw_solver *s, int side, int recv, int f, void **ptr, long *rows)
+{
+    if (!s->slab || side < 0 || side > 1 || f < 0 || f > 9) return TW_ERR_INVALID;
+    const int k = f % 5;
+    if (!s->has_slot(k) || (f >= 5 && !s->res[k])) return TW_ERR_INVALID;
+    const bool open_top = s->row_off > 0, open_bot = s->row_off + s->d.Mx < s->Mx_glob;
+    if ((side == 0 && !open_top) || (side == 1 && !open_bot)) return TW_ERR_INVALID;
+    constexpr long H = 4;
+    const long own0 = s->own0 - s->row_off, own1 = s->own1 - s->row_off;   // local owned rows
+    long r0;
+    if (side == 0) r0 = recv ? own0 - H : own0;   // top: halo above, or the first owned rows
+    else r0 = recv ? own1 : own1 - H;              // bottom: halo below, or the last owned rows
+    char *base = (char *)(f < 5 ? cur_f(s, k) : cur_res(s, k));
+    *ptr = base + (size_t)r0 * s->pitch * s->esz;
+    *rows = H;
+    return TW_OK;
+}
+
+int tw_slab_halo(tw_solver *s, int side, int recv, int f, void **ptr, long *rows, long *row_bytes, long *pitch_bytes)
+{
+    if (check(s) || !ptr || !rows || !row_bytes || !pitch_bytes) return TW_ERR_INVALID;
+    const int rc = slab_rows(s, side, recv, f, ptr, rows);
+    if (rc != TW_OK) return rc;
+    *row_bytes = (long)s->cols[f % 5] * s->esz;
+    *pitch_bytes = s->pitch * s->esz;
+    return TW_OK;
+}
+
+int tw_slab_exchange(tw_solver *up, tw_solver *lo)
+{
+    if (check(up) || check(lo) || !up->slab || !lo->slab) return TW_ERR_INVALID;
+    if (up->Mx_glob != lo->Mx_glob || up->own1 != lo->own0 || up->d.My != lo->d.My || up->esz != lo->esz ||
+        up->d.cpst != lo->d.cpst || up->steps_done != lo->steps_done)
+        return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(lo->d.device));
+    TW_CUDA(cudaStreamSynchronize(lo->st));
+    TW_CUDA(cudaSetDevice(up->d.device));
+    TW_CUDA(cudaStreamSynchronize(up->st));
+    const int nf = up->d.cpst != TW_CPST_00 ? 10 : 5;
+    for (int f = 0; f < nf; f++) {
+        void *src, *dst;
+        long rows, rb, pb;
+        // the upper slab's last owned rows -> the lower's top halo; the lower's first owned rows ->
+        // the upper's bottom halo
+        int rc = tw_slab_halo(up, 1, 0, f, &src, &rows, &rb, &pb);
+        if (rc == TW_OK) rc = tw_slab_halo(lo, 0, 1, f, &dst, &rows, &rb, &pb);
+        if (rc != TW_OK) return rc;
+        TW_CUDA(cudaMemcpy2DAsync(dst, pb, src, pb, rb, rows, cudaMemcpyDefault, up->st));
+        rc = tw_slab_halo(lo, 0, 0, f, &src, &rows, &rb, &pb);
+        if (rc == TW_OK) rc = tw_slab_halo(up, 1, 1, f, &dst, &rows, &rb, &pb);
+        if (rc != TW_OK) return rc;
+        TW_CUDA(cudaMemcpy2DAsync(dst, pb, src, pb, rb, rows, cudaMemcpyDefault, up->st));
+    }
+    TW_CUDA(cudaStreamSynchronize(up->st));
+    return TW_OK;
+}
+
 int tw_data_misfit(tw_solver *s, const double *obs, double *total, double *per_rcv)
 {
     if (check(s) || !obs) return TW_ERR_INVALID;
@@ -1147,6 +1285,10 @@ int tw_get_info(tw_solver *s, tw_info *info)
     const double csz = s->d.precision == TW_FP64 ? 8 : (s->d.coef_fp16 ? 2 : 4);
     info->bytes_per_update = nf * (2.0 * s->esz + (s->d.cpst != TW_CPST_00 ? 2.0 * s->esz : 0.0)) + nf * csz;
     info->device_bytes = s->dev_bytes;
+    info->row_off = s->row_off;
+    info->own_rows[0] = s->own0;
+    info->own_rows[1] = s->own1;
+    info->Mx_glob = s->Mx_glob;
     return TW_OK;
 }
 
