@@ -221,6 +221,14 @@ TW_API int tw_slab_exchange(tw_solver *upper, tw_solver *lower);
 TW_API int tw_slab_halo(tw_solver *s, int side, int recv, int f, void **ptr, long *rows, long *row_bytes,
                         long *pitch_bytes);
 
+/* The halo traffic of one edge as one contiguous device buffer, for a transport that moves
+ * flat buffers (NCCL send/recv between ranks): tw_slab_pack copies the owned rows the neighbour
+ * on `side` needs (every field, then every compensation array) into dst; tw_slab_unpack copies a
+ * buffer packed by that neighbour into this slab's halo rows on `side`. *bytes (pack) is the
+ * buffer size; call with dst NULL to learn it. Both run on the handle's stream. */
+TW_API int tw_slab_pack(tw_solver *s, int side, void *dst, long *bytes);
+TW_API int tw_slab_unpack(tw_solver *s, int side, const void *src);
+
 /* ---- adjoint gradient ---------------------------------------------------------------------
  * No counterpart in the reference (it has no adjoint). Full-waveform gradient of the misfit
  * J = 1/2 sum_{r,f,it} (trace[r][f][it] - obs[r][f][it])^2 by the discrete adjoint of the elastic

@@ -12,7 +12,27 @@ pytestmark = pytest.mark.gpu
 SLOTS = None
 
 
-def run(tw, case, prec, cuts, f0, r0, Nt, slab=True):
+def packed_exchange(up, lo):
+    """The same halo swap through flat device buffers (tw_slab_pack / tw_slab_unpack), as a
+    multi-GPU driver moves them with NCCL."""
+    import torch
+    n = up.halo_bytes(1)
+    assert n == lo.halo_bytes(0)
+    a = torch.empty(n, dtype=torch.uint8, device="cuda:0")
+    b = torch.empty(n, dtype=torch.uint8, device="cuda:0")
+    up.sync()
+    lo.sync()
+    up.pack(1, a.data_ptr())
+    lo.pack(0, b.data_ptr())
+    up.sync()
+    lo.sync()
+    lo.unpack(0, a.data_ptr())
+    up.unpack(1, b.data_ptr())
+    up.sync()
+    lo.sync()
+
+
+def run(tw, case, prec, cuts, f0, r0, Nt, slab=True, packed=False):
     shp = (case.Mx + 2, case.My + 2)
     kw = dict(precision=prec, cpst=case.cpst, central_f=case.central_f, time_delay=case.time_delay, max_steps=Nt)
     slots = [(tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)]
@@ -35,7 +55,10 @@ def run(tw, case, prec, cuts, f0, r0, Nt, slab=True):
         for h in hs:
             h.step(1)
         for up, lo in zip(hs[:-1], hs[1:]):
-            up.exchange(lo)
+            if packed:
+                packed_exchange(up, lo)
+            else:
+                up.exchange(lo)
     for h in hs:
         h.sync()
     fields = [np.zeros_like(a) for a in f0]
@@ -53,9 +76,10 @@ def run(tw, case, prec, cuts, f0, r0, Nt, slab=True):
     return fields, traces, energy
 
 
+@pytest.mark.parametrize("packed", [False, True])
 @pytest.mark.parametrize("prec,cpst", [("f32", "00"), ("f64", "6R"), ("f32", "3C")])
 @pytest.mark.parametrize("cuts", [(0, 24, 48, 72), (0, 40, 72), (0, 16, 56, 72)])
-def test_slabs_equal_the_whole_grid(prec, cpst, cuts):
+def test_slabs_equal_the_whole_grid(prec, cpst, cuts, packed):
     tw = load_twave()
     Mx, My, den, Nt = 72, 60, 72, 9
     rcvs = [("N", "M", 2, den, 7, 2 * den), ("M", "M", 2 * 23 + 1, 2 * den, 2 * 9 + 1, 2 * den),
@@ -69,7 +93,7 @@ def test_slabs_equal_the_whole_grid(prec, cpst, cuts):
     f0 = [(rng.standard_normal(s) * 1e-2).astype(T).astype(np.float64) for s in shapes]
     r0 = None if cpst == "00" else [(rng.standard_normal(s) * 1e-9).astype(T).astype(np.float64) for s in shapes]
     want = run(tw, case, prec, None, f0, r0, Nt, slab=False)
-    got = run(tw, case, prec, cuts, f0, r0, Nt)
+    got = run(tw, case, prec, cuts, f0, r0, Nt, packed=packed)
     for k in range(5):
         assert np.array_equal(got[0][k], want[0][k]), k
     assert np.array_equal(got[1], want[1])

@@ -112,6 +112,8 @@ def lib() -> C.CDLL:
         L.tw_data_misfit.argtypes = [vp, dp, dp, dp]
         L.tw_create_slab.argtypes = [C.POINTER(vp), C.POINTER(GridDesc), C.c_long, C.c_long]
         L.tw_slab_exchange.argtypes = [vp, vp]
+        L.tw_slab_pack.argtypes = [vp, C.c_int, vp, lp]
+        L.tw_slab_unpack.argtypes = [vp, C.c_int, vp]
         L.tw_slab_halo.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(vp), lp, lp, lp]
         L.tw_batch_create.argtypes = [C.POINTER(vp), C.POINTER(vp), C.c_int]
         L.tw_batch_destroy.argtypes = [vp]
@@ -211,6 +213,20 @@ class Solver:
         self.Mx_glob = Mx
         self.row_off, self.own = int(inf.row_off), (int(inf.own_rows[0]), int(inf.own_rows[1]))
         return self
+
+    def halo_bytes(self, side: int) -> int:
+        n = C.c_long()
+        _ok(lib().tw_slab_pack(self.h, side, None, C.byref(n)), "tw_slab_pack")
+        return n.value
+
+    def pack(self, side: int, dst_ptr: int):
+        """The owned rows the neighbour on `side` (0 top, 1 bottom) needs, into device memory."""
+        n = C.c_long()
+        _ok(lib().tw_slab_pack(self.h, side, C.c_void_p(dst_ptr), C.byref(n)), "tw_slab_pack")
+
+    def unpack(self, side: int, src_ptr: int):
+        """A buffer packed by the neighbour on `side` into this slab's halo rows there."""
+        _ok(lib().tw_slab_unpack(self.h, side, C.c_void_p(src_ptr)), "tw_slab_unpack")
 
     def exchange(self, lower: "Solver"):
         """Refresh the halo rows shared with the slab just below (tw_slab_exchange)."""

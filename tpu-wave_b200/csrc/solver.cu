@@ -1159,6 +1159,39 @@ int tw_slab_halo(tw_solver *s, int side, int recv, int f, void **ptr, long *rows
     return TW_OK;
 }
 
+int tw_slab_pack(tw_solver *s, int side, void *dst, long *bytes)
+{
+    if (check(s) || !bytes || !s->slab) return TW_ERR_INVALID;
+    const int nf = s->d.cpst != TW_CPST_00 ? 10 : 5;
+    long total = 0;
+    for (int f = 0; f < nf; f++) {
+        void *src;
+        long rows, rb, pb;
+        const int rc = tw_slab_halo(s, side, 0, f, &src, &rows, &rb, &pb);
+        if (rc != TW_OK) return rc;
+        if (dst) TW_CUDA(cudaMemcpy2DAsync((char *)dst + total, rb, src, pb, rb, rows, cudaMemcpyDefault, s->st));
+        total += rb * rows;
+    }
+    *bytes = total;
+    return TW_OK;
+}
+
+int tw_slab_unpack(tw_solver *s, int side, const void *src)
+{
+    if (check(s) || !src || !s->slab) return TW_ERR_INVALID;
+    const int nf = s->d.cpst != TW_CPST_00 ? 10 : 5;
+    long off = 0;
+    for (int f = 0; f < nf; f++) {
+        void *dst;
+        long rows, rb, pb;
+        const int rc = tw_slab_halo(s, side, 1, f, &dst, &rows, &rb, &pb);
+        if (rc != TW_OK) return rc;
+        TW_CUDA(cudaMemcpy2DAsync(dst, pb, (const char *)src + off, rb, rb, rows, cudaMemcpyDefault, s->st));
+        off += rb * rows;
+    }
+    return TW_OK;
+}
+
 int tw_slab_exchange(tw_solver *up, tw_solver *lo)
 {
     if (check(up) || check(lo) || !up->slab || !lo->slab) return TW_ERR_INVALID;
