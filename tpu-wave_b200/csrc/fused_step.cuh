@@ -5,16 +5,20 @@
 // the state from one buffer and writing it to the other (neighbouring CTAs read old values that
 // this CTA overwrites). Two kinds of CTA share the launch:
 //
-// * interior CTAs (rows [FS_ZONE, Mx - FS_ZONE)): eight independent warps, each streaming down
-//   a strip of FS_WARP_CORE columns with two columns per lane. The x stencil windows live in
-//   registers, the y taps come from the neighbouring lanes by warp shuffles, two lanes on each
-//   side are halo (their velocities feed the stress y taps of the core lanes). A warp computes
-//   velocity row j and then stress row j - 2, so no shared memory and no block barrier is used.
-//   These rows never touch an SBP closure or an SAT penalty.
+// * interior CTAs (rows [FS_ZONE, Mx - FS_ZONE)): FS_WARPS independent warps, each streaming
+//   down a strip of FS_WARP_CORE columns over one row segment, two columns per lane. The x
+//   stencil windows live in registers, the y taps come from the neighbouring lanes by warp
+//   shuffles, two lanes on each side are halo (their velocities feed the stress y taps of the
+//   core lanes). A warp computes velocity row j and then stress row j - 2; each lane stages its
+//   own rows a few ahead through a private cp.async ring in shared memory, so no block barrier
+//   is used. Of the halo rows around a segment only the velocity rows that feed a stress row of
+//   the segment are computed. These rows never touch an SBP closure or an SAT penalty.
 // * boundary CTAs (the FS_ZONE rows at each free surface, or the whole grid when it is small):
 //   a strip of FS_BND_TY columns, its threads split into row groups; phase 1 computes the
 //   velocities of the zone (and two rows beyond) from global memory with the closure and SAT
-//   operators into a shared tile, phase 2 the stresses from that tile.
+//   operators into a shared tile, phase 2 the stresses from that tile. They take the lowest
+//   block indices: their strips are the longest work items, and started first they end before
+//   the last wave of interior CTAs instead of after it.
 //
 // Per point the arithmetic and the order of the right-hand-side terms are those of
 // step_kernels.cu (hence of the reference): results are bit-identical.
@@ -397,7 +401,7 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
     };
 
     // windows: NN rows j-2..j+2, MM0 rows j-2..j+1, MM1 rows j-2..j, MN rows j-4..j, NM rows j-3..j
-    P2<C> NNw[5], M0w[4], M1w[3], MNw[5], NMw[4];
+    P2<C> NNw[5], M0w[4], M1w[3], MNw[5]{}, NMw[4]{};   // (the skipped halo rows stay zero)
     const int jb = x0 - 2, je = x1 + 1;
 #pragma unroll
     for (int q = 0; q < 4; q++) NNw[q] = ld2f(F_NN, jb - 2 + q, pN0, pN1);
@@ -424,7 +428,7 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
         M1w[2] = cur.mm1;
         const bool ownV = j >= x0 && j < x1;
         // ---- velocities of row j
-        {   // MN: x from NN rows j-1..j+2, y from MM syy row j
+        if (j <= x1) {   // MN: x from NN rows j-1..j+2, y from MM syy row j (row x1 + 1 feeds no stress)
             P2<C> p, n;
             lanes(M1w[2], p, n);
             const P2<C> vy = dyNfromM(a.op, M1w[2], p, n);
@@ -453,7 +457,7 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
                 }
             }
         }
-        {   // NM: x from MM sxx rows j-2..j+1, y from NN row j
+        if (j >= x0 - 1) {   // NM: x from MM sxx rows j-2..j+1, y from NN row j (row x0 - 2 feeds no stress)
             P2<C> p, n;
             lanes(NNw[2], p, n);
             P2<C> vy = dyMfromN(a.op, NNw[2], p, n);
@@ -782,9 +786,9 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 4 : TW_FS_MIN_BLOCKS)
     const int cta = blockIdx.x;
     const int rcv_b = a.rcv_off[cta], rcv_e = a.rcv_off[cta + 1];
     EAcc E;
-    const int n_int = a.n_int_cta;
-    if (cta < n_int) {   // interior CTA: FS_WARPS consecutive (segment, strip) warps, segment-major
-        const int gw = cta * FS_WARPS + (threadIdx.x >> 5);
+    const int n_bnd = a.n_zone * a.n_bstrip;
+    if (cta >= n_bnd) {   // interior CTA: FS_WARPS consecutive (segment, strip) warps, segment-major
+        const int gw = (cta - n_bnd) * FS_WARPS + (threadIdx.x >> 5);
         if (gw < a.n_int_seg * a.n_wstrip) {
             const int seg = gw / a.n_wstrip, wstrip = gw - seg * a.n_wstrip;
             const int y0 = wstrip * FS_WARP_CORE;
@@ -793,7 +797,7 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 4 : TW_FS_MIN_BLOCKS)
             else interior_warp<S, C, CPST, ENERGY, true, K>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
         }
     } else {             // boundary CTA (zone, strip)
-        const int b = cta - n_int;
+        const int b = cta;
         boundary_cta<S, C, CPST, ENERGY, K>(a, b % a.n_bstrip, b / a.n_bstrip, it, rcv_b, rcv_e,
                                          reinterpret_cast<C *>(smem_raw), E);
     }

@@ -68,7 +68,10 @@ void launch_energy(const EnergyArgs<S, C> &e, cudaStream_t st);
 #define TW_FS_MIN_BLOCKS 5            // CTAs per SM the register allocation is sized for
 #endif
 #ifndef TW_FS_CTAS_PER_SM
-#define TW_FS_CTAS_PER_SM 15          // CTAs per SM the row segmentation aims at (three waves)
+#define TW_FS_CTAS_PER_SM 15          // CTAs per SM the elastic row segmentation aims at
+#endif
+#ifndef TW_AC_CTAS_PER_SM
+#define TW_AC_CTAS_PER_SM 15          // the same for the fused acoustic step and batches
 #endif
 #ifndef TW_FS_RING
 #define TW_FS_RING 3                  // rows staged ahead per interior warp (FP64: 2)
@@ -108,8 +111,8 @@ struct FusedArgs {
     int max_steps;
     const double *w[5];       // energy weights (ENERGY only)
     double *energy;           // [3][max_steps]: E_p0, E_k, E_p1
-    const int *rcv_off;       // receivers owned by each CTA (CSR over blockIdx.x: interior CTAs
-                              // segment-major, then boundary CTAs zone-major)
+    const int *rcv_off;       // receivers owned by each CTA (CSR over blockIdx.x: boundary CTAs
+                              // zone-major, then interior CTAs segment-major)
     const int *rcv;           // [n][4]: field slot, row, column, trace row (2 * receiver + field)
     double *traces;
 };

@@ -486,11 +486,11 @@ int upload_receivers(tw_solver *s)
             }
             int cta;
             if (zone >= 0) {
-                cta = n_int + zone * s->n_bstrip + col / FS_BND_TY;
+                cta = zone * s->n_bstrip + col / FS_BND_TY;
             } else {
                 int seg = 0;   // the balanced segment holding the row (fused_step.cuh)
                 while (s->ir0 + (int)((long)(seg + 1) * s->int_rows / s->n_int_seg) <= row) seg++;
-                cta = (seg * s->n_wstrip + col / FS_WARP_CORE) / FS_WARPS;
+                cta = s->n_zone * s->n_bstrip + (seg * s->n_wstrip + col / FS_WARP_CORE) / FS_WARPS;
             }
             for (int f = 0; f < 2; f++)
                 if (q[f] >= 0) per[cta].insert(per[cta].end(), {q[f], row, col, 2 * r + f});
@@ -786,7 +786,7 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
         // periodic acoustic with energy off: a second copy of the state, for the fused step of a
         // batch and, on grids of 2^20 points or more, of the handle alone (below that the
         // two-launch kernels are faster: a warp's short row segment is latency-bound); segments
-        // of 8 rows or more, TW_FS_CTAS_PER_SM CTAs of work per SM of a 148-SM B200
+        // of 8 rows or more, TW_AC_CTAS_PER_SM CTAs of work per SM of a 148-SM B200
         s->pfuse = true;
         s->afused = Mx * My >= (1L << 20);
         for (int k = 0; k < 5; k++) {
@@ -800,7 +800,7 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             }
         }
         s->n_wstrip = (int)((My + 1 + FS_WARP_CORE - 1) / FS_WARP_CORE);
-        const int target = std::max(1, 148 * TW_FS_CTAS_PER_SM * FS_WARPS / s->n_wstrip);
+        const int target = std::max(1, 148 * TW_AC_CTAS_PER_SM * FS_WARPS / s->n_wstrip);
         s->n_int_seg = std::max(1, std::min(target, (int)Mx / 8));
         if ((rc_ = s->alloc((void **)&s->d_done, sizeof(int))) != TW_OK) return fail(rc_);
         cudaMemsetAsync(s->d_done, 0, sizeof(int), s->st);
@@ -1611,7 +1611,7 @@ struct tw_batch {
     bool fused = false;
     void *d_ac = nullptr;
     int *d_done = nullptr;
-    int n_warps = 0, per_sm = TW_FS_CTAS_PER_SM;
+    int n_warps = 0, per_sm = TW_AC_CTAS_PER_SM;
     cudaStream_t st = nullptr;
     cudaEvent_t done = nullptr;
     void *d_shots = nullptr, *d_gather = nullptr;
@@ -1803,7 +1803,7 @@ int tw_batch_create(tw_batch **out, tw_solver *const *shots, int n)
     if (e != cudaSuccess) return fail(cuda_fail(e, "tw_batch_create"));
     b->fused = true;
     for (tw_solver *s : b->shots) b->fused = b->fused && s->pfuse;
-    const int rc = b->fused ? batch_fused_layout(b, TW_FS_CTAS_PER_SM) : batch_layout(b, BatchShape{32, 8, 1, 0});
+    const int rc = b->fused ? batch_fused_layout(b, TW_AC_CTAS_PER_SM) : batch_layout(b, BatchShape{32, 8, 1, 0});
     if (rc != TW_OK) return fail(rc);
     *out = b;
     return TW_OK;
