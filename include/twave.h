@@ -49,9 +49,12 @@ enum {
 
 /* ---- enums ------------------------------------------------------------------------------ */
 enum tw_physics { TW_ELASTIC = 0, TW_ACOUSTIC = 1 };
-/* x boundaries: SBP-SAT free surface (cuda/ tree) or periodic (singlecore/ and mpi/ trees);
- * y is always periodic, as in the reference (grid_drvt.tpp:1-3). */
-enum tw_bc { TW_BC_SAT_FREE = 0, TW_BC_PERIODIC = 1 };
+/* x boundaries: SBP-SAT free surface (cuda/ tree), periodic (singlecore/ and mpi/ trees), or the
+ * two x ends joined by the SBP-SAT interface penalty: the branch of secure_bdry for a boundary
+ * type other than 'F' (grid_drvt.tpp:575-693, eta = +-1/2, every grid penalised toward the other
+ * end's projection), which the reference's inputs never select (namespace_input.hpp:155-160).
+ * y is periodic, as in the reference (grid_drvt.tpp:1-3), unless tw_grid_desc.sat_y is set. */
+enum tw_bc { TW_BC_SAT_FREE = 0, TW_BC_PERIODIC = 1, TW_BC_SAT_INTERFACE = 2 };
 /* storage type of the fields; FP64/FP32 compute in the storage type (namespace_type.cuh:16-22);
  * BF16/FP16 (elastic) store 16-bit fields, compute in FP32 and keep FP32 coefficients. The
  * reference's 16-bit mode (PRCSFLAG 16) also computes in 16 bits; this one rounds only what it
@@ -85,6 +88,11 @@ typedef struct {
     int coef_fp16;          /* 1: store the stepping coefficients in FP16 (elastic, FP32 arithmetic; no
                                reference counterpart): 10 B less per update; the medium is quantised to
                                FP16, and coefficients outside its normal range are TW_ERR_UNSUPPORTED */
+    int sat_y;              /* 1: SBP-SAT free surfaces on the two y ends too (all four sides free with
+                               bc_x TW_BC_SAT_FREE): closures and penalties along y with the x tables,
+                               energy norm along y as along x; no reference run (its y is periodic).
+                               0: periodic y (the reference). sat_y and TW_BC_SAT_INTERFACE step with
+                               the two-launch FP64/FP32 kernels; My >= 8 with sat_y */
 } tw_grid_desc;
 
 typedef struct {

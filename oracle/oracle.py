@@ -31,7 +31,8 @@ class _ElasticCfg(C.Structure):
     _fields_ = [("Mx", C.c_int), ("My", C.c_int), ("dx", C.c_double), ("dt", C.c_double),
                 ("central_f", C.c_double), ("time_delay", C.c_double), ("cpst", C.c_int), ("Nt", C.c_int),
                 ("src_grid", C.c_int), ("src_ix", C.c_long), ("src_iy", C.c_long), ("n_rcv", C.c_int),
-                ("rcv_grid", C.POINTER(C.c_int)), ("rcv_ix", C.POINTER(C.c_long)), ("rcv_iy", C.POINTER(C.c_long))]
+                ("rcv_grid", C.POINTER(C.c_int)), ("rcv_ix", C.POINTER(C.c_long)), ("rcv_iy", C.POINTER(C.c_long)),
+                ("bc_x", C.c_int), ("sat_y", C.c_int)]
 
 
 class _AcousticCfg(C.Structure):
@@ -87,6 +88,9 @@ def material(case: refrun.ElasticCase):
     return out
 
 
+BC_X = {"F": 0, "I": 2}
+
+
 def elastic_coefficients(case: refrun.ElasticCase, precision: str):
     """Stored coefficients (T) and energy weights (FP64), as the reference prepares them."""
     T = np.float64 if precision == "f64" else np.float32
@@ -96,9 +100,9 @@ def elastic_coefficients(case: refrun.ElasticCase, precision: str):
               "MN_irho": (1.0 / rho_mn).astype(T), "NM_irho": (1.0 / rho_nm).astype(T)}
     Mx, My = case.Mx, case.My
     w = [np.zeros((Mx + 1, My + 1)), np.zeros((Mx, My + 1)), np.zeros((Mx + 1, My)), np.zeros((Mx, My)), np.zeros((Mx, My))]
-    fn = lib().two_energy_weights_f64 if precision == "f64" else lib().two_energy_weights_f32
+    fn = lib().two_energy_weights_ext_f64 if precision == "f64" else lib().two_energy_weights_ext_f32
     dx = case.num_dx / case.den_dx
-    fn(C.c_int(Mx), C.c_int(My), C.c_double(dx), _p(stored["NN_mu"]), _p(stored["MN_rho"]), _p(stored["NM_rho"]),
+    fn(C.c_int(Mx), C.c_int(My), C.c_double(dx), C.c_int(int(case.sat_y)), _p(stored["NN_mu"]), _p(stored["MN_rho"]), _p(stored["NM_rho"]),
        _p(stored["MM_lambda"]), _p(stored["MM_2mu"]), *[_p(a) for a in w])
     weights = dict(zip(("NN", "MN", "NM", "MM_P1", "MM_P2"), w))
     return stored, weights
@@ -136,7 +140,8 @@ def elastic_run(case: refrun.ElasticCase, precision: str = "f64", fields0=None, 
     ry = np.array([location_to_index(r[1], r[4], r[5], nd, dd) for r in case.rcvs] or [0], np.int64)
     cfg = _ElasticCfg(Mx, My, nd / dd, case.dt, case.central_f, case.time_delay, CPST_INDEX[case.cpst], Nt,
                       src_grid, sx, sy, n, rg.ctypes.data_as(C.POINTER(C.c_int)),
-                      rx.ctypes.data_as(C.POINTER(C.c_long)), ry.ctypes.data_as(C.POINTER(C.c_long)))
+                      rx.ctypes.data_as(C.POINTER(C.c_long)), ry.ctypes.data_as(C.POINTER(C.c_long)),
+                      BC_X[case.bc_x], int(case.sat_y))
     traces = np.zeros((n, 2, Nt))
     E_k, E_p0, E_p1 = np.zeros(Nt), np.zeros(Nt), np.zeros(Nt)
     FA = C.c_void_p * 5

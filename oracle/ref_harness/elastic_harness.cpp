@@ -22,7 +22,9 @@
 //                              int64 rcv[n_rcv][6]  (type_x, type_y, num_x, den_x, num_y, den_y)
 //   ih: 0 magic 0x5457454C, 1 Mx, 2 My, 3 Mx_prmt, 4 My_prmt, 5 num_dx, 6 den_dx, 7 num_dxM,
 //       8 den_dxM, 9 Nt, 10 cpst_N, 11 cpst_S (char code), 12 src_type_x, 13 src_type_y,
-//       14..17 src num_x, den_x, num_y, den_y, 18 n_rcv, 19 quiet
+//       14..17 src num_x, den_x, num_y, den_y, 18 n_rcv, 19 quiet,
+//       20 boundary type of both x ends (0 = 'F'; another letter selects the reference's
+//          SAT interface branch of secure_bdry, grid_drvt.tpp:575-693)
 //   dh: 0 dt, 1 central_f, 2 time_delay
 //   P = (Mx_prmt + 2) * (My_prmt + 2)  (the reference's padded model layout, inverse.cpp:79-90)
 // Output file: float64 loop_seconds; E_k[Nt]; E_p0[Nt]; E_p1[Nt]; traces[n_rcv][2][Nt];
@@ -103,6 +105,12 @@ int main(int argc, char **argv)
     bool_energy = true;
     bool_visual = false;
     ns_input_derived_variables();
+    // ns_input_derived_variables asserts four 'F' sides (namespace_input.hpp:155-160); the x
+    // boundary type is only read by secure_bdry, so the interface branch is selected after it
+    if (ih[20] != 0 && ih[20] != 'F') {
+        Map_bdry_type[{'x', 'L'}] = (char)ih[20];
+        Map_bdry_type[{'x', 'R'}] = (char)ih[20];
+    }
 
     dx = static_cast<double>(num_dx_soln) / static_cast<double>(den_dx_soln);
     dt = dh[0];

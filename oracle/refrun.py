@@ -62,6 +62,8 @@ class ElasticCase:
     My_prmt: int | None = None
     num_dxM: int | None = None
     den_dxM: int | None = None
+    bc_x: str = "F"      # "F" free surfaces; "I" x ends joined by the SAT interface penalty
+    sat_y: bool = False  # free surfaces on the y ends too (restatement only: no reference run)
 
 
 @dataclass
@@ -88,8 +90,11 @@ def run_elastic(case: ElasticCase, precision: str = "f64", perf: bool = False) -
     P = (Mxp + 2) * (Myp + 2)
     for a in (case.rho, case.vp, case.vs):
         assert a.size == P, (a.shape, P)
+    if case.sat_y:
+        raise ValueError("the reference has no run with free surfaces on the y ends")
     cn, cs = CPST_CODES[case.cpst]
     ih = np.zeros(32, np.int64)
+    ih[20] = 0 if case.bc_x == "F" else ord(case.bc_x)
     ih[:20] = [0x5457454C, case.Mx, case.My, Mxp, Myp, case.num_dx, case.den_dx, ndM, ddM,
                case.Nt, cn, ord(cs), ord(case.src[0]), ord(case.src[1]), *case.src[2:6],
                len(case.rcvs), 1]

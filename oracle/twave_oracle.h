@@ -30,6 +30,9 @@ typedef struct {
     int n_rcv;
     const int *rcv_grid;
     const long *rcv_ix, *rcv_iy;
+    int bc_x;                   /* x ends: 0 free surface ('F'), 2 joined by the SAT interface
+                                   penalty (a boundary type other than 'F', grid_drvt.tpp:575-693) */
+    int sat_y;                  /* 1: free surfaces on the y ends too (no reference run; My >= 8) */
 } two_elastic_cfg;
 
 /* grid_parameter.cpp:7-160: bilinear interpolation of the padded node model onto the four
@@ -49,6 +52,14 @@ void two_energy_weights_f64(int Mx, int My, double dx, const double *NN_mu, cons
 void two_energy_weights_f32(int Mx, int My, double dx, const float *NN_mu, const float *MN_rho,
                             const float *NM_rho, const float *MM_lambda, const float *MM_2mu,
                             double *w_NN, double *w_MN, double *w_NM, double *w_MM1, double *w_MM2);
+/* The same with sat_y = 1: the y factor of the norm is then A_diag * dx (storage-rounded) on the
+ * end columns by the grid's y type and dx inside, as along x, instead of the periodic rule. */
+void two_energy_weights_ext_f64(int Mx, int My, double dx, int sat_y, const double *NN_mu, const double *MN_rho,
+                                const double *NM_rho, const double *MM_lambda, const double *MM_2mu,
+                                double *w_NN, double *w_MN, double *w_NM, double *w_MM1, double *w_MM2);
+void two_energy_weights_ext_f32(int Mx, int My, double dx, int sat_y, const float *NN_mu, const float *MN_rho,
+                                const float *NM_rho, const float *MM_lambda, const float *MM_2mu,
+                                double *w_NN, double *w_MN, double *w_NM, double *w_MM1, double *w_MM2);
 
 /* forward_simulation.cpp:21-182 (+ grid_drvt.tpp, grid_update.tpp, grid_energy.cpp:180-216).
  * fields[5] = NN, MN, NM, MM0, MM1 (in: initial state, out: state after Nt steps);

@@ -97,7 +97,8 @@ def product_elastic(case, precision, acoustic=False, fields0=None, resid0=None, 
     s = tw.Solver(case.Mx, case.My, case.num_dx, case.den_dx, case.dt,
                   physics=tw.ACOUSTIC if acoustic else tw.ELASTIC, precision=precision, cpst=case.cpst,
                   central_f=case.central_f, time_delay=case.time_delay, max_steps=max(case.Nt, 1), energy=energy,
-                  coef_fp16=coef_fp16)
+                  coef_fp16=coef_fp16, bc_x=tw.SAT_INTERFACE if case.bc_x == "I" else tw.SAT_FREE,
+                  sat_y=case.sat_y)
     try:
         Mx, My = case.Mx, case.My
         shp = (Mx + 2, My + 2)

@@ -17,11 +17,11 @@ pytestmark = pytest.mark.gpu
 CP = {"0": "00", "3": "3R", "6": "6R"}
 
 
-def make_shot(tw, case, precision, energy=False, bc_x=None):
+def make_shot(tw, case, precision, energy=False, bc_x=None, sat_y=False):
     s = tw.Solver(case.Nx, case.Ny, 1, max(case.Nx, case.Ny), case.dt, physics=tw.ACOUSTIC,
                   bc_x=tw.PERIODIC if bc_x is None else bc_x, precision=precision, cpst=CP[case.cpst],
                   central_f=case.central_f, time_delay=case.time_delay, max_steps=max(case.Nt, 1) + 64,
-                  energy=energy)
+                  energy=energy, sat_y=sat_y)
     s.set_material_grid(tw.NM, 0, case.rho_vx)
     s.set_material_grid(tw.MN, 0, case.rho_vy)
     s.set_material_grid(tw.MM, 0, np.asarray(case.coef_p).reshape(case.Nx, case.Ny))
@@ -83,6 +83,28 @@ def test_every_launch_shape_gives_the_same_result(shape):
     b.step(16)     # one graph replay
     b.step(4)      # eager remainder
     b.sync()
+    for s, r in zip(shots, ref):
+        f, t = state(tw, s)
+        for a, w in zip(f, r[0]):
+            assert np.array_equal(a, w)
+        assert np.array_equal(t, r[1])
+    for h in [b] + shots + ref_shots:
+        h.close()
+
+
+def test_batch_of_boundary_variants_equals_each_shot_alone():
+    """Shots with the x ends joined by the SAT interface and with free y ends batch with the
+    free-surface shots: each carries its variant in its own arguments."""
+    tw = load_twave()
+    modes = [(tw.SAT_INTERFACE, False), (tw.SAT_FREE, True), (tw.SAT_INTERFACE, True), (tw.SAT_FREE, False)]
+    cases = [acoustic_periodic_case(nx, ny, seed=27 + k, cpst="3", Nt=60) for k, (nx, ny) in enumerate(SIZES[:4])]
+    ref_shots = [make_shot(tw, c, "f64", bc_x=m[0], sat_y=m[1]) for c, m in zip(cases, modes)]
+    for s in ref_shots:
+        s.run(60)
+    ref = [state(tw, s) for s in ref_shots]
+    shots = [make_shot(tw, c, "f64", bc_x=m[0], sat_y=m[1]) for c, m in zip(cases, modes)]
+    b = tw.Batch(shots)
+    b.run(60)
     for s, r in zip(shots, ref):
         f, t = state(tw, s)
         for a, w in zip(f, r[0]):

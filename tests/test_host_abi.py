@@ -74,6 +74,11 @@ def _desc(tw, **kw):
     (dict(coef_fp16=1, precision=0), -10),          # FP16 coefficients need FP32 arithmetic
     (dict(coef_fp16=1, cpst=6), -10),               # ... and the plain update
     (dict(coef_fp16=1, physics=1, bc_x=1), -10),    # ... and the elastic stepper
+    (dict(bc_x=3), -1), (dict(sat_y=2), -1),
+    (dict(sat_y=1, My=7), -1),                      # free y ends need 8 columns
+    (dict(sat_y=1, physics=1, bc_x=1), -10),        # free y ends with periodic x
+    (dict(bc_x=2, precision=2), -10),               # the variants: FP64 / FP32 storage
+    (dict(sat_y=1, coef_fp16=1), -10),
 ])
 def test_create_rejects_bad_descriptors_before_touching_the_device(tw, kw, code):
     h = C.c_void_p()

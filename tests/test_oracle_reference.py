@@ -21,7 +21,7 @@ def golden_elastic_case(d):
                               dt=float(d["dt"]), rho=d["rho"], vp=d["vp"], vs=d["vs"],
                               src=tuple(json.loads(str(d["src"]))), rcvs=[tuple(r) for r in json.loads(str(d["rcvs"]))],
                               Nt=int(d["Nt"]), cpst=str(d["cpst"]), central_f=float(d["central_f"]),
-                              time_delay=float(d["time_delay"]))
+                              time_delay=float(d["time_delay"]), bc_x=str(d["bc_x"]) if "bc_x" in d else "F")
 
 
 def golden_acoustic_case(d):
@@ -65,10 +65,11 @@ def test_oracle_matches_golden_acoustic(name, prec):
 
 def test_vs0_gives_identical_normal_stresses():
     """The acoustic limit of the elastic reference: sxx == syy bit for bit when vs = 0."""
-    d = np.load(os.path.join(GOLDEN, "el_20x16_vs0.npz"))
-    for prec in ("f64", "f32"):
-        assert np.array_equal(d[f"{prec}_field_MM0"], d[f"{prec}_field_MM1"])
-        assert not np.any(d[f"{prec}_field_NN"])
+    for name in ("el_20x16_vs0", "el_20x16_if_vs0"):
+        d = np.load(os.path.join(GOLDEN, name + ".npz"))
+        for prec in ("f64", "f32"):
+            assert np.array_equal(d[f"{prec}_field_MM0"], d[f"{prec}_field_MM1"])
+            assert not np.any(d[f"{prec}_field_NN"])
 
 
 @pytest.mark.skipif(not has_ref_binaries(), reason="reference binaries (oracle/_ref) not built")

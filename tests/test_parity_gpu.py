@@ -37,10 +37,12 @@ def test_elastic_matches_reference_golden(name, prec):
         assert energy_close(got[k], d[f"{prec}_{k}"]), k
 
 
+@pytest.mark.parametrize("name", ["el_20x16_vs0", "el_20x16_if_vs0"])
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-def test_acoustic_free_surface_matches_reference_vs0(prec):
-    """Acoustic with SAT free surface = the reference elastic solver with vs = 0 (p = sxx = syy)."""
-    d = np.load(os.path.join(GOLDEN, "el_20x16_vs0.npz"))
+def test_acoustic_free_surface_matches_reference_vs0(name, prec):
+    """Acoustic with SAT free surfaces (or the x ends joined by the SAT interface) = the reference
+    elastic solver with vs = 0 (p = sxx = syy)."""
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
     case = golden_elastic_case(d)
     keep = [i for i, r in enumerate(case.rcvs) if (r[0], r[1]) != ("N", "N")]
     case.rcvs = [case.rcvs[i] for i in keep]

@@ -21,7 +21,7 @@ LIB_PATH = os.path.join(HERE, "lib", "libtwave.so")
 HEADER = os.path.join(HERE, "..", "include", "twave.h")
 
 ELASTIC, ACOUSTIC = 0, 1
-SAT_FREE, PERIODIC = 0, 1
+SAT_FREE, PERIODIC, SAT_INTERFACE = 0, 1, 2
 FP64, FP32, BF16, FP16 = 0, 1, 2, 3
 CPST = {"00": 0, "-3C": 1, "-3R": 2, "3C": 3, "3R": 4, "6C": 5, "6R": 6, "split": 7}
 NN, MN, NM, MM = 0, 1, 2, 3
@@ -45,7 +45,7 @@ class GridDesc(C.Structure):
                 ("Mx", C.c_long), ("My", C.c_long), ("num_dx", C.c_int), ("den_dx", C.c_int),
                 ("dt", C.c_double), ("central_f", C.c_double), ("time_delay", C.c_double),
                 ("source_scaling", C.c_double), ("max_steps", C.c_int), ("energy", C.c_int), ("device", C.c_int),
-                ("coef_fp16", C.c_int)]
+                ("coef_fp16", C.c_int), ("sat_y", C.c_int)]
 
 
 class Info(C.Structure):
@@ -185,10 +185,10 @@ class Solver:
     def __init__(self, Mx: int, My: int, num_dx: int, den_dx: int, dt: float, *, physics: int = ELASTIC,
                  bc_x: int = SAT_FREE, precision: str = "f32", cpst: str = "00", central_f: float = 5.0,
                  time_delay: float = 0.25, source_scaling: float = 1.0, max_steps: int = 1000,
-                 energy: bool = True, device: int = 0, coef_fp16: bool = False):
+                 energy: bool = True, device: int = 0, coef_fp16: bool = False, sat_y: bool = False):
         self.desc = GridDesc(physics, bc_x, PRECISION[precision], CPST[cpst], Mx, My, num_dx, den_dx, dt,
                              central_f, time_delay, source_scaling, max_steps, 1 if energy else 0, device,
-                             1 if coef_fp16 else 0)
+                             1 if coef_fp16 else 0, 1 if sat_y else 0)
         self.h = C.c_void_p()
         _ok(lib().tw_create(C.byref(self.h), C.byref(self.desc)), "tw_create")
         self.Mx, self.My, self.physics, self.bc_x = Mx, My, physics, bc_x
@@ -202,7 +202,7 @@ class Solver:
         self.desc = GridDesc(ELASTIC, SAT_FREE, PRECISION[kw.pop("precision", "f32")], CPST[kw.pop("cpst", "00")], Mx, My,
                              num_dx, den_dx, dt, kw.pop("central_f", 5.0), kw.pop("time_delay", 0.25),
                              kw.pop("source_scaling", 1.0), kw.pop("max_steps", 1000), 1 if energy else 0,
-                             kw.pop("device", 0), 1 if kw.pop("coef_fp16", False) else 0)
+                             kw.pop("device", 0), 1 if kw.pop("coef_fp16", False) else 0, 0)
         if kw:
             raise TypeError(f"unexpected arguments {sorted(kw)}")
         self.h = C.c_void_p()

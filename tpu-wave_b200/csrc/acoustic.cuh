@@ -39,13 +39,15 @@ __device__ __forceinline__ void acoustic_velocity_point(const StepArgs<S, C> &a,
     const long i = (long)ix * pitch + iy;
     constexpr bool kr = Cpst<CPST>::keep_r, kc = Cpst<CPST>::keep_c;
     const S *p = a.f[F_MM0];
+    const bool xif = !PERIODIC && (a.bnd & BND_X_IF), ysat = !PERIODIC && (a.bnd & BND_Y_SAT);
 
-    if (ix < a.Mx) {   // MN (Mx x My+1): velocity along y, y derivative of p only
+    if (ix < a.Mx) {   // MN (Mx x My+1): velocity along y, y derivative of p only (+ the y free surfaces)
         C r, c;
         load_rc<S, C, CPST>(a.res[F_MN], i, r, c);
         const C P = __ldg(a.coef[F_MN] + i);
-        const C v = dy_periodic<false, C>(a.op, p + (long)ix * pitch, a.My, iy);
+        C v = dy_any<false, C>(a.op, p + (long)ix * pitch, a.My, iy, ysat);
         r = add(r, mul(v, P));
+        if (ysat && satN_y<C>(a.op, p + (long)ix * pitch, a.My, iy, v)) r = add(r, mul(v, P));
         C s = to_c<C>(a.f[F_MN][i]);
         time_update<CPST>(s, r, c);
         finish_point(a.f[F_MN], a.res[F_MN], i, s, r, c, kr, kc,
@@ -62,7 +64,9 @@ __device__ __forceinline__ void acoustic_velocity_point(const StepArgs<S, C> &a,
         } else {
             v = dx_from_M<C>(a.op, p, pitch, a.Mx, ix, iy);
             r = add(r, mul(v, P));
-            if (sat_NM<C>(a.op, p, pitch, a.Mx, ix, iy, v)) r = add(r, mul(v, P));
+            const bool sx = xif ? satN_if<C>(a.op, a.Mx, ix, [&](int q) { return ld<C>(p, (long)q * pitch + iy); }, v)
+                                : sat_NM<C>(a.op, p, pitch, a.Mx, ix, iy, v);
+            if (sx) r = add(r, mul(v, P));
         }
         C s = to_c<C>(a.f[F_NM][i]);
         time_update<CPST>(s, r, c);
@@ -86,7 +90,11 @@ __device__ __forceinline__ void acoustic_pressure_point(const StepArgs<S, C> &a,
     C v = PERIODIC ? dx_periodic<true, C>(a.op, a.f[F_NM], pitch, a.Mx, ix, iy)
                    : dx_from_N<C>(a.op, a.f[F_NM], pitch, a.Mx, ix, iy);
     r = add(r, mul(v, K));
-    v = dy_periodic<true, C>(a.op, a.f[F_MN] + (long)ix * pitch, a.My, iy);
+    if (!PERIODIC && (a.bnd & BND_X_IF) &&
+        satM_if<C>(a.op, a.Mx, ix, [&](int q) { return ld<C>(a.f[F_NM], (long)q * pitch + iy); }, v))
+        r = add(r, mul(v, K));
+    v = PERIODIC ? dy_periodic<true, C>(a.op, a.f[F_MN] + (long)ix * pitch, a.My, iy)
+                 : dy_any<true, C>(a.op, a.f[F_MN] + (long)ix * pitch, a.My, iy, a.bnd & BND_Y_SAT);
     r = add(r, mul(v, K));
     C s = to_c<C>(a.f[F_MM0][i]);
     time_update<CPST>(s, r, c);

@@ -104,8 +104,21 @@ __global__ void k_material_finalize(MaterialArgs m)
     const bool elastic = m.physics == 0;
     K **coef = (K **)m.coef;
     // y factor of the norm (grid_energy.cpp:123-152): dx everywhere, then 1 on the first and 0 on
-    // the last (duplicate) point of an N-type-y grid
+    // the last (duplicate) point of an N-type-y grid; with free y ends the x rule along y
+    // (A_diag * dx, storage-rounded, on the end columns by the grid's y type)
     auto y_factor = [&](int g, double w) {
+        if (m.sat_y) {
+            const int n = m.cols[g];
+            double f = dx;
+            if (n == m.My + 1) {
+                if (iy < 4) f = m.nxN[iy];
+                else if (iy >= n - 4) f = m.nxN[4 + iy - (n - 4)];
+            } else {
+                if (iy < 3) f = m.nxM[iy];
+                else if (iy >= n - 3) f = m.nxM[3 + iy - (n - 3)];
+            }
+            return mul(w, f);
+        }
         w = mul(w, dx);
         if (m.cols[g] == m.My + 1 && iy == m.My) w = mul(w, 0.);
         return w;

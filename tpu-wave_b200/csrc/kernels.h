@@ -31,6 +31,7 @@ struct MaterialArgs {
     double nxN[8], nxM[6];    // A_diag * dx rounded to the storage type: N-type L[4] R[4], M-type L[3] R[3]
     int physics, periodic;
     int row_off, Mx_glob;     // a slab: its local row 0 is global row row_off of a grid of Mx_glob cells
+    int sat_y;                // free y ends: the y factor of the energy norm follows the x rule
     int *err;                 // bit 2 set: a coefficient outside the normal range of the FP16 storage
 };
 // define the stepping coefficients (stored as K) and energy weights (make_density_reciprocal,

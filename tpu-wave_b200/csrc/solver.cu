@@ -74,6 +74,7 @@ struct tw_solver {
     // warps, receivers as one flat list in d_rcv_list
     bool afused = false;
     bool pfuse = false;               // double-buffered periodic acoustic: may join a fused batch
+    int bnd = 0;                      // BND_X_IF | BND_Y_SAT (stepper.cuh): two-launch kernels
     int n_rcv_list = 0;
     void *f2[5] = {}, *res2[5] = {};
     int parity = 0;                   // which buffer holds the current state (0: f/res, 1: f2/res2)
@@ -185,6 +186,7 @@ StepArgs<S, C> step_args(const tw_solver *s)
     a.max_steps = s->d.max_steps;
     a.step = s->d_step;
     a.flags = s->d_flags;
+    a.bnd = s->bnd;
     return a;
 }
 
@@ -404,6 +406,7 @@ int finalize_material(tw_solver *s)
     m.periodic = s->periodic;
     m.row_off = (int)s->row_off;
     m.Mx_glob = (int)s->Mx_glob;
+    m.sat_y = s->d.sat_y;
     const bool f64 = s->d.precision == TW_FP64;
     for (int i = 0; i < 4; i++) {
         const double l = SbpTables::A_N_L[i] * m.dx, r = SbpTables::A_N_R[i] * m.dx;
@@ -644,7 +647,7 @@ int tw_create_slab(tw_solver **out, const tw_grid_desc *desc, long row0, long ro
     if (!out || !desc) return TW_ERR_INVALID;
     *out = nullptr;
     const tw_grid_desc &g = *desc;
-    if (g.physics != TW_ELASTIC || g.bc_x != TW_BC_SAT_FREE) return TW_ERR_UNSUPPORTED;
+    if (g.physics != TW_ELASTIC || g.bc_x != TW_BC_SAT_FREE || g.sat_y) return TW_ERR_UNSUPPORTED;
     constexpr long H = 4;   // halo rows: the step's x stencils reach four rows of the old state
     if (row0 < 0 || row1 > g.Mx || row1 - row0 < 2 * FS_ZONE || (row0 > 0 && row0 < 2 * FS_ZONE) ||
         (row1 < g.Mx && g.Mx - row1 < 2 * FS_ZONE))
@@ -667,8 +670,14 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
     *out = nullptr;
     const tw_grid_desc &d = *desc;
     if (d.physics != TW_ELASTIC && d.physics != TW_ACOUSTIC) return TW_ERR_INVALID;
-    if (d.bc_x != TW_BC_SAT_FREE && d.bc_x != TW_BC_PERIODIC) return TW_ERR_INVALID;
+    if (d.bc_x != TW_BC_SAT_FREE && d.bc_x != TW_BC_PERIODIC && d.bc_x != TW_BC_SAT_INTERFACE) return TW_ERR_INVALID;
     if (d.physics == TW_ELASTIC && d.bc_x == TW_BC_PERIODIC) return TW_ERR_UNSUPPORTED;
+    if (d.sat_y != 0 && d.sat_y != 1) return TW_ERR_INVALID;
+    // the interface and the y free surfaces: the two-launch kernels, FP64 / FP32 storage, SAT x
+    if ((d.bc_x == TW_BC_SAT_INTERFACE || d.sat_y) &&
+        (d.bc_x == TW_BC_PERIODIC || d.precision == TW_BF16 || d.precision == TW_FP16 || d.coef_fp16))
+        return TW_ERR_UNSUPPORTED;
+    if (d.sat_y && d.My < 8) return TW_ERR_INVALID;
     if (d.precision < TW_FP64 || d.precision > TW_FP16) return TW_ERR_INVALID;
     if (d.cpst < TW_CPST_00 || d.cpst > TW_CPST_SPLIT) return TW_ERR_INVALID;
     const bool narrow = d.precision == TW_BF16 || d.precision == TW_FP16;
@@ -697,6 +706,7 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
     s->own1 = sl.on ? sl.own1 : d.Mx;
     s->elastic = d.physics == TW_ELASTIC;
     s->periodic = d.bc_x == TW_BC_PERIODIC;
+    s->bnd = (d.bc_x == TW_BC_SAT_INTERFACE ? BND_X_IF : 0) | (d.sat_y ? BND_Y_SAT : 0);
     s->esz = d.precision == TW_FP64 ? 8 : (d.precision == TW_FP32 ? 4 : 2);
     const int Mx_ = (int)d.Mx, My_ = (int)d.My;
     const int rws[5] = {Mx_ + 1, Mx_, Mx_ + 1, Mx_, Mx_}, cls[5] = {My_ + 1, My_ + 1, My_, My_, My_};
@@ -733,7 +743,7 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
         cudaMemsetAsync(s->coef[k], 0, n * csz, s->st);
         cudaMemsetAsync(s->w[k], 0, n * sizeof(double), s->st);
     }
-    if (s->elastic) {
+    if (s->elastic && !s->bnd) {
         // fused elastic path: a second copy of the state and the strip x segment geometry
         s->fused = true;
         switch (d.precision) {
@@ -926,6 +936,9 @@ int tw_set_source(tw_solver *s, int grid, long ix, long iy)
     // the reference stops on a source on the free-surface node rows (forward.cpp:95-96); on the
     // periodic seam it only warns (:97-98) and so does nothing here
     if (!s->periodic && Nx && (ix == 0 || ix == s->Mx_glob)) return TW_ERR_WEAK_BOUNDARY;
+    // free y ends: the same rule on the end columns of an N-type-y grid
+    const bool Ny = grid == TW_NN || grid == TW_MN;
+    if (s->d.sat_y && Ny && (iy == 0 || iy == s->d.My)) return TW_ERR_WEAK_BOUNDARY;
     const long lx = owned_row(s, grid, ix);   // a slab injects only a source in its own rows
     s->src_grid = lx >= 0 ? grid : -1;
     s->src_ix = lx;
@@ -1587,7 +1600,7 @@ extern "C" int tw_adjoint_gradient(tw_solver *s, int nt, const double *obs, int 
 {
     if (check(s) || nt < 1 || ckpt_every < 1 || (!obs && !s->rcv_tab.empty())) return TW_ERR_INVALID;
     if (!s->elastic || s->d.cpst != TW_CPST_00 || (s->d.precision != TW_FP64 && s->d.precision != TW_FP32) ||
-        s->d.coef_fp16)
+        s->d.coef_fp16 || s->bnd)
         return TW_ERR_UNSUPPORTED;
     if (!s->mat_ready) return TW_ERR_STATE;
     if (s->steps_done != 0) return TW_ERR_STATE;   // the forward sweep starts at step 0
@@ -1784,8 +1797,10 @@ int tw_batch_create(tw_batch **out, tw_solver *const *shots, int n)
             if (shots[q] == s) return TW_ERR_INVALID;
         if (s->elastic || s->d.energy) return TW_ERR_UNSUPPORTED;
         if (s->d.cpst != TW_CPST_00 && s->d.cpst != TW_CPST_3R && s->d.cpst != TW_CPST_6R) return TW_ERR_UNSUPPORTED;
+        // one kernel family per batch: periodic or SAT x (each shot's own boundary variant rides in
+        // its arguments)
         if (s->d.device != s0->d.device || s->d.precision != s0->d.precision || s->d.cpst != s0->d.cpst ||
-            s->d.bc_x != s0->d.bc_x)
+            s->periodic != s0->periodic)
             return TW_ERR_UNSUPPORTED;
         if (!s->mat_ready) return TW_ERR_STATE;
     }

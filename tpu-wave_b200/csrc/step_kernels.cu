@@ -23,15 +23,20 @@ __global__ void __launch_bounds__(256) k_elastic_velocity(StepArgs<S, C> a)
     const long i = (long)ix * pitch + iy;
     constexpr bool kr = Cpst<CPST>::keep_r, kc = Cpst<CPST>::keep_c;
 
+    const bool xif = a.bnd & BND_X_IF, ysat = a.bnd & BND_Y_SAT;
     if (ix < a.Mx) {   // MN (Mx x My+1): velocity along y; x from NN, y from MM syy
         C r, c;
         load_rc<S, C, CPST>(a.res[F_MN], i, r, c);
         const C P = __ldg(a.coef[F_MN] + i);
         C v = dx_from_N<C>(a.op, a.f[F_NN], pitch, a.Mx, ix, iy);
         r = add(r, mul(v, P));
-        if (sat_MN<C>(a.op, a.f[F_NN], pitch, a.Mx, ix, iy, v)) r = add(r, mul(v, P));
-        v = dy_periodic<false, C>(a.op, a.f[F_MM1] + (long)ix * pitch, a.My, iy);
+        const bool sx = xif ? satM_if<C>(a.op, a.Mx, ix, [&](int q) { return ld<C>(a.f[F_NN], (long)q * pitch + iy); }, v)
+                            : sat_MN<C>(a.op, a.f[F_NN], pitch, a.Mx, ix, iy, v);
+        if (sx) r = add(r, mul(v, P));
+        const S *m1 = a.f[F_MM1] + (long)ix * pitch;
+        v = dy_any<false, C>(a.op, m1, a.My, iy, ysat);
         r = add(r, mul(v, P));
+        if (ysat && satN_y<C>(a.op, m1, a.My, iy, v)) r = add(r, mul(v, P));
         C s = to_c<C>(a.f[F_MN][i]);
         time_update<CPST>(s, r, c);
         finish_point(a.f[F_MN], a.res[F_MN], i, s, r, c, kr, kc,
@@ -43,9 +48,13 @@ __global__ void __launch_bounds__(256) k_elastic_velocity(StepArgs<S, C> a)
         const C P = __ldg(a.coef[F_NM] + i);
         C v = dx_from_M<C>(a.op, a.f[F_MM0], pitch, a.Mx, ix, iy);
         r = add(r, mul(v, P));
-        if (sat_NM<C>(a.op, a.f[F_MM0], pitch, a.Mx, ix, iy, v)) r = add(r, mul(v, P));
-        v = dy_periodic<true, C>(a.op, a.f[F_NN] + (long)ix * pitch, a.My, iy);
+        const bool sx = xif ? satN_if<C>(a.op, a.Mx, ix, [&](int q) { return ld<C>(a.f[F_MM0], (long)q * pitch + iy); }, v)
+                            : sat_NM<C>(a.op, a.f[F_MM0], pitch, a.Mx, ix, iy, v);
+        if (sx) r = add(r, mul(v, P));
+        const S *nn = a.f[F_NN] + (long)ix * pitch;
+        v = dy_any<true, C>(a.op, nn, a.My, iy, ysat);
         r = add(r, mul(v, P));
+        if (ysat && satM_y<C>(a.op, nn, a.My, iy, v)) r = add(r, mul(v, P));
         C s = to_c<C>(a.f[F_NM][i]);
         time_update<CPST>(s, r, c);
         finish_point(a.f[F_NM], a.res[F_NM], i, s, r, c, kr, kc,
@@ -65,14 +74,17 @@ __global__ void __launch_bounds__(256) k_elastic_stress(StepArgs<S, C> a)
     constexpr bool kr = Cpst<CPST>::keep_r, kc = Cpst<CPST>::keep_c;
     const double *si = a.src_inc + 0;
     const bool src_here = ix == a.src_ix && iy == a.src_iy;
+    const bool xif = a.bnd & BND_X_IF, ysat = a.bnd & BND_Y_SAT;
 
-    {   // NN (Mx+1 x My+1): shear stress; x from MN, y from NM
+    {   // NN (Mx+1 x My+1): shear stress; x from MN (+ the x interface), y from NM
         C r, c;
         load_rc<S, C, CPST>(a.res[F_NN], i, r, c);
         const C P = __ldg(a.coef[F_NN] + i);
         C v = dx_from_M<C>(a.op, a.f[F_MN], pitch, a.Mx, ix, iy);
         r = add(r, mul(v, P));
-        v = dy_periodic<false, C>(a.op, a.f[F_NM] + (long)ix * pitch, a.My, iy);
+        if (xif && satN_if<C>(a.op, a.Mx, ix, [&](int q) { return ld<C>(a.f[F_MN], (long)q * pitch + iy); }, v))
+            r = add(r, mul(v, P));
+        v = dy_any<false, C>(a.op, a.f[F_NM] + (long)ix * pitch, a.My, iy, ysat);
         r = add(r, mul(v, P));
         C s = to_c<C>(a.f[F_NN][i]);
         time_update<CPST>(s, r, c);
@@ -88,7 +100,12 @@ __global__ void __launch_bounds__(256) k_elastic_stress(StepArgs<S, C> a)
         r0 = add(r0, mul(v, L));
         r1 = add(r1, mul(v, L));
         r0 = add(r0, mul(v, M2));
-        v = dy_periodic<true, C>(a.op, a.f[F_MN] + (long)ix * pitch, a.My, iy);
+        if (xif && satM_if<C>(a.op, a.Mx, ix, [&](int q) { return ld<C>(a.f[F_NM], (long)q * pitch + iy); }, v)) {
+            r0 = add(r0, mul(v, L));
+            r1 = add(r1, mul(v, L));
+            r0 = add(r0, mul(v, M2));
+        }
+        v = dy_any<true, C>(a.op, a.f[F_MN] + (long)ix * pitch, a.My, iy, ysat);
         r0 = add(r0, mul(v, L));
         r1 = add(r1, mul(v, L));
         r1 = add(r1, mul(v, M2));

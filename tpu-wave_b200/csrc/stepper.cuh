@@ -30,7 +30,14 @@ struct StepArgs {
     int max_steps;
     const int *step;          // device step counter (read by every kernel of a step)
     int *flags;               // sticky error flags
+    int bnd;                  // BND_X_IF | BND_Y_SAT: the boundary variants below (0: the reference's)
 };
+
+// boundary variants beyond the reference's runs: BND_X_IF joins the two x ends by the SAT
+// interface penalty (the reference's secure_bdry branch for a boundary type other than 'F',
+// grid_drvt.tpp:575-693, on every grid); BND_Y_SAT puts free surfaces on the y ends too (SBP
+// closures and the velocity grids' penalties along y, with the x tables)
+enum { BND_X_IF = 1, BND_Y_SAT = 2 };
 
 // read index of an M-type periodic neighbour (n points): wrap modulo n
 __device__ __forceinline__ int wrap(int j, int n) { return j < 0 ? j + n : (j >= n ? j - n : j); }
@@ -170,6 +177,88 @@ __device__ __forceinline__ bool sat_NM(const Ops<C> &o, A mm, long pitch, int Mx
 #pragma unroll
         for (int w = 0; w < 3; w++) send = add(send, mul(o.pMR[w], ld<C>(mm, (long)(Mx - 3 + w) * pitch + iy)));
         v = mul(o.satNR, sub(send, C(0)));
+        return true;
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------- boundary variants
+// the SAT interface penalty of an M-type-x point i (rows 0..M-1) whose x neighbour is N-type
+// (rows 0..M): the neighbour's end rows projected with {1}; rows 0..2 are penalised with eta = +1/2
+// toward the right end's projection (RECV_L = SEND_R), rows M-3..M-1 with eta = -1/2 toward the
+// left's. eta * A_inv_projection is half the free-surface product, exactly.
+template <class C, class G>
+__device__ __forceinline__ bool satM_if(const Ops<C> &o, int M, int i, G get, C &v)
+{
+    if (i >= 3 && i < M - 3) return false;
+    const C sL = add(C(0), mul(o.pN, get(0))), sR = add(C(0), mul(o.pN, get(M)));
+    v = i < 3 ? mul(mul(C(0.5), o.satML[i]), sub(sL, sR)) : mul(mul(C(0.5), o.satMR[i - (M - 3)]), sub(sR, sL));
+    return true;
+}
+
+// the SAT interface penalty of an N-type-x point i (rows 0..M) whose neighbour is M-type (rows
+// 0..M-1): the neighbour extrapolated to each end with {15/8, -5/4, 3/8}, penalties on rows 0 and M
+template <class C, class G>
+__device__ __forceinline__ bool satN_if(const Ops<C> &o, int M, int i, G get, C &v)
+{
+    if (i != 0 && i != M) return false;
+    C sL = C(0), sR = C(0);
+#pragma unroll
+    for (int w = 0; w < 3; w++) sL = add(sL, mul(o.pML[w], get(w)));
+#pragma unroll
+    for (int w = 0; w < 3; w++) sR = add(sR, mul(o.pMR[w], get(M - 3 + w)));
+    v = i == 0 ? mul(mul(C(0.5), o.satNL), sub(sL, sR)) : mul(mul(C(0.5), o.satNR), sub(sR, sL));
+    return true;
+}
+
+// y derivative with SBP closures at both y ends (free surfaces on all four sides): the x
+// operators dxN / dxM applied along the row
+template <bool FROM_N, class C, class A>
+__device__ __forceinline__ C dy_sbp(const Ops<C> &o, A row, int My, int iy)
+{
+    auto get = [&](int c) { return ld<C>(row, (long)c); };
+    if constexpr (FROM_N) return dxN<C>(o, My, iy, get);
+    else return dxM<C>(o, My, iy, get);
+}
+
+template <bool FROM_N, class C, class A>
+__device__ __forceinline__ C dy_any(const Ops<C> &o, A row, int My, int iy, bool sat_y)
+{
+    return sat_y ? dy_sbp<FROM_N, C>(o, row, My, iy) : dy_periodic<FROM_N, C>(o, row, My, iy);
+}
+
+// free-surface penalty on the y ends of an N-type-y velocity point (MN, neighbour syy of M type):
+// syy extrapolated to column 0 / My, eta = +1 / -1
+template <class C, class A>
+__device__ __forceinline__ bool satN_y(const Ops<C> &o, A row, int My, int iy, C &v)
+{
+    if (iy != 0 && iy != My) return false;
+    C send = C(0);
+    if (iy == 0) {
+#pragma unroll
+        for (int w = 0; w < 3; w++) send = add(send, mul(o.pML[w], ld<C>(row, (long)w)));
+        v = mul(o.satNL, sub(send, C(0)));
+    } else {
+#pragma unroll
+        for (int w = 0; w < 3; w++) send = add(send, mul(o.pMR[w], ld<C>(row, (long)(My - 3 + w))));
+        v = mul(o.satNR, sub(send, C(0)));
+    }
+    return true;
+}
+
+// the same for an M-type-y velocity point (NM, neighbour sxy of N type): sxy at column 0 / My,
+// penalties on columns 0..2 / My-3..My-1
+template <class C, class A>
+__device__ __forceinline__ bool satM_y(const Ops<C> &o, A row, int My, int iy, C &v)
+{
+    if (iy < 3) {
+        const C send = add(C(0), mul(o.pN, ld<C>(row, 0L)));
+        v = mul(o.satML[iy], sub(send, C(0)));
+        return true;
+    }
+    if (iy >= My - 3) {
+        const C send = add(C(0), mul(o.pN, ld<C>(row, (long)My)));
+        v = mul(o.satMR[iy - (My - 3)], sub(send, C(0)));
         return true;
     }
     return false;
