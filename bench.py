@@ -557,9 +557,10 @@ def run_acoustic512(args):
     dt = 0.5 * dx / np.sqrt(2.0)
     rcv_ix, rcv_iy = np.full(16, 128), 16 + 32 * np.arange(16)
     out = {}
-    for mode, bc in (("periodic", tw.PERIODIC), ("free_surface", tw.SAT_FREE)):
+    for mode, bc, sat_y in (("periodic", tw.PERIODIC, False), ("free_surface", tw.SAT_FREE, False),
+                            ("all_sides", tw.SAT_FREE, True)):
         s = tw.Solver(n, n, 1, n, dt, physics=tw.ACOUSTIC, bc_x=bc, precision="f32", cpst="00", central_f=10.0,
-                      time_delay=0.25, max_steps=K + 64, energy=False)
+                      time_delay=0.25, max_steps=K + 64, energy=False, sat_y=sat_y)
         s.set_material_grid(tw.NM, 0, np.ones((n + 1, n)))
         s.set_material_grid(tw.MN, 0, np.ones((n, n + 1)))
         s.set_material_grid(tw.MM, 0, np.ones((n, n)))
@@ -579,6 +580,22 @@ def run_acoustic512(args):
                      "hbm_frac_at_36B": n * n * K / (ms / 1e3) * 36 / 1e9 / measured_peaks()[0],
                      "traces": s.read_receivers()[:, 0, :]}
         s.close()
+        if mode == "all_sides":
+            # no reference run exists for free y ends: the discrete energy after the source stops
+            # (t > delay + 3 / f0) is the check, over 2000 steps (FP64, energy every step)
+            ne = 2000
+            s = tw.Solver(n, n, 1, n, dt, physics=tw.ACOUSTIC, bc_x=bc, precision="f64", cpst="00",
+                          central_f=10.0, time_delay=0.25, max_steps=ne, energy=True, sat_y=True)
+            s.set_material_grid(tw.NM, 0, np.ones((n + 1, n)))
+            s.set_material_grid(tw.MN, 0, np.ones((n, n + 1)))
+            s.set_material_grid(tw.MM, 0, np.ones((n, n)))
+            s.set_source(tw.MM, n // 2, n // 2)
+            s.run(ne)
+            ek, ep0, ep1 = s.read_energy()
+            s.close()
+            E = (ek + 0.5 * (ep0 + ep1))[int((0.25 + 3 / 10.0) / dt) + 1:]
+            out[mode]["energy_min_over_max_after_source"] = float(E.min() / E.max())
+            out[mode]["energy_steps"] = ne
     # the reference's single-core solver (periodic) on the first steps of the same run
     cs = min(K, args.cpu_steps * 10)
     case = refrun.AcousticCase(Nx=n, Ny=n, dx=dx, dt=dt, coef_vx=np.ones((n + 1, n)), coef_vy=np.ones((n, n + 1)),

@@ -69,7 +69,7 @@ void launch_energy(const EnergyArgs<S, C> &e, cudaStream_t st);
 #define TW_FS_MIN_BLOCKS 5            // CTAs per SM the register allocation is sized for
 #endif
 #ifndef TW_FS_CTAS_PER_SM
-#define TW_FS_CTAS_PER_SM 15          // CTAs per SM the elastic row segmentation aims at
+#define TW_FS_CTAS_PER_SM 60          // CTAs per SM the elastic row segmentation aims at (12 waves)
 #endif
 #ifndef TW_AC_CTAS_PER_SM
 #define TW_AC_CTAS_PER_SM 15          // the same for the fused acoustic step and batches
