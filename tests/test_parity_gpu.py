@@ -230,3 +230,41 @@ def test_many_strips_and_segments_match_oracle(cpst, prec):
     assert np.array_equal(got["traces"], want.traces)
     for k in ("E_k", "E_p0", "E_p1"):
         assert energy_close(got[k], getattr(want, k)), k
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_energy_before_a_step_follows_the_state_written_into_the_handle(tw, prec):
+    """E_p0 of a step sums the stresses the step starts from: after 20 steps (graph replays
+    included) E_p0 follows the previous step's E_p1, and after a stress field written into the
+    handle, the next 20 steps' energies equal the oracle's from that state."""
+    Mx, My = 40, 36
+    case = elastic_case(Mx, My, seed=8, Nt=20, rcvs=[], model="layered")
+    T = np.float64 if prec == "f64" else np.float32
+    s = tw.Solver(Mx, My, case.num_dx, case.den_dx, case.dt, precision=prec, central_f=case.central_f,
+                  time_delay=case.time_delay, max_steps=40)
+    try:
+        shp = (Mx + 2, My + 2)
+        s.set_material_model(case.rho.reshape(shp), case.vp.reshape(shp), case.vs.reshape(shp))
+        s.set_source_location(*case.src)
+        s.run(20)
+        keys = [(tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)]
+        state = [s.read_field(g, f) for g, f in keys]
+        state[3] = (state[3] + np.random.default_rng(1).standard_normal(state[3].shape) * 1e-3).astype(T).astype(np.float64)
+        s.write_field(tw.MM, 0, state[3])
+        s.run(20)
+        E_k, E_p0, E_p1 = s.read_energy()
+    finally:
+        s.close()
+    assert energy_close(E_p0[1:20], E_p1[:19])
+    want = orc.elastic_run(case_shifted(case, 20), prec, fields0=state)
+    for got, ref in ((E_p0[20:], want.E_p0), (E_k[20:], want.E_k), (E_p1[20:], want.E_p1)):
+        assert energy_close(got, ref)
+    assert not np.isclose(E_p0[20], E_p1[19], rtol=1e-6)   # the written state changed the energy
+
+
+def case_shifted(case, k):
+    """`case` started k steps later: the source's delay moves back by k dt."""
+    import copy
+    c = copy.copy(case)
+    c.time_delay = case.time_delay - k * case.dt
+    return c

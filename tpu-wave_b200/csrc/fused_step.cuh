@@ -779,7 +779,7 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
 
 // ------------------------------------------------------------------------------- the launch
 template <class S, class C, int CPST, bool ENERGY, class K>
-__global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 4 : TW_FS_MIN_BLOCKS) k_elastic_fused(FusedArgs<S, C> a)
+__global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? TW_FS_MIN_BLOCKS_E : TW_FS_MIN_BLOCKS) k_elastic_fused(FusedArgs<S, C> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int it = *a.step;

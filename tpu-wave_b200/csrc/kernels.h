@@ -68,6 +68,9 @@ void launch_energy(const EnergyArgs<S, C> &e, cudaStream_t st);
 #ifndef TW_FS_MIN_BLOCKS
 #define TW_FS_MIN_BLOCKS 5            // CTAs per SM the register allocation is sized for
 #endif
+#ifndef TW_FS_MIN_BLOCKS_E
+#define TW_FS_MIN_BLOCKS_E 4          // the same for the energy-every-step variant
+#endif
 #ifndef TW_FS_CTAS_PER_SM
 #define TW_FS_CTAS_PER_SM 60          // CTAs per SM the elastic row segmentation aims at (12 waves)
 #endif
