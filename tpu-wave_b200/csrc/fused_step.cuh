@@ -133,6 +133,14 @@ struct Row {   // global values one interior iteration consumes
 // values it will need for a row asynchronously (cp.async) into its own slots a few rows ahead and
 // reads them back when the row comes up: the copies need no registers while in flight, and as a
 // lane only ever reads what it copied itself, no warp or block barrier is involved.
+// resident CTAs per SM the register allocation is sized for (an FP64 value takes two registers:
+// at the FP32 counts the FP64 kernels spilled 400-640 bytes a thread)
+template <class C, bool ENERGY>
+constexpr int fs_min_blocks()
+{
+    return sizeof(C) == 8 ? (ENERGY ? TW_FS_MIN_BLOCKS_E64 : TW_FS_MIN_BLOCKS_64) : (ENERGY ? TW_FS_MIN_BLOCKS_E : TW_FS_MIN_BLOCKS);
+}
+
 template <class C, bool ENERGY>
 constexpr int ring_depth() { return (sizeof(C) == 8 || ENERGY) ? 2 : TW_FS_RING; }
 
@@ -779,7 +787,7 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
 
 // ------------------------------------------------------------------------------- the launch
 template <class S, class C, int CPST, bool ENERGY, class K>
-__global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? TW_FS_MIN_BLOCKS_E : TW_FS_MIN_BLOCKS) k_elastic_fused(FusedArgs<S, C> a)
+__global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<C, ENERGY>()) k_elastic_fused(FusedArgs<S, C> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int it = *a.step;

@@ -71,6 +71,12 @@ void launch_energy(const EnergyArgs<S, C> &e, cudaStream_t st);
 #ifndef TW_FS_MIN_BLOCKS_E
 #define TW_FS_MIN_BLOCKS_E 4          // the same for the energy-every-step variant
 #endif
+#ifndef TW_FS_MIN_BLOCKS_64
+#define TW_FS_MIN_BLOCKS_64 3         // FP64 fields
+#endif
+#ifndef TW_FS_MIN_BLOCKS_E64
+#define TW_FS_MIN_BLOCKS_E64 2        // FP64 fields, energy every step
+#endif
 #ifndef TW_FS_CTAS_PER_SM
 #define TW_FS_CTAS_PER_SM 60          // CTAs per SM the elastic row segmentation aims at (12 waves)
 #endif
