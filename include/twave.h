@@ -204,7 +204,7 @@ TW_API int tw_material_map_noalloc(const double *d_rho, const double *d_vp, cons
 
 /* ---- slab decomposition ------------------------------------------------------------------
  * One elastic grid split along x (data rows) into slabs, each a handle of its own (its own GPU,
- * or all on one). SURVEY-style row decomposition as the reference's MPI tree exchanges halo strips
+ * or all on one), a row decomposition as the reference's MPI tree exchanges halo strips
  * (mpi/src/cpp/namespaces.hpp:611-635), here four rows wide once per step, since a fused step
  * reaches four rows of the old state. tw_create_slab makes the handle of global rows
  * [row0, row1) of the grid `desc` describes (desc->Mx is the whole grid's): its arrays hold those
@@ -236,6 +236,19 @@ TW_API int tw_slab_halo(tw_solver *s, int side, int recv, int f, void **ptr, lon
  * buffer size; call with dst NULL to learn it. Both run on the handle's stream. */
 TW_API int tw_slab_pack(tw_solver *s, int side, void *dst, long *bytes);
 TW_API int tw_slab_unpack(tw_solver *s, int side, const void *src);
+
+/* Step the slabs of a whole grid together, `steps` steps, with the halo exchange fused into the
+ * step kernel: while a slab's step writes its rows next to a cut, it also stores them straight
+ * into the neighbour's halo rows of the same step's output buffers (peer stores over NVLink when
+ * the neighbour is on another GPU of this process; peer access is enabled here, and
+ * TW_ERR_UNSUPPORTED is returned where the GPUs cannot reach each other). Slab k's step waits on
+ * its neighbours' previous step (CUDA events), so no step overwrites a halo row a neighbour still
+ * reads. `slabs` lists every slab of the grid top to bottom (consecutive rows, the same step count
+ * and set-up; FP32 / FP64 storage and coefficients, else TW_ERR_UNSUPPORTED); no tw_slab_exchange
+ * is needed between or after the calls. Returns after queuing;
+ * tw_sync each handle. No counterpart in the reference, whose MPI exchange is a separate
+ * MPI_Sendrecv per halo strip (mpi/src/cpp/namespaces.hpp:611-635). */
+TW_API int tw_slab_run(tw_solver *const *slabs, int n, int steps);
 
 /* ---- adjoint gradient ---------------------------------------------------------------------
  * No counterpart in the reference (it has no adjoint). Full-waveform gradient of the misfit

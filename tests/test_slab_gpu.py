@@ -1,8 +1,9 @@
-"""Slab decomposition of one elastic grid (tw_create_slab / tw_slab_exchange), on one GPU: the
-grid cut into slabs along x, every slab stepped and the halos exchanged after each step, must
-give the whole grid's fields on every owned row and its traces bit for bit, and its energies to
-1e-12 (sums in another order). Covers the free-surface zones of the first and last slab, open
-inner edges, compensation arrays in the halo, sources and receivers in any slab."""
+"""Slab decomposition of one elastic grid (tw_create_slab / tw_slab_exchange / tw_slab_run), on
+one GPU: the grid cut into slabs along x, every slab stepped and the halos exchanged after each
+step (by copies, by packed buffers, or by the step kernel's own stores into the neighbours' halo
+rows), must give the whole grid's fields on every owned row and its traces bit for bit, and its
+energies to 1e-12 (sums in another order). Covers the free-surface zones of the first and last
+slab, open inner edges, compensation arrays in the halo, sources and receivers in any slab."""
 import numpy as np
 import pytest
 
@@ -32,7 +33,7 @@ def packed_exchange(up, lo):
     lo.sync()
 
 
-def run(tw, case, prec, cuts, f0, r0, Nt, slab=True, packed=False):
+def run(tw, case, prec, cuts, f0, r0, Nt, slab=True, mode="copy"):
     shp = (case.Mx + 2, case.My + 2)
     kw = dict(precision=prec, cpst=case.cpst, central_f=case.central_f, time_delay=case.time_delay, max_steps=Nt)
     slots = [(tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)]
@@ -51,11 +52,14 @@ def run(tw, case, prec, cuts, f0, r0, Nt, slab=True, packed=False):
         if r0 is not None:
             for (g, f), a in zip(slots, r0):
                 h.write_resid(g, f, a[off:off + h.shape(g)[0]])
-    for _ in range(Nt):
+    if mode == "fused":   # in two calls: the buffers alternate across calls too
+        tw.Solver.slab_run(hs, 3)
+        tw.Solver.slab_run(hs, Nt - 3)
+    for _ in range(Nt if mode != "fused" else 0):
         for h in hs:
             h.step(1)
         for up, lo in zip(hs[:-1], hs[1:]):
-            if packed:
+            if mode == "packed":
                 packed_exchange(up, lo)
             else:
                 up.exchange(lo)
@@ -76,10 +80,10 @@ def run(tw, case, prec, cuts, f0, r0, Nt, slab=True, packed=False):
     return fields, traces, energy
 
 
-@pytest.mark.parametrize("packed", [False, True])
+@pytest.mark.parametrize("mode", ["copy", "packed", "fused"])
 @pytest.mark.parametrize("prec,cpst", [("f32", "00"), ("f64", "6R"), ("f32", "3C")])
 @pytest.mark.parametrize("cuts", [(0, 24, 48, 72), (0, 40, 72), (0, 16, 56, 72)])
-def test_slabs_equal_the_whole_grid(prec, cpst, cuts, packed):
+def test_slabs_equal_the_whole_grid(prec, cpst, cuts, mode):
     tw = load_twave()
     Mx, My, den, Nt = 72, 60, 72, 9
     rcvs = [("N", "M", 2, den, 7, 2 * den), ("M", "M", 2 * 23 + 1, 2 * den, 2 * 9 + 1, 2 * den),
@@ -93,7 +97,7 @@ def test_slabs_equal_the_whole_grid(prec, cpst, cuts, packed):
     f0 = [(rng.standard_normal(s) * 1e-2).astype(T).astype(np.float64) for s in shapes]
     r0 = None if cpst == "00" else [(rng.standard_normal(s) * 1e-9).astype(T).astype(np.float64) for s in shapes]
     want = run(tw, case, prec, None, f0, r0, Nt, slab=False)
-    got = run(tw, case, prec, cuts, f0, r0, Nt, packed=packed)
+    got = run(tw, case, prec, cuts, f0, r0, Nt, mode=mode)
     for k in range(5):
         assert np.array_equal(got[0][k], want[0][k]), k
     assert np.array_equal(got[1], want[1])
@@ -111,5 +115,14 @@ def test_slab_arguments():
     b = tw.Solver.slab(72, 60, 1, 72, 1e-3, 48, 72)
     with pytest.raises(tw.TwError):
         a.exchange(b)                                     # not adjacent
+    with pytest.raises(tw.TwError):
+        tw.Solver.slab_run([a, b], 1)                     # not the whole grid, not consecutive
+    shp = (74, 62)
+    rho, vp, vs = np.full(shp, 2.0), np.full(shp, 3.0), np.full(shp, 1.7)
+    c = tw.Solver.slab(72, 60, 1, 72, 1e-3, 40, 72, max_steps=4)
+    c.set_material_model(rho, vp, vs)
+    with pytest.raises(tw.TwError):
+        tw.Solver.slab_run([a, c], 1)                     # a has no material yet
     a.close()
     b.close()
+    c.close()

@@ -112,6 +112,7 @@ def lib() -> C.CDLL:
         L.tw_data_misfit.argtypes = [vp, dp, dp, dp]
         L.tw_create_slab.argtypes = [C.POINTER(vp), C.POINTER(GridDesc), C.c_long, C.c_long]
         L.tw_slab_exchange.argtypes = [vp, vp]
+        L.tw_slab_run.argtypes = [C.POINTER(vp), C.c_int, C.c_int]
         L.tw_slab_pack.argtypes = [vp, C.c_int, vp, lp]
         L.tw_slab_unpack.argtypes = [vp, C.c_int, vp]
         L.tw_slab_halo.argtypes = [vp, C.c_int, C.c_int, C.c_int, C.POINTER(vp), lp, lp, lp]
@@ -231,6 +232,13 @@ class Solver:
     def exchange(self, lower: "Solver"):
         """Refresh the halo rows shared with the slab just below (tw_slab_exchange)."""
         _ok(lib().tw_slab_exchange(self.h, lower.h), "tw_slab_exchange")
+
+    @staticmethod
+    def slab_run(slabs, steps: int):
+        """Step all slabs of a grid (top to bottom) `steps` steps with the halo exchange fused into
+        the step kernel (tw_slab_run); returns after queuing."""
+        arr = (C.c_void_p * len(slabs))(*[s.h.value for s in slabs])
+        _ok(lib().tw_slab_run(arr, len(slabs), steps), "tw_slab_run")
 
     def close(self):
         if self.h:

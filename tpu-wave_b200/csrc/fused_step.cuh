@@ -175,11 +175,32 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 
 }  // namespace
 
+// the owned values of a lane's column pair (and their residual or low parts) into row pointers o, ro
+template <class S, bool EDGE, bool TWO>
+__device__ __forceinline__ void store_pair(S *o, S *ro, int c0, int c1, S h0, S h1, S l0, S l1, bool o0, bool o1)
+{
+    using V2 = typename Vec2<S>::T;
+    if (!EDGE) {
+        if (o0) {
+            *reinterpret_cast<V2 *>(o + c0) = V2{h0, h1};
+            if (TWO) *reinterpret_cast<V2 *>(ro + c0) = V2{l0, l1};
+        }
+    } else if (o0 && o1 && !(c0 & 1)) {
+        *reinterpret_cast<V2 *>(o + c0) = V2{h0, h1};
+        if (TWO) *reinterpret_cast<V2 *>(ro + c0) = V2{l0, l1};
+    } else {
+        if (o0) { o[c0] = h0; if (TWO) ro[c0] = l0; }
+        if (o1) { o[c1] = h1; if (TWO) ro[c1] = l1; }
+    }
+}
+
 // ------------------------------------------------------------------------------- interior warp
 // EDGE: the strip touches the periodic wrap or the end of a row, so lanes may have non-adjacent
 // physical columns, unowned columns or the seam; otherwise every pair is adjacent, aligned and
 // owned by the core lanes, and loads and stores are single vector accesses
-template <class S, class C, int CPST, bool ENERGY, bool EDGE, class K>
+// PUSH: the slab is linked to its neighbours (tw_slab_run) and stores its rows next to a cut into
+// their halo rows as well
+template <class S, class C, int CPST, bool ENERGY, bool EDGE, class K, bool PUSH>
 __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int it, int rcv_b, int rcv_e, EAcc &E,
                               unsigned char *ring)
 {
@@ -368,7 +389,6 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
     // the second array holds the residual (R, C codes) or the low part lo = s - hi (split)
     constexpr bool TWO = Cpst<CPST>::any;
     auto put = [&](int f, int row, const P2<C> &s, const P2<C> &r, const P2<C> &cc, bool o0, bool o1) {
-        using V2 = typename Vec2<S>::T;
         S *o = a.out[f] + row * pitch;
         S *ro = TWO ? a.rout[f] + row * pitch : nullptr;
         if ((o0 && !finite(s.a)) || (o1 && !finite(s.b))) atomicOr(a.flags, FLAG_NONFINITE);
@@ -377,17 +397,17 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
         if constexpr (SPLIT) { l0 = to_s<S>(sub(s.a, to_c<C>(h0))); l1 = to_s<S>(sub(s.b, to_c<C>(h1))); }
         if constexpr (KR) { l0 = to_s<S>(r.a); l1 = to_s<S>(r.b); }
         if constexpr (KC) { l0 = to_s<S>(cc.a); l1 = to_s<S>(cc.b); }
-        if (!EDGE) {
-            if (o0) {
-                *reinterpret_cast<V2 *>(o + c0) = V2{h0, h1};
-                if (TWO) *reinterpret_cast<V2 *>(ro + c0) = V2{l0, l1};
-            }
-        } else if (o0 && o1 && !(c0 & 1)) {
-            *reinterpret_cast<V2 *>(o + c0) = V2{h0, h1};
-            if (TWO) *reinterpret_cast<V2 *>(ro + c0) = V2{l0, l1};
-        } else {
-            if (o0) { o[c0] = h0; if (TWO) ro[c0] = l0; }
-            if (o1) { o[c1] = h1; if (TWO) ro[c1] = l1; }
+        store_pair<S, EDGE, TWO>(o, ro, c0, c1, h0, h1, l0, l1, o0, o1);
+        // a slab linked to its neighbours also stores its rows next to a cut into their halo rows
+        // (the same column layout; peer memory on another GPU is written over NVLink)
+        if constexpr (PUSH) {
+#pragma unroll
+            for (int side = 0; side < 2; side++)
+                if ((unsigned)(row - a.push_row[side]) < (unsigned)FS_HALO) {
+                    const long pr = (long)(row + a.peer_shift[side]) * pitch;
+                    store_pair<S, EDGE, TWO>(a.peer_out[side][f] + pr, TWO ? a.peer_rout[side][f] + pr : nullptr, c0, c1,
+                                             h0, h1, l0, l1, o0, o1);
+                }
         }
         if (nr > 0 || rmany) {
             if (o0) record(f, row, c0, (double)s.a);
@@ -786,7 +806,7 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
 }
 
 // ------------------------------------------------------------------------------- the launch
-template <class S, class C, int CPST, bool ENERGY, class K>
+template <class S, class C, int CPST, bool ENERGY, class K, bool PUSH = false>
 __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<C, ENERGY>()) k_elastic_fused(FusedArgs<S, C> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -801,8 +821,8 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<C, ENERGY>()) k_
             const int seg = gw / a.n_wstrip, wstrip = gw - seg * a.n_wstrip;
             const int y0 = wstrip * FS_WARP_CORE;
             unsigned char *ring = smem_raw + (threadIdx.x >> 5) * RingLayout<S, C, CPST, ENERGY, K>::warp;
-            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false, K>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
-            else interior_warp<S, C, CPST, ENERGY, true, K>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
+            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false, K, PUSH>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
+            else interior_warp<S, C, CPST, ENERGY, true, K, PUSH>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
         }
     } else {             // boundary CTA (zone, strip)
         const int b = cta;
@@ -856,7 +876,14 @@ cudaError_t set_attr(int)
     cudaError_t e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, true, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)fused_smem_bytes<S, C, N, true, K>(FS_SMALL_MX + 1));
     if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_elastic_fused<S, C, N, false, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, false, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)fused_smem_bytes<S, C, N, false, K>(FS_SMALL_MX + 1));
+    if (e != cudaSuccess || sizeof(S) != sizeof(C) || sizeof(K) != sizeof(C)) return e;
+    // the linked-slab variants (FP32 / FP64 storage)
+    e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, true, K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)fused_smem_bytes<S, C, N, true, K>(FS_SMALL_MX + 1));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_elastic_fused<S, C, N, false, K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)fused_smem_bytes<S, C, N, false, K>(FS_SMALL_MX + 1));
 }
 }  // namespace
@@ -907,6 +934,26 @@ void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, bool coef16, 
                 switch (cpst) { TW_FUSED_CASE16(0) }
             }
 #undef TW_FUSED_CASE16
+            return;
+        }
+    }
+    if constexpr (sizeof(S) == sizeof(C)) {
+        if (a.peer_out[0][0] || a.peer_out[1][0]) {   // a slab linked to its neighbours
+#define TW_FUSED_PUSH(N)                                                                                  \
+    case N:                                                                                               \
+        if (energy) k_elastic_fused<S, C, N, true, C, true><<<grid, block, fused_smem_bytes<S, C, N, true>(a.tile_rows), st>>>(a); \
+        else k_elastic_fused<S, C, N, false, C, true><<<grid, block, fused_smem_bytes<S, C, N, false>(a.tile_rows), st>>>(a);     \
+        break;
+            switch (cpst) {
+                TW_FUSED_PUSH(0)
+                TW_FUSED_PUSH(1)
+                TW_FUSED_PUSH(2)
+                TW_FUSED_PUSH(3)
+                TW_FUSED_PUSH(4)
+                TW_FUSED_PUSH(5)
+                TW_FUSED_PUSH(6)
+            }
+#undef TW_FUSED_PUSH
             return;
         }
     }

@@ -89,6 +89,7 @@ void launch_energy(const EnergyArgs<S, C> &e, cudaStream_t st);
 constexpr int FS_WARP_CORE = 56;      // 28 core lanes x 2 columns; 2 halo lanes on each side
 constexpr int FS_WARPS = TW_FS_WARPS;
 constexpr int FS_ZONE = 8;
+constexpr int FS_HALO = 4;              // a slab's halo rows at an open edge (the step's x reach)
 // both CTA kinds share the launch and its block size
 constexpr int FS_THREADS_MAX = FS_WARPS * 32;
 constexpr int FS_BND_THREADS = FS_THREADS_MAX;   // row groups of FS_BND_W threads
@@ -121,6 +122,12 @@ struct FusedArgs {
     int max_steps;
     const double *w[5];       // energy weights (ENERGY only)
     double *energy;           // [3][max_steps]: E_p0, E_k, E_p1
+    // slabs linked in one process (tw_slab_run): the neighbour above (0) / below (1) receives this
+    // slab's local rows [push_row[side], push_row[side] + FS_HALO) of every field (and residual)
+    // at its own local row + peer_shift[side]; null pointers: no neighbour
+    S *peer_out[2][5];
+    S *peer_rout[2][5];
+    int push_row[2], peer_shift[2];
     const int *rcv_off;       // receivers owned by each CTA (CSR over blockIdx.x: boundary CTAs
                               // zone-major, then interior CTAs segment-major)
     const int *rcv;           // [n][4]: field slot, row, column, trace row (2 * receiver + field)

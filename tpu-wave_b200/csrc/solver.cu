@@ -75,6 +75,7 @@ struct tw_solver {
     bool afused = false;
     bool pfuse = false;               // double-buffered periodic acoustic: may join a fused batch
     int bnd = 0;                      // BND_X_IF | BND_Y_SAT (stepper.cuh): two-launch kernels
+    tw_solver *link[2] = {};          // during tw_slab_run: the slabs above / below
     int n_rcv_list = 0;
     void *f2[5] = {}, *res2[5] = {};
     int parity = 0;                   // which buffer holds the current state (0: f/res, 1: f2/res2)
@@ -322,6 +323,18 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
     a.rcv_off = s->d_rcv_off;
     a.rcv = s->d_rcv_list;
     a.traces = s->d_traces;
+    a.push_row[0] = a.push_row[1] = -(1 << 30);
+    for (int side = 0; side < 2; side++) {
+        const tw_solver *p = s->link[side];
+        if (!p) continue;
+        // the neighbour steps in lockstep: its output buffer of this step has our parity
+        for (int k = 0; k < 5; k++) {
+            a.peer_out[side][k] = (S *)(s->parity ? p->f[k] : p->f2[k]);
+            a.peer_rout[side][k] = (S *)(s->parity ? p->res[k] : p->res2[k]);
+        }
+        a.push_row[side] = (int)(side == 0 ? s->own0 - s->row_off : s->own1 - s->row_off - FS_HALO);
+        a.peer_shift[side] = (int)(s->row_off - p->row_off);
+    }
     launch_fused<S, C>(a, s->d.cpst, s->d.energy != 0, s->d.coef_fp16 != 0, st);
 }
 
@@ -1232,6 +1245,87 @@ int tw_slab_exchange(tw_solver *up, tw_solver *lo)
     }
     TW_CUDA(cudaStreamSynchronize(up->st));
     return TW_OK;
+}
+
+int tw_slab_run(tw_solver *const *slabs, int n, int steps)
+{
+    if (!slabs || n < 1 || steps < 0) return TW_ERR_INVALID;
+    for (int i = 0; i < n; i++) {
+        tw_solver *s = slabs[i];
+        if (check(s) || !s->slab || !s->fused || !s->mat_ready) return check(s) ? TW_ERR_INVALID : TW_ERR_STATE;
+        // the linked step kernels exist for FP32 / FP64 storage and coefficients
+        if (s->d.precision == TW_BF16 || s->d.precision == TW_FP16 || s->d.coef_fp16) return TW_ERR_UNSUPPORTED;
+        if (s->steps_done + (long)steps > s->d.max_steps) return TW_ERR_RECORD_FULL;
+        const tw_solver *t = slabs[0];
+        if (s->Mx_glob != t->Mx_glob || s->d.My != t->d.My || s->d.precision != t->d.precision ||
+            s->d.cpst != t->d.cpst || s->steps_done != t->steps_done || s->parity != t->parity)
+            return TW_ERR_INVALID;
+        if (i > 0 && slabs[i - 1]->own1 != s->own0) return TW_ERR_INVALID;   // consecutive slabs, top to bottom
+    }
+    if (slabs[0]->own0 != 0 || slabs[n - 1]->own1 != slabs[0]->Mx_glob) return TW_ERR_INVALID;   // the whole grid
+    // neighbours on other GPUs are written through peer access (NVLink)
+    for (int i = 0; i + 1 < n; i++) {
+        const int d0 = slabs[i]->d.device, d1 = slabs[i + 1]->d.device;
+        if (d0 == d1) continue;
+        int ok01 = 0, ok10 = 0;
+        TW_CUDA(cudaDeviceCanAccessPeer(&ok01, d0, d1));
+        TW_CUDA(cudaDeviceCanAccessPeer(&ok10, d1, d0));
+        if (!ok01 || !ok10) return TW_ERR_UNSUPPORTED;
+        for (int q = 0; q < 2; q++) {
+            TW_CUDA(cudaSetDevice(q ? d1 : d0));
+            const cudaError_t e = cudaDeviceEnablePeerAccess(q ? d0 : d1, 0);
+            if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+            else if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceEnablePeerAccess");
+        }
+    }
+    std::vector<cudaEvent_t> ev(n, nullptr);
+    int rc = TW_OK;
+    for (int i = 0; i < n && rc == TW_OK; i++) {
+        cudaSetDevice(slabs[i]->d.device);
+        if (cudaEventCreateWithFlags(&ev[i], cudaEventDisableTiming) != cudaSuccess) rc = TW_ERR_CUDA;
+    }
+    for (int i = 0; i < n; i++) {
+        slabs[i]->link[0] = i > 0 ? slabs[i - 1] : nullptr;
+        slabs[i]->link[1] = i + 1 < n ? slabs[i + 1] : nullptr;
+    }
+    // step k of a slab writes its cut rows into the neighbours' output buffers of step k, which
+    // their step k - 1 read as input: it starts after the neighbours' step k - 1 (and its own)
+    for (int k = 0; k < steps && rc == TW_OK; k++) {
+        for (int i = 0; i < n && rc == TW_OK; i++) {
+            tw_solver *s = slabs[i];
+            cudaSetDevice(s->d.device);
+            if (k > 0) {
+                if (i > 0 && cudaStreamWaitEvent(s->st, ev[i - 1], 0) != cudaSuccess) rc = TW_ERR_CUDA;
+                if (i + 1 < n && cudaStreamWaitEvent(s->st, ev[i + 1], 0) != cudaSuccess) rc = TW_ERR_CUDA;
+            } else {   // the first step waits for whatever the neighbours had queued before
+                for (int q : {i - 1, i + 1})
+                    if (q >= 0 && q < n && (cudaEventRecord(ev[q], slabs[q]->st) != cudaSuccess ||
+                                            cudaStreamWaitEvent(s->st, ev[q], 0) != cudaSuccess))
+                        rc = TW_ERR_CUDA;
+            }
+        }
+        for (int i = 0; i < n && rc == TW_OK; i++) {
+            tw_solver *s = slabs[i];
+            cudaSetDevice(s->d.device);
+            enqueue(s, 1, s->st);
+            if (cudaEventRecord(ev[i], s->st) != cudaSuccess) rc = TW_ERR_CUDA;
+        }
+        if (rc == TW_OK)
+            for (int i = 0; i < n; i++) slabs[i]->steps_done += 1;
+    }
+    for (int i = 0; i < n; i++) {
+        slabs[i]->link[0] = slabs[i]->link[1] = nullptr;
+        cudaSetDevice(slabs[i]->d.device);
+        if (ev[i]) cudaEventDestroy(ev[i]);
+    }
+    if (rc == TW_OK) {
+        for (int i = 0; i < n; i++) {
+            cudaSetDevice(slabs[i]->d.device);
+            const cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return cuda_fail(e, "tw_slab_run");
+        }
+    }
+    return rc;
 }
 
 int tw_data_misfit(tw_solver *s, const double *obs, double *total, double *per_rcv)
