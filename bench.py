@@ -38,6 +38,10 @@ shots along row 16, 256 receivers on NM row 4; observed traces from the layered 
 Gaussian anomaly, gradient of the misfit with respect to rho, vp, vs of the layered medium,
 checkpoints every 50 steps; checked against central differences (h = 1e-3) along 8 random
 directions and by the dot-product identity of the state map (FP64).
+
+`--workload variants` times the boundary variants on the elastic 2048 x 2048 FP32 workload: the x
+ends joined by the SAT interface, free surfaces on all four sides, and both, beside the
+reference's configuration.
 """
 from __future__ import annotations
 
@@ -757,6 +761,47 @@ def run_adjoint(args):
     print(json.dumps(line), flush=True)
 
 
+def run_variants(args):
+    """The boundary variants on the elastic 2048^2 FP32 workload: the x ends joined by the SAT
+    interface, free surfaces on all four sides, both; against the reference's configuration."""
+    import torch
+    tw = load_twave()
+    torch.cuda.set_device(0)
+    rho, vp, vs, dt, (sx, sy) = build_model(0)
+    rx, ry = receivers()
+    K = args.steps
+    peak, peak_note = measured_peaks()
+    out = {}
+    for name, bc, sat_y in (("free_x_periodic_y", tw.SAT_FREE, False), ("interface_x", tw.SAT_INTERFACE, False),
+                            ("free_all_sides", tw.SAT_FREE, True), ("interface_x_free_y", tw.SAT_INTERFACE, True)):
+        s = tw.Solver(MX, MY, 1, DEN_DX, dt, physics=tw.ELASTIC, precision="f32", cpst="00", central_f=F0,
+                      time_delay=DELAY, max_steps=args.warmup + K, energy=False, bc_x=bc, sat_y=sat_y)
+        s.set_material_model(rho, vp, vs)
+        s.set_source(tw.MM, sx, sy)
+        s.add_receivers(tw.NM, rx, ry)
+        stream = torch.cuda.ExternalStream(s.stream())
+        s.run(args.warmup)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        s.step(K)
+        e1.record(stream)
+        s.sync()
+        ms = e0.elapsed_time(e1)
+        s.close()
+        gpts = MX * MY * K / (ms / 1e3) / 1e9
+        out[name] = {"gpts": gpts, "ms_per_step": ms / K, "hbm_frac_at_60B": gpts * 60 / peak,
+                     "kernels": "fused step" if (bc == tw.SAT_FREE and not sat_y) else "two launches per step"}
+    line = {"metric": METRIC, "value": out["free_all_sides"]["gpts"], "unit": UNIT, "n_gpus": 1, "steps": K,
+            "warmup": args.warmup, "ms_per_step": out["free_all_sides"]["ms_per_step"], "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "boundary variants of the elastic 2048x2048 FP32 workload (energy off); value: free "
+                                   "surfaces on all four sides", "peak": f"{peak} GB/s {peak_note}",
+                       "l2": "inputs larger than L2, no flush"},
+            "variants": out}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
@@ -765,7 +810,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--cpu-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", choices=["elastic2048", "acoustic512", "mixed", "batch", "adjoint"],
+    ap.add_argument("--workload", choices=["elastic2048", "acoustic512", "mixed", "batch", "adjoint", "variants"],
                     default="elastic2048")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -774,10 +819,10 @@ def main():
     if args.impl == "reference":
         run_reference_arm(args, dist)
         return
-    if args.workload in ("acoustic512", "mixed", "batch", "adjoint"):
+    if args.workload in ("acoustic512", "mixed", "batch", "adjoint", "variants"):
         if dist.rank == 0:
             {"acoustic512": run_acoustic512, "mixed": run_mixed, "batch": run_batch,
-             "adjoint": run_adjoint}[args.workload](args)
+             "adjoint": run_adjoint, "variants": run_variants}[args.workload](args)
         return
     run_ours(args, dist)
 
