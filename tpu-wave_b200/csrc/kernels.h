@@ -81,7 +81,7 @@ void launch_energy(const EnergyArgs<S, C> &e, cudaStream_t st);
 #define TW_FS_CTAS_PER_SM 60          // CTAs per SM the elastic row segmentation aims at (12 waves)
 #endif
 #ifndef TW_AC_CTAS_PER_SM
-#define TW_AC_CTAS_PER_SM 15          // the same for the fused acoustic step and batches
+#define TW_AC_CTAS_PER_SM 32          // the same for the fused acoustic step and batches
 #endif
 #ifndef TW_FS_RING
 #define TW_FS_RING 3                  // rows staged ahead per interior warp (FP64: 2)

@@ -1969,7 +1969,7 @@ int tw_batch_tune(tw_batch *b, int steps, double *best_ms)
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     std::vector<BatchShape> cand;
     if (b->fused) {   // fused batches: the CTAs-per-SM target of the segmentation
-        for (int per_sm : {2, 4, 8, 15, 24, 32}) cand.push_back(BatchShape{0, 0, 0, per_sm});
+        for (int per_sm : {2, 4, 8, 15, 24, 32, 48, 64}) cand.push_back(BatchShape{0, 0, 0, per_sm});
     } else {
         for (int tx : {32, 64, 128, 256})
             for (int rpt : {1, 2, 4})
