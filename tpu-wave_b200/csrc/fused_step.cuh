@@ -636,7 +636,8 @@ __device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int
 }
 
 // ------------------------------------------------------------------------------- boundary CTA
-template <class S, class C, int CPST, bool ENERGY, class K>
+// XIF: the x ends joined by the SAT interface (zone kind 3, or 2 on a small grid)
+template <class S, class C, int CPST, bool ENERGY, class K, bool XIF>
 __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int it, int rcv_b, int rcv_e, C *tile,
                              EAcc &E)
 {
@@ -651,12 +652,23 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
     const bool core = t >= 4 && t < 4 + FS_BND_TY;
     const bool ownN = core && c <= My, ownM = core && c < My;
     const bool velT = t >= 2 && t < NT - 2;
-    int zr0, zr1;   // zone rows (N-type grids up to zr1, M-type up to min(zr1, Mx - 1))
+    // zone rows zr0[p]..zr1[p] (N-type grids up to zr1, M-type up to min(zr1, Mx - 1)) of one part,
+    // or of two (kind 3: the top and the bottom zone in one CTA, when the SAT interface couples
+    // the two x ends); velocity rows vr0[p]..vr1[p], stored in the tile from row toff[p]
+    int np = 1, zr0[2] = {0, 0}, zr1[2] = {0, 0};
     const int kind = a.zone_kind[zone];
-    if (kind == 2) { zr0 = 0; zr1 = Mx; }
-    else if (kind == 0) { zr0 = 0; zr1 = FS_ZONE - 1; }
-    else { zr0 = Mx - FS_ZONE; zr1 = Mx; }
-    const int vr0 = max(zr0 - 2, 0), vr1 = min(zr1 + 2, Mx);
+    if (kind == 2) { zr0[0] = 0; zr1[0] = Mx; }
+    else if (kind == 0) { zr0[0] = 0; zr1[0] = FS_ZONE - 1; }
+    else if (kind == 1 || !XIF) { zr0[0] = Mx - FS_ZONE; zr1[0] = Mx; }
+    else { np = 2; zr0[0] = 0; zr1[0] = FS_ZONE - 1; zr0[1] = Mx - FS_ZONE; zr1[1] = Mx; }
+    if constexpr (!XIF) np = 1;
+    int vr0[2], vr1[2], toff[2] = {0, 0};
+    for (int p = 0; p < np; p++) {
+        vr0[p] = max(zr0[p] - 2, 0);
+        vr1[p] = min(zr1[p] + 2, Mx);
+    }
+    if (np == 2) toff[1] = vr1[0] - vr0[0] + 1;
+    auto tr = [&](int j) { return (XIF && np == 2 && j >= vr0[1]) ? toff[1] + j - vr0[1] : j - vr0[0]; };
     C *tMN = tile, *tNM = tile + a.tile_rows * NT;
 
     bool mine = false;   // does any receiver of the CTA sit in this thread's column
@@ -691,15 +703,18 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
 
     // phase 1: velocities of rows vr0..vr1 at every velocity column (physical reads)
     if (velT) {
-        for (int j = vr0 + g; j <= vr1; j += RG) {
-            const bool ownRow = j >= zr0 && j <= zr1;
+        for (int p = 0; p < np; p++)
+        for (int j = vr0[p] + g; j <= vr1[p]; j += RG) {
+            const bool ownRow = j >= zr0[p] && j <= zr1[p];
             if (j < Mx) {   // MN
                 C r, cc;
                 ldr(F_MN, j, pN, r, cc);
                 const C P = ld<C>(reinterpret_cast<const K *>(a.coef[F_MN]), (long)j * pitch + pN);
                 C v = dx_from_N<C>(a.op, FA(F_NN), pitch, Mx, j, pN);
                 r = add(r, mul(v, P));
-                if (sat_MN<C>(a.op, FA(F_NN), pitch, Mx, j, pN, v)) r = add(r, mul(v, P));
+                const bool sx = XIF ? satM_if<C>(a.op, Mx, j, [&](int q) { return ld<C>(FA(F_NN), (long)q * pitch + pN); }, v)
+                                      : sat_MN<C>(a.op, FA(F_NN), pitch, Mx, j, pN, v);
+                if (sx) r = add(r, mul(v, P));
                 v = dy_periodic<false, C>(a.op, FA(F_MM1) + (long)j * pitch, My, pN);
                 r = add(r, mul(v, P));
                 C s = ld<C>(FA(F_MN), (long)j * pitch + pN);
@@ -707,7 +722,7 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
                 if (a.src_grid == G_MN && j == a.src_ix)
                     if (pN == a.src_iy) s = to_s<C>(add((double)s, a.src_inc[it]));
                 s = quant<S, C, CPST>(s);
-                tMN[(j - vr0) * NT + t] = s;
+                tMN[tr(j) * NT + t] = s;
                 if (ownRow && ownN) {
                     put(F_MN, j, s, r, cc);
                     if (ENERGY) E.k = add(E.k, mul(mul((double)s, __ldg(a.w[F_MN] + (long)j * pitch + c)), (double)s));
@@ -719,7 +734,9 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
                 const C P = ld<C>(reinterpret_cast<const K *>(a.coef[F_NM]), (long)j * pitch + pM);
                 C v = dx_from_M<C>(a.op, FA(F_MM0), pitch, Mx, j, pM);
                 r = add(r, mul(v, P));
-                if (sat_NM<C>(a.op, FA(F_MM0), pitch, Mx, j, pM, v)) r = add(r, mul(v, P));
+                const bool sx = XIF ? satN_if<C>(a.op, Mx, j, [&](int q) { return ld<C>(FA(F_MM0), (long)q * pitch + pM); }, v)
+                                      : sat_NM<C>(a.op, FA(F_MM0), pitch, Mx, j, pM, v);
+                if (sx) r = add(r, mul(v, P));
                 v = dy_periodic<true, C>(a.op, FA(F_NN) + (long)j * pitch, My, pM);
                 r = add(r, mul(v, P));
                 C s = ld<C>(FA(F_NM), (long)j * pitch + pM);
@@ -727,7 +744,7 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
                 if (a.src_grid == G_NM && j == a.src_ix)
                     if (pM == a.src_iy) s = to_s<C>(add((double)s, a.src_inc[it]));
                 s = quant<S, C, CPST>(s);
-                tNM[(j - vr0) * NT + t] = s;
+                tNM[tr(j) * NT + t] = s;
                 if (ownRow && ownM) {
                     put(F_NM, j, s, r, cc);
                     if (ENERGY) E.k = add(E.k, mul(mul((double)s, __ldg(a.w[F_NM] + (long)j * pitch + c)), (double)s));
@@ -738,17 +755,19 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
     __syncthreads();
     // phase 2: stresses of the zone rows from the velocity tile
     if (core) {
-        for (int i = zr0 + g; i <= zr1; i += RG) {
+        for (int p = 0; p < np; p++)
+        for (int i = zr0[p] + g; i <= zr1[p]; i += RG) {
             const long o = (long)i * pitch + c;
             if (ownN) {   // NN
                 C r, cc;
                 ldr(F_NN, i, c, r, cc);
                 const C P = ld<C>(reinterpret_cast<const K *>(a.coef[F_NN]), o);
-                C v = dxM<C>(a.op, Mx, i, [&](int rr) { return tMN[(rr - vr0) * NT + t]; });
+                C v = dxM<C>(a.op, Mx, i, [&](int rr) { return tMN[tr(rr) * NT + t]; });
                 r = add(r, mul(v, P));
+                if (XIF && satN_if<C>(a.op, Mx, i, [&](int q) { return tMN[tr(q) * NT + t]; }, v)) r = add(r, mul(v, P));
                 v = C(0);
 #pragma unroll
-                for (int w = 0; w < 4; w++) v = add(v, mul(tNM[(i - vr0) * NT + t - 2 + w], a.op.st[w]));
+                for (int w = 0; w < 4; w++) v = add(v, mul(tNM[tr(i) * NT + t - 2 + w], a.op.st[w]));
                 r = add(r, mul(v, P));
                 const C old = ld<C>(FA(F_NN), o);
                 C s = old;
@@ -769,13 +788,18 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
                 ldr(F_MM1, i, c, r1, k1);
                 const C L = ld<C>(reinterpret_cast<const K *>(a.coef[F_MM0]), o),
                         M2 = ld<C>(reinterpret_cast<const K *>(a.coef[F_MM1]), o);
-                C v = dxN<C>(a.op, Mx, i, [&](int rr) { return tNM[(rr - vr0) * NT + t]; });
+                C v = dxN<C>(a.op, Mx, i, [&](int rr) { return tNM[tr(rr) * NT + t]; });
                 r0 = add(r0, mul(v, L));
                 r1 = add(r1, mul(v, L));
                 r0 = add(r0, mul(v, M2));
+                if (XIF && satM_if<C>(a.op, Mx, i, [&](int q) { return tNM[tr(q) * NT + t]; }, v)) {
+                    r0 = add(r0, mul(v, L));
+                    r1 = add(r1, mul(v, L));
+                    r0 = add(r0, mul(v, M2));
+                }
                 v = C(0);
 #pragma unroll
-                for (int w = 0; w < 4; w++) v = add(v, mul(tMN[(i - vr0) * NT + t - 1 + w], a.op.st[w]));
+                for (int w = 0; w < 4; w++) v = add(v, mul(tMN[tr(i) * NT + t - 1 + w], a.op.st[w]));
                 r0 = add(r0, mul(v, L));
                 r1 = add(r1, mul(v, L));
                 r1 = add(r1, mul(v, M2));
@@ -806,7 +830,9 @@ __device__ void boundary_cta(const FusedArgs<S, C> &a, int bstrip, int zone, int
 }
 
 // ------------------------------------------------------------------------------- the launch
-template <class S, class C, int CPST, bool ENERGY, class K, bool PUSH = false>
+// MODE 0: a handle of its own; 1: a slab linked to its neighbours (tw_slab_run); 2: the x ends
+// joined by the SAT interface
+template <class S, class C, int CPST, bool ENERGY, class K, int MODE = 0>
 __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<C, ENERGY>()) k_elastic_fused(FusedArgs<S, C> a)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -821,12 +847,12 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<C, ENERGY>()) k_
             const int seg = gw / a.n_wstrip, wstrip = gw - seg * a.n_wstrip;
             const int y0 = wstrip * FS_WARP_CORE;
             unsigned char *ring = smem_raw + (threadIdx.x >> 5) * RingLayout<S, C, CPST, ENERGY, K>::warp;
-            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false, K, PUSH>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
-            else interior_warp<S, C, CPST, ENERGY, true, K, PUSH>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
+            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false, K, MODE == 1>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
+            else interior_warp<S, C, CPST, ENERGY, true, K, MODE == 1>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
         }
     } else {             // boundary CTA (zone, strip)
         const int b = cta;
-        boundary_cta<S, C, CPST, ENERGY, K>(a, b % a.n_bstrip, b / a.n_bstrip, it, rcv_b, rcv_e,
+        boundary_cta<S, C, CPST, ENERGY, K, MODE == 2>(a, b % a.n_bstrip, b / a.n_bstrip, it, rcv_b, rcv_e,
                                          reinterpret_cast<C *>(smem_raw), E);
     }
     if (ENERGY) {
@@ -879,12 +905,13 @@ cudaError_t set_attr(int)
     e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, false, K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)fused_smem_bytes<S, C, N, false, K>(FS_SMALL_MX + 1));
     if (e != cudaSuccess || sizeof(S) != sizeof(C) || sizeof(K) != sizeof(C)) return e;
-    // the linked-slab variants (FP32 / FP64 storage)
-    e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, true, K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)fused_smem_bytes<S, C, N, true, K>(FS_SMALL_MX + 1));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_elastic_fused<S, C, N, false, K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)fused_smem_bytes<S, C, N, false, K>(FS_SMALL_MX + 1));
+    // the linked-slab and SAT-interface variants (FP32 / FP64 storage)
+    const int big = (int)fused_smem_bytes<S, C, N, true, K>(FS_SMALL_MX + 1), small = (int)fused_smem_bytes<S, C, N, false, K>(FS_SMALL_MX + 1);
+    if ((e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, true, K, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, big)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, false, K, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, small)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(k_elastic_fused<S, C, N, true, K, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, big)) != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute(k_elastic_fused<S, C, N, false, K, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, small);
 }
 }  // namespace
 
@@ -938,22 +965,29 @@ void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, bool coef16, 
         }
     }
     if constexpr (sizeof(S) == sizeof(C)) {
-        if (a.peer_out[0][0] || a.peer_out[1][0]) {   // a slab linked to its neighbours
-#define TW_FUSED_PUSH(N)                                                                                  \
+        // a slab linked to its neighbours (mode 1), or the x ends joined by the SAT interface (2)
+        const int mode = a.xif ? 2 : ((a.peer_out[0][0] || a.peer_out[1][0]) ? 1 : 0);
+        if (mode) {
+#define TW_FUSED_MODE(N)                                                                                  \
     case N:                                                                                               \
-        if (energy) k_elastic_fused<S, C, N, true, C, true><<<grid, block, fused_smem_bytes<S, C, N, true>(a.tile_rows), st>>>(a); \
-        else k_elastic_fused<S, C, N, false, C, true><<<grid, block, fused_smem_bytes<S, C, N, false>(a.tile_rows), st>>>(a);     \
+        if (mode == 1) {                                                                                  \
+            if (energy) k_elastic_fused<S, C, N, true, C, 1><<<grid, block, fused_smem_bytes<S, C, N, true>(a.tile_rows), st>>>(a); \
+            else k_elastic_fused<S, C, N, false, C, 1><<<grid, block, fused_smem_bytes<S, C, N, false>(a.tile_rows), st>>>(a);     \
+        } else {                                                                                          \
+            if (energy) k_elastic_fused<S, C, N, true, C, 2><<<grid, block, fused_smem_bytes<S, C, N, true>(a.tile_rows), st>>>(a); \
+            else k_elastic_fused<S, C, N, false, C, 2><<<grid, block, fused_smem_bytes<S, C, N, false>(a.tile_rows), st>>>(a);     \
+        }                                                                                                 \
         break;
             switch (cpst) {
-                TW_FUSED_PUSH(0)
-                TW_FUSED_PUSH(1)
-                TW_FUSED_PUSH(2)
-                TW_FUSED_PUSH(3)
-                TW_FUSED_PUSH(4)
-                TW_FUSED_PUSH(5)
-                TW_FUSED_PUSH(6)
+                TW_FUSED_MODE(0)
+                TW_FUSED_MODE(1)
+                TW_FUSED_MODE(2)
+                TW_FUSED_MODE(3)
+                TW_FUSED_MODE(4)
+                TW_FUSED_MODE(5)
+                TW_FUSED_MODE(6)
             }
-#undef TW_FUSED_PUSH
+#undef TW_FUSED_MODE
             return;
         }
     }

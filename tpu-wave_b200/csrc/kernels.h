@@ -110,7 +110,9 @@ struct FusedArgs {
     int n_int_seg, int_rows;  // interior rows [ir0, ir0 + int_rows), in n_int_seg balanced segments
     int ir0;                  // FS_ZONE below a free surface; the halo depth below an open slab edge
     int n_zone;               // boundary zones: 0, 1 or 2, of the kinds zone_kind[]
-    int zone_kind[2];         // 0: the FS_ZONE rows at the top free surface, 1: at the bottom, 2: the whole grid
+    int zone_kind[2];         // 0: the FS_ZONE rows at the top free surface, 1: at the bottom, 2: the whole grid,
+                              // 3: both ends in one CTA (the x ends joined by the SAT interface)
+    int xif;                  // the x ends joined by the SAT interface (boundary CTAs only)
     int n_wstrip, n_bstrip;   // interior warp strips, boundary strips
     int n_int_cta;            // interior CTAs: the n_int_seg x n_wstrip warps, FS_WARPS per CTA
     int tile_rows;

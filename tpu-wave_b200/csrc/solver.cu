@@ -307,6 +307,7 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
     a.n_zone = s->n_zone;
     a.zone_kind[0] = s->zone_kind[0];
     a.zone_kind[1] = s->zone_kind[1];
+    a.xif = (s->bnd & BND_X_IF) ? 1 : 0;
     a.n_wstrip = s->n_wstrip;
     a.n_bstrip = s->n_bstrip;
     a.n_int_cta = s->n_int_cta;
@@ -498,7 +499,7 @@ int upload_receivers(tw_solver *s)
             int zone = -1;            // the boundary zone holding the row, if any
             for (int z = 0; z < s->n_zone; z++) {
                 const int k = s->zone_kind[z];
-                if (k == 2 || (k == 0 && row < FS_ZONE) || (k == 1 && row >= Mx - FS_ZONE)) zone = z;
+                if (k == 2 || ((k == 0 || k == 3) && row < FS_ZONE) || ((k == 1 || k == 3) && row >= Mx - FS_ZONE)) zone = z;
             }
             int cta;
             if (zone >= 0) {
@@ -756,7 +757,7 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
         cudaMemsetAsync(s->coef[k], 0, n * csz, s->st);
         cudaMemsetAsync(s->w[k], 0, n * sizeof(double), s->st);
     }
-    if (s->elastic && !s->bnd) {
+    if (s->elastic && !(s->bnd & BND_Y_SAT)) {
         // fused elastic path: a second copy of the state and the strip x segment geometry
         s->fused = true;
         switch (d.precision) {
@@ -789,9 +790,14 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             // at an open edge its interior reaches the four halo rows.
             const bool top = s->row_off == 0, bot = s->row_off + Mx == s->Mx_glob;
             s->n_zone = 0;
-            if (top) s->zone_kind[s->n_zone++] = 0;
-            if (bot) s->zone_kind[s->n_zone++] = 1;
-            s->tile_rows = 12;
+            if (s->bnd & BND_X_IF) {   // the interface couples the ends: both zones in one CTA
+                s->zone_kind[s->n_zone++] = 3;
+                s->tile_rows = 2 * (FS_ZONE + 2) + 1;
+            } else {
+                if (top) s->zone_kind[s->n_zone++] = 0;
+                if (bot) s->zone_kind[s->n_zone++] = 1;
+                s->tile_rows = 12;
+            }
             s->ir0 = top ? FS_ZONE : 4;
             s->int_rows = (int)Mx - (bot ? FS_ZONE : 4) - s->ir0;
             if (s->int_rows < 8) return fail(TW_ERR_INVALID);
