@@ -791,7 +791,8 @@ def run_variants(args):
         s.close()
         gpts = MX * MY * K / (ms / 1e3) / 1e9
         out[name] = {"gpts": gpts, "ms_per_step": ms / K, "hbm_frac_at_60B": gpts * 60 / peak,
-                     "kernels": "two launches per step" if sat_y else "fused step"}
+                     "kernels": "fused step, then the points next to the y ends recomputed (two launches)"
+                                if sat_y else "fused step"}
     line = {"metric": METRIC, "value": out["free_all_sides"]["gpts"], "unit": UNIT, "n_gpus": 1, "steps": K,
             "warmup": args.warmup, "ms_per_step": out["free_all_sides"]["ms_per_step"], "higher_is_better": True,
             "dtype": "f32", "data": "synthetic",

@@ -4,7 +4,9 @@
   boundary type other than 'F', grid_drvt.tpp:575-693): bit-identical to the reference's own
   solver (golden fixtures `*_if_*`, in test_parity_gpu.py) and to the restatement here;
 * free surfaces on all four sides (no reference run): bit-identical to the restatement, whose
-  y operators the transposition test of test_boundary_variants_cpu.py holds to the x ones.
+  y operators the transposition test of test_boundary_variants_cpu.py holds to the x ones; from
+  16 columns on they run on the fused step with the points next to the y ends recomputed, below
+  on the two-launch kernels, and the sizes here cover both (and strips of several warps).
 
 Energies are FP64 sums taken in a different order: relative tolerance 1e-12.
 """
@@ -23,7 +25,7 @@ MODES = [("I", False), ("F", True), ("I", True)]
 @pytest.mark.parametrize("bc,sat_y", MODES)
 @pytest.mark.parametrize("cpst", CPST_CODES)
 @pytest.mark.parametrize("prec", ["f64", "f32"])
-@pytest.mark.parametrize("Mx,My", [(24, 40), (37, 9), (8, 8)])
+@pytest.mark.parametrize("Mx,My", [(24, 40), (37, 9), (8, 8), (30, 117)])
 def test_elastic_variant_random_state_matches_oracle(bc, sat_y, cpst, prec, Mx, My):
     case = elastic_case(Mx, My, seed=Mx * My + 1, cpst=cpst, Nt=3, rcvs=[])
     case.bc_x, case.sat_y = bc, sat_y

@@ -138,6 +138,36 @@ struct FusedArgs {
 template <class S, class C>
 void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, bool coef16, cudaStream_t st);
 
+// free y ends on the fused step (ysat_fix.cu): the fused kernel steps every column with the
+// periodic y rule; these two launches then recompute, from the step's input buffers, the points
+// whose y stencils meet an end (velocities, then the stresses that read them), with the SBP
+// closures and penalties along y, overwriting the output buffers, and correct the step's energy
+// records and the traces of receivers there
+template <class S, class C>
+struct YFixArgs {
+    const S *in[5];
+    S *out[5];
+    const S *rin[5];
+    S *rout[5];
+    const C *coef[5];
+    long pitch;
+    int Mx, My;
+    Ops<C> op;
+    int xif;                  // the x ends joined by the SAT interface
+    const double *src_inc;
+    int src_grid, src_ix, src_iy;
+    const int *step;          // advanced by the fused kernel: this step is *step - 1
+    int *flags;
+    int max_steps;
+    const double *w[5];       // energy weights (energy on), else null
+    double *energy;
+    const int *rcv;           // the flat receiver table (field slots, row, column)
+    int n_rcv;
+    double *traces;
+};
+template <class S, class C>
+void launch_ysat_fix(const YFixArgs<S, C> &a, int cpst, cudaStream_t st);
+
 // fused periodic acoustic step (acoustic_fused.cu): one shot, or a batch of shots in one launch
 template <class S, class C>
 struct AcShot {

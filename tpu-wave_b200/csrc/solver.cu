@@ -346,6 +346,36 @@ void enqueue_fused_step(tw_solver *s, cudaStream_t st)
     void **fin = s->parity ? s->f2 : s->f, **fout = s->parity ? s->f : s->f2;
     void **rin = s->parity ? s->res2 : s->res, **rout = s->parity ? s->res : s->res2;
     enqueue_fused_io<S, C>(s, fin, fout, rin, rout, st);
+    if constexpr (sizeof(S) == sizeof(C)) {
+        if (s->bnd & BND_Y_SAT) {   // free y ends: recompute the points next to them (ysat_fix.cu)
+            YFixArgs<S, C> y{};
+            for (int k = 0; k < 5; k++) {
+                y.in[k] = (const S *)fin[k];
+                y.out[k] = (S *)fout[k];
+                y.rin[k] = (const S *)rin[k];
+                y.rout[k] = (S *)rout[k];
+                y.coef[k] = (const C *)s->coef[k];
+                y.w[k] = s->w[k];
+            }
+            y.pitch = s->pitch;
+            y.Mx = (int)s->d.Mx;
+            y.My = (int)s->d.My;
+            y.op = make_ops<C>((double)s->d.num_dx / (double)s->d.den_dx, s->d.dt, false);
+            y.xif = (s->bnd & BND_X_IF) ? 1 : 0;
+            y.src_inc = s->src_inc;
+            y.src_grid = s->src_grid;
+            y.src_ix = (int)s->src_ix;
+            y.src_iy = (int)s->src_iy;
+            y.step = s->d_step;
+            y.flags = s->d_flags;
+            y.max_steps = s->d.max_steps;
+            y.energy = s->d.energy ? s->d_energy : nullptr;
+            y.rcv = s->d_rcv;
+            y.n_rcv = (int)(s->rcv_tab.size() / 4);
+            y.traces = s->d_traces;
+            launch_ysat_fix<S, C>(y, s->d.cpst, st);
+        }
+    }
     s->parity ^= 1;
 }
 
@@ -757,8 +787,10 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
         cudaMemsetAsync(s->coef[k], 0, n * csz, s->st);
         cudaMemsetAsync(s->w[k], 0, n * sizeof(double), s->st);
     }
-    if (s->elastic && !(s->bnd & BND_Y_SAT)) {
-        // fused elastic path: a second copy of the state and the strip x segment geometry
+    if (s->elastic && (!(s->bnd & BND_Y_SAT) || My >= 16)) {
+        // fused elastic path: a second copy of the state and the strip x segment geometry (free
+        // y ends: the fused step plus the recomputation of the columns next to them, which stay
+        // apart from 16 columns on)
         s->fused = true;
         switch (d.precision) {
         case TW_FP64: e = prepare_fused<double, double>(); break;
