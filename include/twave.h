@@ -91,8 +91,8 @@ typedef struct {
     int sat_y;              /* 1: SBP-SAT free surfaces on the two y ends too (all four sides free with
                                bc_x TW_BC_SAT_FREE): closures and penalties along y with the x tables,
                                energy norm along y as along x; no reference run (its y is periodic).
-                               0: periodic y (the reference). sat_y and TW_BC_SAT_INTERFACE step with
-                               the two-launch FP64/FP32 kernels; My >= 8 with sat_y */
+                               0: periodic y (the reference). sat_y and TW_BC_SAT_INTERFACE need
+                               FP64/FP32 storage; My >= 8 with sat_y */
 } tw_grid_desc;
 
 typedef struct {
