@@ -24,7 +24,9 @@
 //       8 den_dxM, 9 Nt, 10 cpst_N, 11 cpst_S (char code), 12 src_type_x, 13 src_type_y,
 //       14..17 src num_x, den_x, num_y, den_y, 18 n_rcv, 19 quiet,
 //       20 boundary type of both x ends (0 = 'F'; another letter selects the reference's
-//          SAT interface branch of secure_bdry, grid_drvt.tpp:575-693)
+//          SAT interface branch of secure_bdry, grid_drvt.tpp:575-693),
+//       21 untimed warm-up passes: the whole run of Nt steps is made this many times from rest
+//          before the timed pass (the outputs are those of the timed pass, identical to them)
 //   dh: 0 dt, 1 central_f, 2 time_delay
 //   P = (Mx_prmt + 2) * (My_prmt + 2)  (the reference's padded model layout, inverse.cpp:79-90)
 // Output file: float64 loop_seconds; E_k[Nt]; E_p0[Nt]; E_p1[Nt]; traces[n_rcv][2][Nt];
@@ -186,18 +188,20 @@ int main(int argc, char **argv)
     }
     Fwd_Specs.process_rcv_locations(rcv_in);
 
-    for (auto &g : Grids)
-        for (int f = 0; f < g.N_soln; f++) g.Vec_soln.at(f).set_constant(0.);
-    Record_E_k.set_constant(0.);
-    Record_E_p0.set_constant(0.);
-    Record_E_p1.set_constant(0.);
-
     double loop_seconds = 0.0;
-    if (Nt > 0) {
-        auto t0 = std::chrono::steady_clock::now();
-        if (!dispatch_cpst(Fwd_Specs, cpst_N, cpst_S)) { std::fprintf(stderr, "bad cpst\n"); return 2; }
-        auto t1 = std::chrono::steady_clock::now();
-        loop_seconds = std::chrono::duration<double>(t1 - t0).count();
+    const int64_t passes = 1 + (ih[21] > 0 ? ih[21] : 0);
+    for (int64_t pass = 0; pass < passes; pass++) {
+        for (auto &g : Grids)
+            for (int f = 0; f < g.N_soln; f++) g.Vec_soln.at(f).set_constant(0.);
+        Record_E_k.set_constant(0.);
+        Record_E_p0.set_constant(0.);
+        Record_E_p1.set_constant(0.);
+        if (Nt > 0) {
+            auto t0 = std::chrono::steady_clock::now();
+            if (!dispatch_cpst(Fwd_Specs, cpst_N, cpst_S)) { std::fprintf(stderr, "bad cpst\n"); return 2; }
+            auto t1 = std::chrono::steady_clock::now();
+            loop_seconds = std::chrono::duration<double>(t1 - t0).count();
+        }
     }
 
     if (quiet) {

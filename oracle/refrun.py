@@ -64,6 +64,7 @@ class ElasticCase:
     den_dxM: int | None = None
     bc_x: str = "F"      # "F" free surfaces; "I" x ends joined by the SAT interface penalty
     sat_y: bool = False  # free surfaces on the y ends too (restatement only: no reference run)
+    warm_passes: int = 0  # untimed runs of the same Nt steps before the timed one (outputs unchanged)
 
 
 @dataclass
@@ -95,6 +96,7 @@ def run_elastic(case: ElasticCase, precision: str = "f64", perf: bool = False) -
     cn, cs = CPST_CODES[case.cpst]
     ih = np.zeros(32, np.int64)
     ih[20] = 0 if case.bc_x == "F" else ord(case.bc_x)
+    ih[21] = case.warm_passes
     ih[:20] = [0x5457454C, case.Mx, case.My, Mxp, Myp, case.num_dx, case.den_dx, ndM, ddM,
                case.Nt, cn, ord(cs), ord(case.src[0]), ord(case.src[1]), *case.src[2:6],
                len(case.rcvs), 1]

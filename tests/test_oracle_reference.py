@@ -86,6 +86,21 @@ def test_oracle_matches_live_reference(Mx, My, cpst, seed):
 
 
 @pytest.mark.skipif(not has_ref_binaries(), reason="reference binaries (oracle/_ref) not built")
+def test_reference_warm_up_pass_leaves_outputs_unchanged():
+    """The benchmark's reference arm times the pass after an untimed one: that pass starts
+    from rest again and must give the outputs of a single pass, bit for bit."""
+    import dataclasses
+    case = elastic_case(17, 12, seed=15, cpst="00", Nt=30, model="layered")
+    one = refrun.run_elastic(case, "f32", perf=True)
+    two = refrun.run_elastic(dataclasses.replace(case, warm_passes=1), "f32", perf=True)
+    for k in one.fields:
+        assert np.array_equal(one.fields[k], two.fields[k]), k
+    assert np.array_equal(one.traces, two.traces)
+    for a, b in ((one.E_k, two.E_k), (one.E_p0, two.E_p0), (one.E_p1, two.E_p1)):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.skipif(not has_ref_binaries(), reason="reference binaries (oracle/_ref) not built")
 def test_oracle_matches_live_reference_acoustic():
     case = acoustic_periodic_case(14, 22, seed=21, cpst="6", Nt=40)
     for prec in ("f64", "f32"):
