@@ -261,6 +261,7 @@ __device__ __forceinline__ void gather_block(const GatherArgs<S> &g)
 template <class S>
 __global__ void k_gather(GatherArgs<S> g)
 {
+    pdl_enter();
     gather_block(g);
 }
 
@@ -274,7 +275,7 @@ __global__ void k_batch_gather(const GatherArgs<S> *g)
 template <class S>
 void launch_gather(const GatherArgs<S> &g, cudaStream_t st)
 {
-    k_gather<S><<<1, 256, 0, st>>>(g);
+    launch_pdl(k_gather<S>, dim3(1), dim3(256), 0, st, g);
 }
 template void launch_gather<double>(const GatherArgs<double> &, cudaStream_t);
 template void launch_gather<float>(const GatherArgs<float> &, cudaStream_t);

@@ -6,6 +6,33 @@
 
 namespace tw {
 
+// Programmatic dependent launch, for the short kernels of the launch-bound small-grid steps: a
+// kernel launched by launch_pdl may be scheduled while the previous kernel in the stream is still
+// running; it first waits (griddepcontrol.wait) until that kernel has finished and its writes are
+// visible, so it reads exactly what an ordinary launch would, and then lets the next kernel be
+// scheduled as its own blocks retire. What is saved is the gap between launches. (On the
+// one-launch fused elastic step it did not pay, so that launch stays ordinary.)
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;\n" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+template <class... P, class... A>
+inline cudaError_t launch_pdl(void (*k)(P...), dim3 g, dim3 b, size_t smem, cudaStream_t st, A... args)
+{
+    cudaLaunchConfig_t cfg{};
+    cfg.gridDim = g;
+    cfg.blockDim = b;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k, args...);
+}
+
 // one half of a time step: half 0 = velocities (+ V source), half 1 = stresses (+ S source)
 template <class S, class C>
 void launch_half(int physics, int periodic, int cpst, int half, const StepArgs<S, C> &a, cudaStream_t st);

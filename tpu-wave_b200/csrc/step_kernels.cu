@@ -125,12 +125,14 @@ __global__ void __launch_bounds__(256) k_elastic_stress(StepArgs<S, C> a)
 template <class S, class C, int CPST, bool PERIODIC>
 __global__ void __launch_bounds__(256) k_acoustic_velocity(StepArgs<S, C> a)
 {
+    pdl_enter();
     acoustic_velocity_point<S, C, CPST, PERIODIC>(a, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
 template <class S, class C, int CPST, bool PERIODIC>
 __global__ void __launch_bounds__(256) k_acoustic_pressure(StepArgs<S, C> a)
 {
+    pdl_enter();
     acoustic_pressure_point<S, C, CPST, PERIODIC>(a, blockIdx.y * blockDim.y + threadIdx.y, blockIdx.x * blockDim.x + threadIdx.x);
 }
 
@@ -147,11 +149,11 @@ void launch_cpst(int physics, int periodic, int half, const StepArgs<S, C> &a, c
         if (half == 0) k_elastic_velocity<S, C, CPST><<<gN, b, 0, st>>>(a);
         else k_elastic_stress<S, C, CPST><<<gN, b, 0, st>>>(a);
     } else if (periodic) {
-        if (half == 0) k_acoustic_velocity<S, C, CPST, true><<<gN, b, 0, st>>>(a);
-        else k_acoustic_pressure<S, C, CPST, true><<<gM, b, 0, st>>>(a);
+        if (half == 0) launch_pdl(k_acoustic_velocity<S, C, CPST, true>, gN, b, 0, st, a);
+        else launch_pdl(k_acoustic_pressure<S, C, CPST, true>, gM, b, 0, st, a);
     } else {
-        if (half == 0) k_acoustic_velocity<S, C, CPST, false><<<gN, b, 0, st>>>(a);
-        else k_acoustic_pressure<S, C, CPST, false><<<gM, b, 0, st>>>(a);
+        if (half == 0) launch_pdl(k_acoustic_velocity<S, C, CPST, false>, gN, b, 0, st, a);
+        else launch_pdl(k_acoustic_pressure<S, C, CPST, false>, gM, b, 0, st, a);
     }
 }
 }  // namespace
