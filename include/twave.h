@@ -115,6 +115,13 @@ typedef struct tw_solver tw_solver;
 TW_API int tw_create(tw_solver **out, const tw_grid_desc *desc);
 TW_API void tw_destroy(tw_solver *s);
 
+/* Device memory of destroyed handles. A handle takes its buffers from a per-device memory pool
+ * (stream-ordered) and tw_destroy returns them to it; the pool keeps them, so that creating the
+ * next handle of a similar size maps no new memory (the reference allocates and frees per run,
+ * grid.cuh:216-375 and cuda_container_run_time.cuh:268-275). This call gives the memory the
+ * pool keeps on `device` back to the driver. No counterpart in the reference. */
+TW_API int tw_release_cached_memory(int device);
+
 /* Material from the reference's padded node model: Class_Grid::retrieve_forward_parameter,
  * define_parameters_energy, adjust_parameters_energy_periodic and make_density_reciprocal
  * (grid_parameter.cpp:7-160, grid_energy.cpp:8-177; main_host_FDM_2D.tpp:146-168).

@@ -23,6 +23,9 @@ from dataclasses import dataclass, field
 import numpy as np
 
 REF_DIR = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_ref")
+# where the reference's sources are (only the oracle build and the tests of its example files
+# read them); TW_REFERENCE_DIR overrides the default location
+REFERENCE_DIR = os.environ.get("TW_REFERENCE_DIR", "/root/reference")
 
 CPST_CODES = {"00": (0, "0"), "-3C": (-3, "C"), "-3R": (-3, "R"), "3C": (3, "C"),
               "3R": (3, "R"), "6C": (6, "C"), "6R": (6, "R")}

@@ -24,9 +24,11 @@ def _ensure_built():
         subprocess.run([sys.executable, os.path.join(ROOT, "tpu-wave_b200", "build.py")], check=True)
     if not os.path.exists(os.path.join(ROOT, "oracle", "_build", "libtwave_oracle.so")):
         subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "oracle"], check=True)
-    ref_present = os.path.isdir("/root/reference")
+    from oracle.refrun import REFERENCE_DIR
+    ref_present = os.path.isdir(REFERENCE_DIR)
     if ref_present and not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "twref_elastic_f64")):
-        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle"), "ref"], check=True)
+        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(ROOT, "oracle"), "ref", f"REF={REFERENCE_DIR}"],
+                       check=True)
 
 
 _ensure_built()

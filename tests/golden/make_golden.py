@@ -5,8 +5,8 @@
 The reference ships no golden vectors, known-answer tests or result files (its only data are the
 homogeneous InputFile/SrcRcv examples), so these fixtures are its outputs on seeded inputs:
 oracle/_ref/twref_elastic_{f64,f32} (cuda/src/cpp host solver) and
-oracle/_ref/twref_acoustic_{f64,f32} (singlecore solver), built from /root/reference by
-`make -C oracle ref`. Each .npz holds the case inputs and, per precision, the final fields, the
+oracle/_ref/twref_acoustic_{f64,f32} (singlecore solver), built from the reference's sources
+(oracle.refrun.REFERENCE_DIR, environment variable TW_REFERENCE_DIR) by `make -C oracle ref`. Each .npz holds the case inputs and, per precision, the final fields, the
 receiver traces, the three energy records, the stored coefficients and the energy weights.
 The "_if_" fixtures select the reference's SAT interface branch for both x ends (a boundary type
 other than 'F', grid_drvt.tpp:575-693), which the reference's own inputs never reach.

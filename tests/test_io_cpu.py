@@ -7,8 +7,9 @@ import numpy as np
 import pytest
 
 from cases import load_twave
+from oracle.refrun import REFERENCE_DIR
 
-REF_DATA = "/root/reference/cuda/data/homogeneous"
+REF_DATA = os.path.join(REFERENCE_DIR, "cuda", "data", "homogeneous")
 
 
 @pytest.fixture(scope="module")

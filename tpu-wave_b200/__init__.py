@@ -84,6 +84,7 @@ def lib() -> C.CDLL:
         L.tw_create.argtypes = [C.POINTER(vp), C.POINTER(GridDesc)]
         L.tw_destroy.argtypes = [vp]
         L.tw_destroy.restype = None
+        L.tw_release_cached_memory.argtypes = [C.c_int]
         L.tw_set_material_model.argtypes = [vp, dp, dp, dp, C.c_long, C.c_long, C.c_int, C.c_int]
         L.tw_set_material_grid.argtypes = [vp, C.c_int, C.c_int, dp, C.c_long]
         L.tw_set_source_location.argtypes = [vp, C.c_char, C.c_char, C.c_long, C.c_long, C.c_long, C.c_long]
@@ -171,6 +172,11 @@ def io_read_model(path: str, Mx_prmt: int, My_prmt: int) -> np.ndarray:
     out = np.zeros((Mx_prmt + 2, My_prmt + 2))
     _ok(lib().tw_io_read_model(path.encode(), Mx_prmt, My_prmt, _dp(out)), "tw_io_read_model")
     return out
+
+
+def release_cached_memory(device: int = 0):
+    """Give the device memory that destroyed handles left in the per-device pool back to the driver."""
+    _ok(lib().tw_release_cached_memory(device), "tw_release_cached_memory")
 
 
 def location_to_index(gtype: str, num: int, den: int, num_dx: int, den_dx: int) -> int:

@@ -26,13 +26,30 @@ FLAGS = ["-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-li
          "-I" + os.path.join(HERE, "..", "include")]
 
 
+def _headers_mtime() -> float:
+    files = [f for f in glob.glob(os.path.join(CSRC, "*")) if not f.endswith(".cu")]
+    files += glob.glob(os.path.join(HERE, "..", "include", "*.h"))
+    return max(os.path.getmtime(f) for f in files)
+
+
 def _deps_mtime() -> float:
     files = glob.glob(os.path.join(CSRC, "*")) + glob.glob(os.path.join(HERE, "..", "include", "*.h"))
     return max(os.path.getmtime(f) for f in files)
 
 
+def _obj_of(src: str) -> str:
+    return os.path.join(OBJ, os.path.splitext(os.path.basename(src))[0] + ".o")
+
+
+def _stale(src: str, force: bool) -> bool:
+    obj = _obj_of(src)
+    if force or not os.path.exists(obj):
+        return True
+    return os.path.getmtime(obj) < max(os.path.getmtime(src), _headers_mtime())
+
+
 def _compile(src: str) -> str:
-    obj = os.path.join(OBJ, os.path.splitext(os.path.basename(src))[0] + ".o")
+    obj = _obj_of(src)
     cmd = [NVCC, *FLAGS, "-c", src, "-o", obj]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -46,8 +63,12 @@ def build(force: bool = False, verbose: bool = False) -> str:
     if not force and os.path.exists(LIB) and os.path.getmtime(LIB) >= _deps_mtime():
         return LIB
     sources = sorted(glob.glob(os.path.join(CSRC, "*.cu")))
-    with cf.ThreadPoolExecutor(max_workers=min(8, len(sources))) as ex:
-        objs = list(ex.map(_compile, sources))
+    # a source is recompiled when it, or any header, is newer than its object
+    stale = [s for s in sources if _stale(s, force)]
+    if stale:
+        with cf.ThreadPoolExecutor(max_workers=min(8, len(stale))) as ex:
+            list(ex.map(_compile, stale))
+    objs = [_obj_of(s) for s in sources]
     cmd = [NVCC, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB, *objs, "-lcudart"]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <algorithm>
 #include <array>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -54,6 +55,51 @@ bool location_to_index(char type, long num, long den, int num_dx, int den_dx, lo
     if (d == 0 || n % d != 0) return false;
     *out = n / d;
     return true;
+}
+
+// One memory pool per device for the handles' buffers. A destroyed handle returns its buffers
+// to the pool, which keeps them (release threshold: everything), so that the next handle of a
+// similar size - the next shot of an inversion, the next call of a caller that creates a handle
+// per simulation - maps no new device memory. tw_release_cached_memory gives it back.
+constexpr int MAX_DEVICES = 64;
+std::mutex g_pool_mu;
+cudaMemPool_t g_pool[MAX_DEVICES] = {};
+
+cudaMemPool_t handle_pool(int device, cudaError_t *err)
+{
+    *err = cudaSuccess;
+    if (device < 0 || device >= MAX_DEVICES) { *err = cudaErrorInvalidDevice; return nullptr; }
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pool[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t p = nullptr;
+        if ((*err = cudaMemPoolCreate(&p, &props)) != cudaSuccess) return nullptr;
+        unsigned long long keep = ~0ull;   // cuuint64_t
+        if ((*err = cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) {
+            cudaMemPoolDestroy(p);
+            return nullptr;
+        }
+        g_pool[device] = p;
+    }
+    return g_pool[device];
+}
+
+// let device `peer` read and write the handle buffers of device `owner` (peer stores of the
+// linked slab step, peer copies of the slab exchange)
+cudaError_t pool_peer_access(int owner, int peer)
+{
+    cudaError_t e;
+    cudaMemPool_t p = handle_pool(owner, &e);
+    if (e != cudaSuccess) return e;
+    cudaMemAccessDesc a{};
+    a.location.type = cudaMemLocationTypeDevice;
+    a.location.id = peer;
+    a.flags = cudaMemAccessFlagsProtReadWrite;
+    return cudaMemPoolSetAccess(p, &a, 1);
 }
 
 }  // namespace
@@ -107,15 +153,23 @@ struct tw_solver {
     int sticky = TW_OK;
     cudaGraphExec_t gexec = nullptr;
     int graph_steps = 0;
+    int graph_parity = 0;             // the buffer the captured graph starts from
     double dev_bytes = 0;
 
     ~tw_solver();
+    // device buffers come from the device's handle pool, ordered on the handle's stream
     int alloc(void **p, size_t bytes)
     {
-        cudaError_t e = cudaMalloc(p, bytes);
-        if (e != cudaSuccess) { cuda_fail(e, "cudaMalloc"); return TW_ERR_NOMEM; }
+        cudaError_t e = cudaSuccess;
+        cudaMemPool_t pool = handle_pool(d.device, &e);
+        if (e == cudaSuccess) e = cudaMallocFromPoolAsync(p, bytes, pool, st);
+        if (e != cudaSuccess) { *p = nullptr; cuda_fail(e, "cudaMallocFromPoolAsync"); return TW_ERR_NOMEM; }
         dev_bytes += (double)bytes;
         return TW_OK;
+    }
+    void release(void *p)
+    {
+        if (p) cudaFreeAsync(p, st);
     }
     bool has_slot(int slot) const { return rows[slot] > 0; }
     void drop_graph()
@@ -129,14 +183,16 @@ struct tw_solver {
 tw_solver::~tw_solver()
 {
     drop_graph();
+    if (!st) return;   // nothing was allocated before the stream
     for (int k = 0; k < 5; k++) {
-        cudaFree(f[k]); cudaFree(res[k]); cudaFree(coef[k]); cudaFree(w[k]); cudaFree(mat[k]);
+        release(f[k]); release(res[k]); release(coef[k]); release(w[k]); release(mat[k]);
     }
-    for (int k = 0; k < 5; k++) { cudaFree(f2[k]); cudaFree(res2[k]); }
-    cudaFree(d_done); cudaFree(d_rcv_off); cudaFree(d_rcv_list); cudaFree(model);
-    cudaFree(src_inc); cudaFree(d_step); cudaFree(d_flags); cudaFree(d_rcv); cudaFree(d_err);
-    cudaFree(d_traces); cudaFree(d_energy);
-    if (st) cudaStreamDestroy(st);
+    for (int k = 0; k < 5; k++) { release(f2[k]); release(res2[k]); }
+    release(d_done); release(d_rcv_off); release(d_rcv_list); release(model);
+    release(src_inc); release(d_step); release(d_flags); release(d_rcv); release(d_err);
+    release(d_traces); release(d_energy);
+    cudaStreamSynchronize(st);   // the buffers are back in the pool before the next handle asks
+    cudaStreamDestroy(st);
 }
 
 namespace {
@@ -502,8 +558,8 @@ int upload_receivers(tw_solver *s)
 {
     const int n = (int)(s->rcv_tab.size() / 4);
     if (n > s->rcv_cap) {
-        cudaFree(s->d_rcv);
-        cudaFree(s->d_traces);
+        s->release(s->d_rcv);
+        s->release(s->d_traces);
         s->d_rcv = nullptr;
         s->d_traces = nullptr;
         int cap = s->rcv_cap ? s->rcv_cap : 16;
@@ -548,7 +604,7 @@ int upload_receivers(tw_solver *s)
             list.insert(list.end(), per[c].begin(), per[c].end());
         }
         if ((int)list.size() > s->rcv_list_cap) {
-            cudaFree(s->d_rcv_list);
+            s->release(s->d_rcv_list);
             s->d_rcv_list = nullptr;
             int cap = 64;
             while (cap < (int)list.size()) cap *= 2;
@@ -567,7 +623,7 @@ int upload_receivers(tw_solver *s)
                 if (q[f] >= 0) list.insert(list.end(), {q[f], q[2], q[3], 2 * r + f});
         }
         if ((int)list.size() > s->rcv_list_cap) {
-            cudaFree(s->d_rcv_list);
+            s->release(s->d_rcv_list);
             s->d_rcv_list = nullptr;
             int cap = 64;
             while (cap < (int)list.size()) cap *= 2;
@@ -643,6 +699,25 @@ int write_device_array(tw_solver *s, void *dev, int prec, int esz, int slot, con
 int check(tw_solver *s)
 {
     return s ? TW_OK : TW_ERR_INVALID;
+}
+
+// peer access between two devices in both directions, for contexts and for the handle pools
+int link_devices(int d0, int d1)
+{
+    if (d0 == d1) return TW_OK;
+    int ok01 = 0, ok10 = 0;
+    TW_CUDA(cudaDeviceCanAccessPeer(&ok01, d0, d1));
+    TW_CUDA(cudaDeviceCanAccessPeer(&ok10, d1, d0));
+    if (!ok01 || !ok10) return TW_ERR_UNSUPPORTED;
+    for (int q = 0; q < 2; q++) {
+        TW_CUDA(cudaSetDevice(q ? d1 : d0));
+        const cudaError_t e = cudaDeviceEnablePeerAccess(q ? d0 : d1, 0);
+        if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
+        else if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceEnablePeerAccess");
+    }
+    TW_CUDA(pool_peer_access(d0, d1));
+    TW_CUDA(pool_peer_access(d1, d0));
+    return TW_OK;
 }
 
 }  // namespace
@@ -891,6 +966,21 @@ void tw_destroy(tw_solver *s)
     delete s;
 }
 
+int tw_release_cached_memory(int device)
+{
+    if (device < 0 || device >= MAX_DEVICES) return TW_ERR_INVALID;
+    cudaMemPool_t p;
+    {
+        std::lock_guard<std::mutex> lk(g_pool_mu);
+        p = g_pool[device];
+    }
+    if (!p) return TW_OK;
+    TW_CUDA(cudaSetDevice(device));
+    TW_CUDA(cudaDeviceSynchronize());   // frees still queued on a stream complete first
+    TW_CUDA(cudaMemPoolTrimTo(p, 0));
+    return TW_OK;
+}
+
 int tw_set_material_model(tw_solver *s, const double *rho, const double *vp, const double *vs, long Mx_prmt,
                           long My_prmt, int num_dxM, int den_dxM)
 {
@@ -903,11 +993,25 @@ int tw_set_material_model(tw_solver *s, const double *rho, const double *vp, con
     }
     TW_CUDA(cudaSetDevice(s->d.device));
     const long Nxp = Mx_prmt + 1, Nyp = My_prmt + 1, P = (Nxp + 1) * (Nyp + 1);
-    double *buf = nullptr;   // rho, vp, vs, lambda, 2mu, mu on the padded model
-    TW_CUDA(cudaMalloc((void **)&buf, sizeof(double) * 6 * P));
-    double *drho = buf, *dvp = buf + P, *dvs = buf + 2 * P, *lam = buf + 3 * P, *m2 = buf + 4 * P, *mu = buf + 5 * P;
+    // rho, vp, vs land in the handle's model copy (kept for the model gradient of
+    // tw_adjoint_gradient); lambda, 2mu, mu on the padded model in a temporary from the pool
+    if (s->model && (s->model_Mxp != Mx_prmt || s->model_Myp != My_prmt)) {
+        s->release(s->model);
+        s->model = nullptr;
+    }
+    s->model_set = false;
     int rc = TW_OK;
-    auto done = [&](int code) { cudaStreamSynchronize(s->st); cudaFree(buf); return code; };
+    if (!s->model && (rc = s->alloc((void **)&s->model, sizeof(double) * 3 * P)) != TW_OK) {
+        s->model = nullptr;
+        return rc;
+    }
+    s->model_Mxp = Mx_prmt;
+    s->model_Myp = My_prmt;
+    double *der = nullptr;
+    if ((rc = s->alloc((void **)&der, sizeof(double) * 3 * P)) != TW_OK) return rc;
+    double *drho = s->model, *dvp = s->model + P, *dvs = s->model + 2 * P;
+    double *lam = der, *m2 = der + P, *mu = der + 2 * P;
+    auto done = [&](int code) { s->release(der); cudaStreamSynchronize(s->st); return code; };
     cudaError_t e;
     if ((e = cudaMemcpyAsync(drho, rho, sizeof(double) * P, cudaMemcpyHostToDevice, s->st)) != cudaSuccess ||
         (e = cudaMemcpyAsync(dvp, vp, sizeof(double) * P, cudaMemcpyHostToDevice, s->st)) != cudaSuccess)
@@ -931,19 +1035,7 @@ int tw_set_material_model(tw_solver *s, const double *rho, const double *vp, con
     if ((e = cudaStreamSynchronize(s->st)) != cudaSuccess) return done(cuda_fail(e, "model"));
     if (herr) return done(TW_ERR_MODEL_BOUNDS);
     rc = finalize_material(s);
-    if (rc == TW_OK) {   // keep rho, vp, vs for the model gradient (tw_adjoint_gradient)
-        if (s->model && (s->model_Mxp != Mx_prmt || s->model_Myp != My_prmt)) {
-            cudaFree(s->model);
-            s->model = nullptr;
-        }
-        if (!s->model && (e = cudaMalloc((void **)&s->model, sizeof(double) * 3 * P)) != cudaSuccess) {
-            s->model = nullptr;
-            return done(cuda_fail(e, "model copy"));
-        }
-        if ((e = cudaMemcpyAsync(s->model, buf, sizeof(double) * 3 * P, cudaMemcpyDeviceToDevice, s->st)) != cudaSuccess)
-            return done(cuda_fail(e, "model copy"));
-        s->model_Mxp = Mx_prmt;
-        s->model_Myp = My_prmt;
+    if (rc == TW_OK) {   // the node model now describes the material (tw_adjoint_gradient)
         s->model_ndM = num_dxM;
         s->model_ddM = den_dxM;
         s->model_set = true;
@@ -1081,27 +1173,35 @@ int tw_step(tw_solver *s, int n)
     if (s->steps_done + (long)n > s->d.max_steps) return TW_ERR_RECORD_FULL;
     if (n == 0) return TW_OK;
     TW_CUDA(cudaSetDevice(s->d.device));
-    // a graph of G steps captured once and replayed; leftover steps are launched directly
+    // a graph of G steps captured once and replayed; leftover steps are launched directly. The
+    // graph is captured on the first call of any length when the records hold G steps, so that
+    // a short first call (a warm-up) leaves the next long call only replays and direct launches.
     const int G = 16;
+    // the one-launch steps alternate buffers, and their graph starts from the first one; the
+    // two-launch kernels update the current buffer in place, and their graph is bound to it
+    // (a batch step may have moved the state of a double-buffered shot to the other buffer)
+    const int gpar = (s->fused || s->afused) ? 0 : s->parity;
+    if ((!s->gexec || s->graph_steps != G || s->graph_parity != gpar) && s->d.max_steps >= G) {
+        s->drop_graph();
+        cudaGraph_t graph;
+        TW_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+        const int parity0 = s->parity;
+        s->parity = gpar;
+        enqueue(s, G, s->st);
+        s->parity = parity0;   // capture only records; replays advance the parity below
+        TW_CUDA(cudaStreamEndCapture(s->st, &graph));
+        cudaError_t e = cudaGraphInstantiate(&s->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
+        s->graph_steps = G;
+        s->graph_parity = gpar;
+    }
     int left = n;
     if ((s->fused || s->afused) && s->parity && left > 0 && n >= G) {
         enqueue(s, 1, s->st);   // captured graphs start from the first buffer
         left--;
     }
-    if (left >= G) {
-        if (!s->gexec || s->graph_steps != G) {
-            s->drop_graph();
-            cudaGraph_t graph;
-            TW_CUDA(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-            const int parity0 = s->parity;
-            enqueue(s, G, s->st);
-            s->parity = parity0;   // capture only records; replays advance the parity below
-            TW_CUDA(cudaStreamEndCapture(s->st, &graph));
-            cudaError_t e = cudaGraphInstantiate(&s->gexec, graph, 0);
-            cudaGraphDestroy(graph);
-            if (e != cudaSuccess) return cuda_fail(e, "cudaGraphInstantiate");
-            s->graph_steps = G;
-        }
+    if (left >= G && s->gexec) {
         while (left >= G) {
             TW_CUDA(cudaGraphLaunch(s->gexec, s->st));
             left -= G;   // G is even: the parity is unchanged
@@ -1262,6 +1362,10 @@ int tw_slab_exchange(tw_solver *up, tw_solver *lo)
     if (up->Mx_glob != lo->Mx_glob || up->own1 != lo->own0 || up->d.My != lo->d.My || up->esz != lo->esz ||
         up->d.cpst != lo->d.cpst || up->steps_done != lo->steps_done)
         return TW_ERR_INVALID;
+    if (up->d.device != lo->d.device) {
+        const int rc = link_devices(up->d.device, lo->d.device);
+        if (rc != TW_OK) return rc;
+    }
     TW_CUDA(cudaSetDevice(lo->d.device));
     TW_CUDA(cudaStreamSynchronize(lo->st));
     TW_CUDA(cudaSetDevice(up->d.device));
@@ -1303,18 +1407,8 @@ int tw_slab_run(tw_solver *const *slabs, int n, int steps)
     if (slabs[0]->own0 != 0 || slabs[n - 1]->own1 != slabs[0]->Mx_glob) return TW_ERR_INVALID;   // the whole grid
     // neighbours on other GPUs are written through peer access (NVLink)
     for (int i = 0; i + 1 < n; i++) {
-        const int d0 = slabs[i]->d.device, d1 = slabs[i + 1]->d.device;
-        if (d0 == d1) continue;
-        int ok01 = 0, ok10 = 0;
-        TW_CUDA(cudaDeviceCanAccessPeer(&ok01, d0, d1));
-        TW_CUDA(cudaDeviceCanAccessPeer(&ok10, d1, d0));
-        if (!ok01 || !ok10) return TW_ERR_UNSUPPORTED;
-        for (int q = 0; q < 2; q++) {
-            TW_CUDA(cudaSetDevice(q ? d1 : d0));
-            const cudaError_t e = cudaDeviceEnablePeerAccess(q ? d0 : d1, 0);
-            if (e == cudaErrorPeerAccessAlreadyEnabled) cudaGetLastError();
-            else if (e != cudaSuccess) return cuda_fail(e, "cudaDeviceEnablePeerAccess");
-        }
+        const int rc = link_devices(slabs[i]->d.device, slabs[i + 1]->d.device);
+        if (rc != TW_OK) return rc;
     }
     std::vector<cudaEvent_t> ev(n, nullptr);
     int rc = TW_OK;
@@ -1350,6 +1444,14 @@ int tw_slab_run(tw_solver *const *slabs, int n, int steps)
         }
         if (rc == TW_OK)
             for (int i = 0; i < n; i++) slabs[i]->steps_done += 1;
+    }
+    // the last step of a slab still stores into its neighbours' rows: each slab's stream waits
+    // for its neighbours' last step, so that synchronising, stepping, reading or destroying one
+    // handle alone afterwards is ordered after every write into its buffers
+    for (int i = 0; i < n && rc == TW_OK && steps > 0; i++) {
+        cudaSetDevice(slabs[i]->d.device);
+        for (int q : {i - 1, i + 1})
+            if (q >= 0 && q < n && cudaStreamWaitEvent(slabs[i]->st, ev[q], 0) != cudaSuccess) rc = TW_ERR_CUDA;
     }
     for (int i = 0; i < n; i++) {
         slabs[i]->link[0] = slabs[i]->link[1] = nullptr;
