@@ -44,7 +44,8 @@ enum {
     TW_ERR_UNSUPPORTED = -10,   /* combination not implemented (e.g. elastic with periodic x) */
     TW_ERR_MODEL_BOUNDS = -11,  /* interpolation stepped out of the model (grid_parameter.cpp:54-56) */
     TW_ERR_TOO_LARGE = -12,     /* model larger than the no-allocation scratch (TW_NOALLOC_MAX_MODEL_POINTS) */
-    TW_ERR_IO = -13             /* a file could not be opened, read or written, or is malformed */
+    TW_ERR_IO = -13,            /* a file could not be opened, read or written, or is malformed */
+    TW_ERR_TIMEOUT = -14        /* a wait inside a step kernel gave up (a staged copy did not arrive) */
 };
 
 /* ---- enums ------------------------------------------------------------------------------ */
@@ -280,7 +281,8 @@ TW_API int tw_adjoint_gradient(tw_solver *s, int nt, const double *obs, int ckpt
 
 /* Data misfit of the recorded traces against observed ones: calculate_data_misfit
  * (forward.cpp:414-445), sum over steps and fields of (trace - obs)^2 per receiver (no factor
- * 1/2: twice tw_adjoint_gradient's J). obs: [n_rcv][2][steps_done]; per_rcv may be NULL. */
+ * 1/2: twice tw_adjoint_gradient's J), the difference taken in the storage precision for FP32
+ * handles as the reference's FP32 build does. obs: [n_rcv][2][steps_done]; per_rcv may be NULL. */
 TW_API int tw_data_misfit(tw_solver *s, const double *obs, double *total, double *per_rcv);
 
 /* ---- batched shots ---------------------------------------------------------------------

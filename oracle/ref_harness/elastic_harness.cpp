@@ -27,7 +27,15 @@
 //          SAT interface branch of secure_bdry, grid_drvt.tpp:575-693),
 //       21 untimed warm-up passes: the whole run of Nt steps is made this many times from rest
 //          before the timed pass (the outputs are those of the timed pass, identical to them)
+//       22 1: observed traces follow the receiver table (float64 [n_rcv][2][Nt], the second
+//          field ignored on single-field grids); after the run the reference's
+//          calculate_data_misfit (forward.cpp:414-445) compares them with the recorded traces
 //   dh: 0 dt, 1 central_f, 2 time_delay
+// Optional third argument: a folder into which the reference's own writers put their files
+// after the run (output_solution_record and output_energy, forward.cpp:215-325, with the text
+// output that bool_visual selects).
+// With ih[22] = 1 the output file ends with the total misfit and one misfit per receiver (input
+// order).
 //   P = (Mx_prmt + 2) * (My_prmt + 2)  (the reference's padded model layout, inverse.cpp:79-90)
 // Output file: float64 loop_seconds; E_k[Nt]; E_p0[Nt]; E_p1[Nt]; traces[n_rcv][2][Nt];
 //              fields NN, MN, NM, MM0, MM1 (reference sizes, row-major, x slow);
@@ -82,7 +90,7 @@ void put_vec(std::FILE *f, run_time_vector<ns_type::host_precision> &v)
 
 int main(int argc, char **argv)
 {
-    if (argc != 3) { std::fprintf(stderr, "usage: %s input.bin output.bin\n", argv[0]); return 2; }
+    if (argc != 3 && argc != 4) { std::fprintf(stderr, "usage: %s input.bin output.bin [folder]\n", argv[0]); return 2; }
     std::FILE *fi = std::fopen(argv[1], "rb");
     if (!fi) { std::fprintf(stderr, "cannot open %s\n", argv[1]); return 2; }
     int64_t ih[32];
@@ -125,6 +133,9 @@ int main(int argc, char **argv)
         std::fread(vs.data(), 8, P, fi) != (size_t)P) { std::fprintf(stderr, "short model\n"); return 2; }
     std::vector<int64_t> rcv((size_t)n_rcv * 6);
     if (n_rcv > 0 && std::fread(rcv.data(), 8, rcv.size(), fi) != rcv.size()) { std::fprintf(stderr, "short rcv\n"); return 2; }
+    const bool misfit = ih[22] == 1;
+    std::vector<double> obs(misfit ? (size_t)n_rcv * 2 * Nt : 0);
+    if (misfit && !obs.empty() && std::fread(obs.data(), 8, obs.size(), fi) != obs.size()) { std::fprintf(stderr, "short obs\n"); return 2; }
     std::fclose(fi);
 
     int saved_stdout = -1;
@@ -204,6 +215,31 @@ int main(int argc, char **argv)
         }
     }
 
+    // the observed traces into the reference's record matrices, receiver by receiver in input
+    // order (grouped per grid type in input order, as process_rcv_locations stored them)
+    std::vector<double> misfit_rcv;
+    if (misfit) {
+        std::map<std::array<char, 2>, int> k_of;
+        for (int r = 0; r < n_rcv; r++) {
+            std::array<char, 2> t = rcv_in[r].rcv_grid_type;
+            int k = k_of[t]++;
+            auto &M = Fwd_Specs.Map_grid_record_rcv.at(t).at(k);
+            for (int f = 0; f < M.rows; f++)
+                for (int it = 0; it < Nt; it++) M.at(f, it) = (ns_type::host_precision)obs[((size_t)r * 2 + f) * Nt + it];
+        }
+        Fwd_Specs.calculate_data_misfit();
+        std::map<std::array<char, 2>, int> k2;
+        for (int r = 0; r < n_rcv; r++) {
+            std::array<char, 2> t = rcv_in[r].rcv_grid_type;
+            misfit_rcv.push_back(Fwd_Specs.Map_grid_misfit_rcv.at(t).at(k2[t]++));
+        }
+    }
+    if (argc == 4) {   // the reference's own writers (main_host_FDM_2D.tpp:270-272)
+        bool_visual = true;
+        Fwd_Specs.output_solution_record(argv[3]);
+        Fwd_Specs.output_energy(argv[3]);
+    }
+
     if (quiet) {
         std::fflush(stdout);
         dup2(saved_stdout, 1);
@@ -249,6 +285,11 @@ int main(int argc, char **argv)
     put(fo, NM.Vec_prmt_enrg.at(0).ptr, (size_t)NM.Vec_prmt_enrg.at(0).length);
     put(fo, MM.Vec_prmt_enrg.at(0).ptr, (size_t)MM.Vec_prmt_enrg.at(0).length);
     put(fo, MM.Vec_prmt_enrg.at(1).ptr, (size_t)MM.Vec_prmt_enrg.at(1).length);
+    if (misfit) {
+        const double total = Fwd_Specs.data_misfit;
+        put(fo, &total, 1);
+        put(fo, misfit_rcv.data(), misfit_rcv.size());
+    }
     std::fclose(fo);
     return 0;
 }

@@ -80,13 +80,19 @@ class ElasticResult:
     fields: dict               # NN, MN, NM, MM0, MM1 at reference sizes
     coefs: dict                # NN_mu, MN_irho, NM_irho, MM_lambda, MM_2mu
     weights: dict              # NN, MN, NM, MM_P1, MM_P2 (energy weights incl. norms)
+    misfit_total: float | None = None      # calculate_data_misfit against `obs` (when given)
+    misfit_rcv: np.ndarray | None = None   # per receiver, input order
 
 
 def _elastic_sizes(Mx, My):
     return {"NN": (Mx + 1, My + 1), "MN": (Mx, My + 1), "NM": (Mx + 1, My), "MM0": (Mx, My), "MM1": (Mx, My)}
 
 
-def run_elastic(case: ElasticCase, precision: str = "f64", perf: bool = False) -> ElasticResult:
+def run_elastic(case: ElasticCase, precision: str = "f64", perf: bool = False, obs: np.ndarray | None = None,
+                out_folder: str | None = None) -> ElasticResult:
+    """Run the reference's elastic solver on `case`. obs ([n_rcv][2][Nt] observed traces): also
+    return the reference's calculate_data_misfit against them. out_folder: let the reference's
+    own writers (output_solution_record, output_energy) put their text files there."""
     Mxp = case.Mx if case.Mx_prmt is None else case.Mx_prmt
     Myp = case.My if case.My_prmt is None else case.My_prmt
     ndM = case.num_dx if case.num_dxM is None else case.num_dxM
@@ -100,6 +106,7 @@ def run_elastic(case: ElasticCase, precision: str = "f64", perf: bool = False) -
     ih = np.zeros(32, np.int64)
     ih[20] = 0 if case.bc_x == "F" else ord(case.bc_x)
     ih[21] = case.warm_passes
+    ih[22] = 1 if obs is not None else 0
     ih[:20] = [0x5457454C, case.Mx, case.My, Mxp, Myp, case.num_dx, case.den_dx, ndM, ddM,
                case.Nt, cn, ord(cs), ord(case.src[0]), ord(case.src[1]), *case.src[2:6],
                len(case.rcvs), 1]
@@ -114,7 +121,10 @@ def run_elastic(case: ElasticCase, precision: str = "f64", perf: bool = False) -
             for a in (case.rho, case.vp, case.vs):
                 f.write(np.ascontiguousarray(a, np.float64).tobytes())
             f.write(rcv.tobytes())
-        subprocess.run([ref_binary(name), fin, fout], check=True, stdout=subprocess.DEVNULL)
+            if obs is not None:
+                f.write(np.ascontiguousarray(obs, np.float64).reshape(len(case.rcvs), 2, case.Nt).tobytes())
+        cmd = [ref_binary(name), fin, fout] + ([out_folder] if out_folder else [])
+        subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
         out = np.fromfile(fout, np.float64)
     Nt, n = case.Nt, len(case.rcvs)
     pos = 0
@@ -138,8 +148,12 @@ def run_elastic(case: ElasticCase, precision: str = "f64", perf: bool = False) -
     for key, g in (("NN", "NN"), ("MN", "MN"), ("NM", "NM"), ("MM_P1", "MM0"), ("MM_P2", "MM1")):
         s = sizes[g]
         weights[key] = take(s[0] * s[1], s)
+    mt, mr = None, None
+    if obs is not None:
+        mt = float(take(1)[0])
+        mr = take(n).copy()
     assert pos == out.size, (pos, out.size)
-    return ElasticResult(loop, E_k, E_p0, E_p1, traces, fields, coefs, weights)
+    return ElasticResult(loop, E_k, E_p0, E_p1, traces, fields, coefs, weights, mt, mr)
 
 
 @dataclass

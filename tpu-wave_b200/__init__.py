@@ -30,7 +30,7 @@ PRECISION = {"f64": FP64, "f32": FP32, "bf16": BF16, "fp16": FP16}
 
 ERRORS = {0: "TW_OK", -1: "TW_ERR_INVALID", -2: "TW_ERR_CUDA", -3: "TW_ERR_NOMEM", -4: "TW_ERR_STATE",
           -5: "TW_ERR_LOCATION", -6: "TW_ERR_OUTSIDE", -7: "TW_ERR_WEAK_BOUNDARY", -8: "TW_ERR_RECORD_FULL",
-          -9: "TW_ERR_NONFINITE", -10: "TW_ERR_UNSUPPORTED", -11: "TW_ERR_MODEL_BOUNDS", -12: "TW_ERR_TOO_LARGE", -13: "TW_ERR_IO"}
+          -9: "TW_ERR_NONFINITE", -10: "TW_ERR_UNSUPPORTED", -11: "TW_ERR_MODEL_BOUNDS", -12: "TW_ERR_TOO_LARGE", -13: "TW_ERR_IO", -14: "TW_ERR_TIMEOUT"}
 
 
 class TwError(RuntimeError):

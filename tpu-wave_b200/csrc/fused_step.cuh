@@ -201,13 +201,13 @@ __device__ __forceinline__ void store_pair(S *o, S *ro, int c0, int c1, S h0, S 
 // PUSH: the slab is linked to its neighbours (tw_slab_run) and stores its rows next to a cut into
 // their halo rows as well
 template <class S, class C, int CPST, bool ENERGY, bool EDGE, class K, bool PUSH>
-__device__ void interior_warp(const FusedArgs<S, C> &a, int wstrip, int seg, int it, int rcv_b, int rcv_e, EAcc &E,
+__device__ void interior_warp(const FusedArgs<S, C> &a, int y0, int seg, int it, int rcv_b, int rcv_e, EAcc &E,
                               unsigned char *ring)
 {
     constexpr bool KR = Cpst<CPST>::keep_r, KC = Cpst<CPST>::keep_c, SPLIT = Cpst<CPST>::split;
     const int lane = threadIdx.x & 31;
     const int Mx = a.Mx, My = a.My, pitch = (int)a.pitch;
-    const int y0 = wstrip * FS_WARP_CORE;
+    // y0: the first of the strip's FS_WARP_CORE columns (even)
     const int c0 = y0 - 4 + 2 * lane, c1 = c0 + 1;
     const int pM0 = pmod(c0, My), pM1 = pmod(c1, My);
     const int pN0 = (c0 >= 0 && c0 <= My) ? c0 : pM0, pN1 = (c1 >= 0 && c1 <= My) ? c1 : pM1;
@@ -847,8 +847,8 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<C, ENERGY>()) k_
             const int seg = gw / a.n_wstrip, wstrip = gw - seg * a.n_wstrip;
             const int y0 = wstrip * FS_WARP_CORE;
             unsigned char *ring = smem_raw + (threadIdx.x >> 5) * RingLayout<S, C, CPST, ENERGY, K>::warp;
-            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false, K, MODE == 1>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
-            else interior_warp<S, C, CPST, ENERGY, true, K, MODE == 1>(a, wstrip, seg, it, rcv_b, rcv_e, E, ring);
+            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<S, C, CPST, ENERGY, false, K, MODE == 1>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
+            else interior_warp<S, C, CPST, ENERGY, true, K, MODE == 1>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
         }
     } else {             // boundary CTA (zone, strip)
         const int b = cta;

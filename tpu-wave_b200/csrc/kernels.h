@@ -161,9 +161,36 @@ struct FusedArgs {
                               // zone-major, then interior CTAs segment-major)
     const int *rcv;           // [n][4]: field slot, row, column, trace row (2 * receiver + field)
     double *traces;
+    // the TMA-staged step (k_elastic_tma, tma_step.cuh): the interior rows of columns
+    // [TMA_Y0, y_tma_end) in n_tseg balanced segments x n_tstrip strips of TMA_CORE columns, one
+    // CTA each; the other interior columns (the periodic seam among them) in n_ostrip warp strips
+    // of FS_WARP_CORE columns (the first at column 0, the others from y_tma_end on) over n_oseg
+    // segments, FS_WARPS warps to a CTA. Block order: boundary CTAs, warp-strip CTAs, TMA CTAs.
+    int n_tseg, n_tstrip, n_tcta;
+    int n_oseg, n_ostrip, n_octa;
+    int y_tma_end;
 };
 template <class S, class C>
 void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, bool coef16, cudaStream_t st);
+
+// the TMA-staged fused step: FP32 fields and coefficients, plain update. The host encodes one
+// tensor map per array and buffer parity (tw_tma_maps) when the handle is created.
+constexpr int TMA_CORE = 120;        // core columns of a TMA strip (thread lanes 1..30, 4 columns each)
+constexpr int TMA_Y0 = FS_WARP_CORE; // the first TMA strip starts after the first warp strip
+constexpr int TMA_W = 128;           // columns a TMA strip loads: 4 halo on each side
+constexpr int TMA_ROWS = 4;          // rows per TMA block: one per warp
+constexpr int TMA_NMAP = 15;         // tensor maps: 5 fields, 5 coefficients, 5 energy weights
+struct TmaMaps {
+    alignas(64) unsigned char m[TMA_NMAP][128];   // CUtensorMap objects (opaque, 128 bytes each)
+};
+enum { TM_NN = 0, TM_MN, TM_NM, TM_MM0, TM_MM1, TM_PMN, TM_PNM, TM_MU, TM_LAM, TM_M2,
+       TM_WMN, TM_WNM, TM_WNN, TM_WM3, TM_WM4 };
+// how many strips and segments the TMA-staged step uses for a grid (0 strips: not applicable)
+int tma_strips(long My);
+template <class S, class C>
+cudaError_t prepare_tma();
+template <class S, class C>
+void launch_tma(const FusedArgs<S, C> &a, const TmaMaps &maps, bool energy, cudaStream_t st);
 
 // free y ends on the fused step (ysat_fix.cu): the fused kernel steps every column with the
 // periodic y rule; these two launches then recompute, from the step's input buffers, the points

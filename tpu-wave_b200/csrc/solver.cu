@@ -5,11 +5,14 @@
 // weights, source table and receiver records of one simulation and one CUDA stream. Steps are
 // enqueued asynchronously and replayed from a CUDA graph; every kernel of a step reads the step
 // index from a device counter, so one captured graph serves every replay.
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <algorithm>
 #include <array>
@@ -126,6 +129,11 @@ struct tw_solver {
     void *f2[5] = {}, *res2[5] = {};
     int parity = 0;                   // which buffer holds the current state (0: f/res, 1: f2/res2)
     int n_int_seg = 0, int_rows = 0, n_zone = 1, n_wstrip = 0, n_bstrip = 1, n_int_cta = 0, tile_rows = 1;
+    // the TMA-staged fused step (tma_step.cuh): strips, segments and CTAs, and one set of tensor
+    // maps per buffer parity (the input fields alternate between f and f2)
+    bool tma = false;
+    int n_tseg = 0, n_tstrip = 0, n_tcta = 0, n_ostrip = 0, y_tma_end = 0;
+    TmaMaps *tmaps = nullptr;
     int ir0 = FS_ZONE, zone_kind[2] = {0, 1};
     // a slab of a larger grid (slab decomposition along x): local row r is global row r + row_off
     // of a grid of Mx_glob cells; it owns global rows [own0, own1) of every grid (plus the last
@@ -183,6 +191,7 @@ struct tw_solver {
 tw_solver::~tw_solver()
 {
     drop_graph();
+    delete[] tmaps;
     if (!st) return;   // nothing was allocated before the stream
     for (int k = 0; k < 5; k++) {
         release(f[k]); release(res[k]); release(coef[k]); release(w[k]); release(mat[k]);
@@ -392,6 +401,21 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
         a.push_row[side] = (int)(side == 0 ? s->own0 - s->row_off : s->own1 - s->row_off - FS_HALO);
         a.peer_shift[side] = (int)(s->row_off - p->row_off);
     }
+    if constexpr (sizeof(S) == 4 && sizeof(C) == 4) {
+        // the TMA-staged step reads through tensor maps of the handle's own two buffers; a step
+        // between other buffers (the adjoint's segment recomputation) takes the per-warp kernel
+        if (s->tma && (fin == s->f || fin == s->f2) && fout == (fin == s->f ? s->f2 : s->f)) {
+            a.n_tseg = s->n_tseg;
+            a.n_tstrip = s->n_tstrip;
+            a.n_tcta = s->n_tcta;
+            a.n_oseg = s->n_int_seg;
+            a.n_ostrip = s->n_ostrip;
+            a.n_octa = s->n_int_cta;
+            a.y_tma_end = s->y_tma_end;
+            launch_tma<S, C>(a, s->tmaps[fin == s->f ? 0 : 1], s->d.energy != 0, st);
+            return;
+        }
+    }
     launch_fused<S, C>(a, s->d.cpst, s->d.energy != 0, s->d.coef_fp16 != 0, st);
 }
 
@@ -574,8 +598,7 @@ int upload_receivers(tw_solver *s)
     if (s->fused) {
         // per-CTA receiver lists: a receiver belongs to the CTA whose segment owns its row and
         // whose strip owns its column (fused_step.cu)
-        const int n_int = s->n_int_cta;
-        const int nctas = n_int + s->n_zone * s->n_bstrip;
+        const int nctas = s->n_int_cta + s->n_zone * s->n_bstrip + s->n_tcta;
         std::vector<std::vector<int>> per(nctas);
         const int Mx = (int)s->d.Mx;
         for (int r = 0; r < n; r++) {
@@ -587,13 +610,23 @@ int upload_receivers(tw_solver *s)
                 const int k = s->zone_kind[z];
                 if (k == 2 || ((k == 0 || k == 3) && row < FS_ZONE) || ((k == 1 || k == 3) && row >= Mx - FS_ZONE)) zone = z;
             }
+            // the balanced segment of n segments of the interior rows holding the row (fused_step.cuh)
+            auto seg_of = [&](int n) {
+                int seg = 0;
+                while (s->ir0 + (int)((long)(seg + 1) * s->int_rows / n) <= row) seg++;
+                return seg;
+            };
             int cta;
+            const int n_bnd = s->n_zone * s->n_bstrip;
             if (zone >= 0) {
                 cta = zone * s->n_bstrip + col / FS_BND_TY;
+            } else if (s->tma && col >= TMA_Y0 && col < s->y_tma_end) {   // a TMA strip CTA
+                cta = n_bnd + s->n_int_cta + seg_of(s->n_tseg) * s->n_tstrip + (col - TMA_Y0) / TMA_CORE;
+            } else if (s->tma) {                                         // a warp strip
+                const int os = col < TMA_Y0 ? 0 : 1 + (col - s->y_tma_end) / FS_WARP_CORE;
+                cta = n_bnd + (seg_of(s->n_int_seg) * s->n_ostrip + os) / FS_WARPS;
             } else {
-                int seg = 0;   // the balanced segment holding the row (fused_step.cuh)
-                while (s->ir0 + (int)((long)(seg + 1) * s->int_rows / s->n_int_seg) <= row) seg++;
-                cta = s->n_zone * s->n_bstrip + (seg * s->n_wstrip + col / FS_WARP_CORE) / FS_WARPS;
+                cta = n_bnd + (seg_of(s->n_int_seg) * s->n_wstrip + col / FS_WARP_CORE) / FS_WARPS;
             }
             for (int f = 0; f < 2; f++)
                 if (q[f] >= 0) per[cta].insert(per[cta].end(), {q[f], row, col, 2 * r + f});
@@ -696,6 +729,54 @@ int write_device_array(tw_solver *s, void *dev, int prec, int esz, int slot, con
     return TW_OK;
 }
 
+// cuTensorMapEncodeTiled from the driver, found at run time (the library links the runtime only)
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static std::once_flag once;
+    std::call_once(once, [] {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+        else
+            cudaGetLastError();
+    });
+    return fn;
+}
+
+// a tensor map over `rows` rows of `pitch` elements (FP32 or FP64) with boxes of TMA_W x TMA_ROWS
+int encode_rows(unsigned char *out, const void *ptr, bool f64, long rows, long pitch)
+{
+    const auto enc = tensor_map_encoder();
+    if (!enc) return TW_ERR_UNSUPPORTED;
+    const cuuint64_t dims[2] = {(cuuint64_t)pitch, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)pitch * (f64 ? 8 : 4)};
+    const cuuint32_t box[2] = {(cuuint32_t)TMA_W, (cuuint32_t)TMA_ROWS};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r = enc(reinterpret_cast<CUtensorMap *>(out),
+                           f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                           const_cast<void *>(ptr), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        g_cuda_error = "cuTensorMapEncodeTiled failed (" + std::to_string((int)r) + ")";
+        return TW_ERR_CUDA;
+    }
+    return TW_OK;
+}
+
+// an integer tuning knob from the environment (absent or malformed: the default)
+int env_int(const char *name, int dflt)
+{
+    const char *v = std::getenv(name);
+    if (!v || !*v) return dflt;
+    char *end = nullptr;
+    const long x = std::strtol(v, &end, 10);
+    return (end && *end == 0) ? (int)x : dflt;
+}
+
 int check(tw_solver *s)
 {
     return s ? TW_OK : TW_ERR_INVALID;
@@ -742,6 +823,7 @@ const char *tw_strerror(int status)
     case TW_ERR_MODEL_BOUNDS: return "material interpolation outside the model";
     case TW_ERR_TOO_LARGE: return "model larger than the no-allocation scratch (TW_NOALLOC_MAX_MODEL_POINTS)";
     case TW_ERR_IO: return "file missing, unreadable, unwritable or malformed";
+    case TW_ERR_TIMEOUT: return "a wait inside a step kernel gave up (a staged copy did not arrive)";
     }
     return "unknown status";
 }
@@ -912,7 +994,44 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             s->n_int_seg = std::max(1, std::min(target, s->int_rows / 8));
             s->n_int_cta = (s->n_int_seg * s->n_wstrip + FS_WARPS - 1) / FS_WARPS;
         }
-        const int nctas = s->n_int_cta + s->n_zone * s->n_bstrip;
+        // the TMA-staged step (tma_step.cuh): FP32 fields and coefficients, plain update, the
+        // reference's x ends, a handle of its own (not a linked slab), at least one TMA strip.
+        // TW_TMA=1 in the environment selects it (default: the per-warp kernel);
+        // TW_TMA_CTAS_PER_SM sets the CTAs of work per SM its row segmentation aims at.
+        const int nts = tma_strips(My);
+        if (d.precision == TW_FP32 && d.cpst == TW_CPST_00 && !d.coef_fp16 && !s->slab && !(s->bnd & BND_X_IF) &&
+            s->n_int_seg > 0 && nts > 0 && env_int("TW_TMA", 0) != 0) {
+            int n_sm = 148;
+            cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, d.device);
+            s->tma = true;
+            s->n_tstrip = nts;
+            s->y_tma_end = TMA_Y0 + TMA_CORE * nts;
+            // warp strips: the first at column 0, the others from y_tma_end to the seam column My
+            s->n_ostrip = 1 + (int)((My + 1 - s->y_tma_end + FS_WARP_CORE - 1) / FS_WARP_CORE);
+            const int per_sm = std::max(1, env_int("TW_TMA_CTAS_PER_SM", 8));
+            const int max_seg = std::max(1, s->int_rows / 8);
+            s->n_tseg = std::max(1, std::min(max_seg, (n_sm * per_sm + nts / 2) / nts));
+            s->n_int_seg = std::max(1, std::min(max_seg, 2 * s->n_tseg));
+            s->n_int_cta = (s->n_int_seg * s->n_ostrip + FS_WARPS - 1) / FS_WARPS;
+            s->n_tcta = s->n_tseg * s->n_tstrip;
+            e = prepare_tma<float, float>();
+            if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
+            s->tmaps = new (std::nothrow) TmaMaps[2];
+            if (!s->tmaps) return fail(TW_ERR_NOMEM);
+            // maps by field slot: the fields of buffer `par`, the coefficients, the energy weights
+            const int fmap[5] = {TM_NN, TM_MN, TM_NM, TM_MM0, TM_MM1};
+            const int cmap[5] = {TM_MU, TM_PMN, TM_PNM, TM_LAM, TM_M2};
+            const int wmap[5] = {TM_WNN, TM_WMN, TM_WNM, TM_WM3, TM_WM4};
+            for (int par = 0; par < 2; par++)
+                for (int k = 0; k < 5; k++) {
+                    TmaMaps &m = s->tmaps[par];
+                    if ((rc_ = encode_rows(m.m[fmap[k]], par ? s->f2[k] : s->f[k], false, s->rows[k], s->pitch)) != TW_OK ||
+                        (rc_ = encode_rows(m.m[cmap[k]], s->coef[k], false, s->rows[k], s->pitch)) != TW_OK ||
+                        (rc_ = encode_rows(m.m[wmap[k]], s->w[k], true, s->rows[k], s->pitch)) != TW_OK)
+                        return fail(rc_);
+                }
+        }
+        const int nctas = s->n_int_cta + s->n_zone * s->n_bstrip + s->n_tcta;
         if ((rc_ = s->alloc((void **)&s->d_done, sizeof(int))) != TW_OK) return fail(rc_);
         cudaMemsetAsync(s->d_done, 0, sizeof(int), s->st);
         if ((rc_ = s->alloc((void **)&s->d_rcv_off, sizeof(int) * (nctas + 1))) != TW_OK) return fail(rc_);
@@ -1220,7 +1339,8 @@ int tw_sync(tw_solver *s)
     int flags = 0;
     TW_CUDA(cudaMemcpyAsync(&flags, s->d_flags, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     TW_CUDA(cudaStreamSynchronize(s->st));
-    if (flags & FLAG_NONFINITE) s->sticky = TW_ERR_NONFINITE;
+    if (flags & FLAG_TIMEOUT) s->sticky = TW_ERR_TIMEOUT;
+    else if (flags & FLAG_NONFINITE) s->sticky = TW_ERR_NONFINITE;
     else if (flags & FLAG_RECORD_FULL) s->sticky = TW_ERR_RECORD_FULL;
     return s->sticky;
 }
@@ -1477,6 +1597,9 @@ int tw_data_misfit(tw_solver *s, const double *obs, double *total, double *per_r
         const int rc = tw_read_receivers(s, tr.data());
         if (rc != TW_OK) return rc;
     }
+    // the reference keeps records and observations in its storage precision and squares their
+    // difference in double: pow((double)(RESULT - record), 2) (forward.cpp:436-437)
+    const bool f32 = s->d.precision == TW_FP32;
     double J = 0.;
     for (int r = 0; r < n; r++) {
         double Jr = 0.;   // sum over steps and the grid's fields, in the reference's order
@@ -1484,7 +1607,8 @@ int tw_data_misfit(tw_solver *s, const double *obs, double *total, double *per_r
         for (int it = 0; it < nt; it++)
             for (int f = 0; f < nf; f++) {
                 const size_t i = (2 * (size_t)r + f) * nt + it;
-                Jr += (tr[i] - obs[i]) * (tr[i] - obs[i]);
+                const double d = f32 ? (double)((float)tr[i] - (float)obs[i]) : tr[i] - obs[i];
+                Jr += std::pow(d, 2);
             }
         if (per_rcv) per_rcv[r] = Jr;
         J += Jr;

@@ -15,7 +15,7 @@ namespace tw {
 
 enum { G_NN = 0, G_MN = 1, G_NM = 2, G_MM = 3 };
 enum { F_NN = 0, F_MN = 1, F_NM = 2, F_MM0 = 3, F_MM1 = 4 };
-enum { FLAG_NONFINITE = 1, FLAG_RECORD_FULL = 2 };
+enum { FLAG_NONFINITE = 1, FLAG_RECORD_FULL = 2, FLAG_TIMEOUT = 4 };
 
 template <class S, class C>
 struct StepArgs {
