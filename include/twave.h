@@ -278,6 +278,20 @@ TW_API int tw_slab_run(tw_solver *const *slabs, int n, int steps);
 TW_API int tw_adjoint_gradient(tw_solver *s, int nt, const double *obs, int ckpt_every, double *misfit,
                                double *const *g_grid, double *g_rho, double *g_vp, double *g_vs,
                                double *const *g_state);
+/* The same gradient with binomial checkpointing (the revolve schedule family of Griewank and
+ * Walther) in `slots` states: reversing n steps with c free slots advances a = min(n - 1,
+ * C(c + t - 1, c)) steps into a slot, t the smallest number with C(c + t, c) >= n, and recurses on
+ * both parts; the first advances are the forward sweep itself (traces and energies recorded once).
+ * Device memory: slots + 5 states plus 15 field-sized arrays, for any nt; the forward steps taken
+ * grow as memory shrinks (tw_revolve_plan). The gradient equals tw_adjoint_gradient's for any
+ * slot count. No counterpart in the reference (it has no adjoint). */
+TW_API int tw_adjoint_gradient_revolve(tw_solver *s, int nt, const double *obs, int slots, double *misfit,
+                                       double *const *g_grid, double *g_rho, double *g_vp, double *g_vs,
+                                       double *const *g_state);
+/* The schedule of tw_adjoint_gradient_revolve alone (host only, no GPU): the forward steps it
+ * takes for nt steps in `slots` states, and its number of actions; the schedule is replayed on
+ * labels and checked (every adjoint step n meets the forward states n and n + 1). */
+TW_API int tw_revolve_plan(int nt, int slots, long *forward_steps, int *n_actions);
 
 /* Data misfit of the recorded traces against observed ones: calculate_data_misfit
  * (forward.cpp:414-445), sum over steps and fields of (trace - obs)^2 per receiver (no factor

@@ -53,29 +53,54 @@ def random_state(case, seed):
     return [rng.standard_normal(s) for s in [(Mx + 1, My + 1), (Mx, My + 1), (Mx + 1, My), (Mx, My), (Mx, My)]]
 
 
-@pytest.mark.parametrize("nt,K", [(1, 1), (30, 7), (30, 50)])
-def test_dot_product_identity_of_the_state_map(nt, K):
+class StateMap:
+    """The linear map from the initial fields to the traces (no source) and its transpose by the
+    adjoint, for the autograd wrapper Traces (adjoint_torch.py)."""
+
+    def __init__(self, tw, case, nt, K=0, slots=0):
+        self.tw, self.case, self.nt, self.K, self.slots = tw, case, nt, K, slots
+        self.keys = [(tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)]
+        self.misfit = None
+
+    def _handle(self, x):
+        s = solver(self.tw, self.case, source=False)
+        for (g, f), a in zip(self.keys, x):
+            s.write_field(g, f, a)
+        return s
+
+    def forward(self, x):
+        s = self._handle(x)
+        s.run(self.nt)
+        d = s.read_receivers()
+        s.close()
+        return d
+
+    def transpose(self, x, obs):
+        s = self._handle(x)
+        out = s.adjoint_gradient(self.nt, obs, ckpt_every=max(self.K, 1), model=False, state=True, slots=self.slots)
+        s.close()
+        self.misfit = out["misfit"]
+        return [out["state"][k] for k in KEYS]
+
+
+@pytest.mark.parametrize("nt,K,slots", [(1, 1, 0), (30, 7, 0), (30, 50, 0), (30, 0, 1), (30, 0, 4)])
+def test_dot_product_identity_of_the_state_map(nt, K, slots):
+    """<L x, y> = <x, L^T y> with L^T y from autograd's vector-Jacobian product of the traces."""
+    import torch
+    from adjoint_torch import Traces
     tw = load_twave()
     Mx, My, den = 24, 20, 24
     case = elastic_case(Mx, My, seed=3, Nt=nt, den_dx=den, rcvs=rcvs_for(Mx, My, den))
-    x = random_state(case, 1)
-    slots = [(tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)]
-    s = solver(tw, case, source=False)
-    for (g, f), a in zip(slots, x):
-        s.write_field(g, f, a)
-    s.run(nt)
-    d = s.read_receivers()
-    s.close()
-    y = np.random.default_rng(2).standard_normal(d.shape) * single_field_mask(tw, case)
-    s = solver(tw, case, source=False)
-    for (g, f), a in zip(slots, x):
-        s.write_field(g, f, a)
-    out = s.adjoint_gradient(nt, d - y, ckpt_every=K, model=False, state=True)
-    s.close()
-    lhs = float(np.sum(d * y))
-    rhs = float(sum(np.sum(a * out["state"][k]) for a, k in zip(x, KEYS)))
-    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), np.sqrt(np.sum(d * d) * np.sum(y * y)))
-    assert abs(out["misfit"] - 0.5 * np.sum(y * y)) <= 1e-12 * np.sum(y * y)
+    x = [torch.from_numpy(a).requires_grad_(True) for a in random_state(case, 1)]
+    runner = StateMap(tw, case, nt, K=K, slots=slots)
+    d = Traces.apply(*x, runner)
+    y = torch.from_numpy(np.random.default_rng(2).standard_normal(tuple(d.shape)) * single_field_mask(tw, case))
+    g = torch.autograd.grad(d, x, grad_outputs=y)
+    lhs = float(torch.sum(d * y))
+    rhs = float(sum(torch.sum(a * b) for a, b in zip(x, g)))
+    dd, yy = float(torch.sum(d * d)), float(torch.sum(y * y))
+    assert abs(lhs - rhs) <= 1e-12 * max(abs(lhs), np.sqrt(dd * yy))
+    assert abs(runner.misfit - 0.5 * yy) <= 1e-12 * yy
 
 
 def _misfit_case():
@@ -107,14 +132,23 @@ def test_gradient_matches_central_differences():
         h.close()
         return 0.5 * float(np.sum((t - obs) ** 2))
 
-    s = solver(tw, case)
-    g = s.adjoint_gradient(nt, obs, ckpt_every=25)
-    s.close()
-    assert abs(g["misfit"] - J(rho, vp, vs)) <= 1e-12 * g["misfit"]
+    import torch
+    from adjoint_torch import Misfit
+
+    def runner(r, p, q):
+        h = solver(tw, case, rho=r, vp=p, vs=q)
+        out = h.adjoint_gradient(nt, obs, ckpt_every=25)
+        h.close()
+        return out["misfit"], out
+
+    m = [torch.from_numpy(a.copy()).requires_grad_(True) for a in (rho, vp, vs)]
+    Jt = Misfit.apply(*m, runner)
+    grads = torch.autograd.grad(Jt, m)
+    assert abs(float(Jt) - J(rho, vp, vs)) <= 1e-12 * float(Jt)
     rng = np.random.default_rng(5)
     for k in range(8):
         d = [rng.standard_normal(shp) * a for a in (rho, vp, vs)]   # relative perturbation directions
-        ana = sum(float(np.sum(gg * dd)) for gg, dd in zip((g["rho"], g["vp"], g["vs"]), d))
+        ana = sum(float(torch.sum(gg * torch.from_numpy(dd))) for gg, dd in zip(grads, d))
         err = {}
         for eps in (1e-3, 1e-4):
             fd = (J(rho + eps * d[0], vp + eps * d[1], vs + eps * d[2]) -
@@ -167,3 +201,121 @@ def test_adjoint_rejections():
         s.adjoint_gradient(10, obs)
     assert e.value.code == -10
     s.close()
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_revolve_schedule_gives_the_same_gradient(prec):
+    """Binomial checkpointing in 1, 2, 3, 7 and nt state slots against checkpoints every 13 steps:
+    the same forward states reach every adjoint step, so the per-grid gradients are bit-identical
+    and the node gradients (FP64 atomics) equal to 1e-12; the handle ends as after tw_step(nt)."""
+    tw = load_twave()
+    case = _misfit_case()
+    nt = case.Nt
+    ref = solver(tw, case, precision=prec)
+    ref.run(nt)
+    traces = ref.read_receivers()
+    fields = [ref.read_field(g, f) for g, f in ((tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1))]
+    ref.close()
+    obs = traces * 0.9
+    s = solver(tw, case, precision=prec)
+    want = s.adjoint_gradient(nt, obs, ckpt_every=13)
+    s.close()
+    for slots in (1, 2, 3, 7, nt):
+        s = solver(tw, case, precision=prec)
+        got = s.adjoint_gradient(nt, obs, slots=slots)
+        assert s.info().steps_done == nt
+        assert np.array_equal(s.read_receivers(), traces)
+        for (gr, f), a in zip(((tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)), fields):
+            assert np.array_equal(s.read_field(gr, f), a)
+        s.close()
+        assert got["misfit"] == want["misfit"]
+        for k, v in got["grid"].items():
+            assert np.array_equal(v, want["grid"][k]), (slots, k)
+        for k in ("rho", "vp", "vs"):
+            assert np.abs(got[k] - want[k]).max() <= 1e-12 * np.abs(want[k]).max(), (slots, k)
+
+
+@pytest.mark.parametrize("slots", [0, 3])
+def test_recomputed_steps_leave_the_energy_records_alone(slots):
+    """With the energy on, the gradient call's records equal a plain run's: steps recomputed from
+    checkpoints add nothing to them."""
+    tw = load_twave()
+    case = _misfit_case()
+    nt = case.Nt
+    shp = (case.Mx + 2, case.My + 2)
+
+    def make():
+        h = tw.Solver(case.Mx, case.My, case.num_dx, case.den_dx, case.dt, precision="f64", central_f=case.central_f,
+                      time_delay=case.time_delay, max_steps=nt, energy=True)
+        h.set_material_model(case.rho.reshape(shp), case.vp.reshape(shp), case.vs.reshape(shp))
+        h.set_source_location(*case.src)
+        for r in case.rcvs:
+            h.add_receiver_location(*r)
+        return h
+    h = make()
+    h.run(nt)
+    want = h.read_energy()
+    obs = h.read_receivers() * 0.9
+    h.close()
+    h = make()
+    h.adjoint_gradient(nt, obs, ckpt_every=11, slots=slots)
+    got = h.read_energy()
+    h.close()
+    for a, b in zip(got, want):
+        assert np.abs(a - b).max() <= 1e-12 * np.abs(b).max()
+
+
+def test_gradient_at_the_c5_size_matches_central_differences():
+    """The C5 configuration's grid and length in FP64 (1024 x 1024, 2000 steps, one of its shots on
+    row 16, 256 receivers on NM row 4, the layered medium with observed data from the 5 % anomaly):
+    central differences of the misfit along 3 random relative directions at h = 1e-3 and 5e-4, and
+    their Richardson extrapolation (4 D(h/2) - D(h)) / 3, which removes the h^2 truncation term,
+    against the adjoint value from autograd (Misfit wrapper)."""
+    import torch
+    import bench
+    from adjoint_torch import Misfit
+    tw = load_twave()
+    n, nt = bench.ADJ_N, 2000
+    rho, vp, vs, bump = bench.adjoint_media()
+    dt = bench.CFL * (1.0 / bench.DEN_DX) / (np.sqrt(2.0) * (vp * bump).max())
+    rx, ry = np.full(256, 4), 4 * np.arange(256)
+
+    def run(r, p, q, adjoint_obs=None):
+        h = tw.Solver(n, n, 1, bench.DEN_DX, dt, precision="f64", central_f=bench.F0, time_delay=bench.DELAY,
+                      max_steps=nt, energy=False)
+        h.set_material_model(r, p, q)
+        h.set_source(tw.MM, 16, 512)
+        h.add_receivers(tw.NM, rx, ry)
+        if adjoint_obs is not None:
+            out = h.adjoint_gradient(nt, adjoint_obs, ckpt_every=50)
+            h.close()
+            return out
+        h.run(nt)
+        t = h.read_receivers()
+        h.close()
+        return t
+
+    obs = run(rho, vp * bump, vs * bump)
+
+    def J(r, p, q):
+        return 0.5 * float(np.sum((run(r, p, q) - obs) ** 2))
+
+    def runner(r, p, q):
+        out = run(r, p, q, adjoint_obs=obs)
+        return out["misfit"], out
+
+    m = [torch.from_numpy(a.copy()).requires_grad_(True) for a in (rho, vp, vs)]
+    grads = torch.autograd.grad(Misfit.apply(*m, runner), m)
+    rng = np.random.default_rng(bench.ADJ_SEED + 1)
+    for k in range(3):
+        d = [rng.standard_normal(rho.shape) * a for a in (rho, vp, vs)]
+        ana = sum(float(torch.sum(g * torch.from_numpy(dd))) for g, dd in zip(grads, d))
+
+        def D(h):
+            return (J(rho + h * d[0], vp + h * d[1], vs + h * d[2]) - J(rho - h * d[0], vp - h * d[1], vs - h * d[2])) / (2 * h)
+        d1, d2 = D(1e-3), D(5e-4)
+        rich = (4 * d2 - d1) / 3
+        e1, e2, er = (abs(v - ana) / abs(ana) for v in (d1, d2, rich))
+        print(f"direction {k}: rel err h=1e-3 {e1:.3e}, h=5e-4 {e2:.3e}, Richardson {er:.3e}")
+        assert e2 <= e1 * 0.35 + 1e-9          # second-order convergence of the differences
+        assert er <= 1e-4, (k, e1, e2, er)      # the extrapolated difference agrees with the adjoint

@@ -106,6 +106,8 @@ def lib() -> C.CDLL:
                                               C.c_int, C.c_int, vp, vp, vp, vp, vp, vp]
         L.tw_location_to_index.argtypes = [C.c_char, C.c_long, C.c_long, C.c_int, C.c_int, lp]
         L.tw_adjoint_gradient.argtypes = [vp, C.c_int, dp, C.c_int, dp, C.POINTER(dp), dp, dp, dp, C.POINTER(dp)]
+        L.tw_adjoint_gradient_revolve.argtypes = [vp, C.c_int, dp, C.c_int, dp, C.POINTER(dp), dp, dp, dp, C.POINTER(dp)]
+        L.tw_revolve_plan.argtypes = [C.c_int, C.c_int, lp, C.POINTER(C.c_int)]
         L.tw_io_read_input.argtypes = [C.c_char_p, C.POINTER(IoInput)]
         L.tw_io_read_srcrcv.argtypes = [C.c_char_p, C.c_void_p, C.c_int, C.POINTER(C.c_int)]
         L.tw_io_read_model.argtypes = [C.c_char_p, C.c_long, C.c_long, dp]
@@ -177,6 +179,13 @@ def io_read_model(path: str, Mx_prmt: int, My_prmt: int) -> np.ndarray:
 def release_cached_memory(device: int = 0):
     """Give the device memory that destroyed handles left in the per-device pool back to the driver."""
     _ok(lib().tw_release_cached_memory(device), "tw_release_cached_memory")
+
+
+def revolve_plan(nt: int, slots: int):
+    """(forward steps, actions) of the binomial checkpointing schedule (tw_revolve_plan; host only)."""
+    f, n = C.c_long(), C.c_int()
+    _ok(lib().tw_revolve_plan(nt, slots, C.byref(f), C.byref(n)), "tw_revolve_plan")
+    return f.value, n.value
 
 
 def location_to_index(gtype: str, num: int, den: int, num_dx: int, den_dx: int) -> int:
@@ -376,8 +385,10 @@ class Solver:
         _ok(lib().tw_profile(self.h, n, _dp(ms)), "tw_profile")
         return ms
 
-    def adjoint_gradient(self, nt: int, obs, ckpt_every: int = 50, model: bool = True, state: bool = False):
-        """Misfit and gradients (tw_adjoint_gradient). obs: [n_rcv, 2, nt]. Returns a dict with
+    def adjoint_gradient(self, nt: int, obs, ckpt_every: int = 50, model: bool = True, state: bool = False,
+                         slots: int = 0):
+        """Misfit and gradients (tw_adjoint_gradient; with slots > 0 tw_adjoint_gradient_revolve,
+        binomial checkpointing in that many states). obs: [n_rcv, 2, nt]. Returns a dict with
         "misfit", "grid" (NN mu, MN rho, NM rho, MM lambda, MM 2mu), and "rho", "vp", "vs" (padded
         node model, when model=True) and "state" (initial fields, when state=True)."""
         o = np.ascontiguousarray(np.asarray(obs, np.float64).reshape(self.n_rcv, 2, nt)) if self.n_rcv else np.zeros(1)
@@ -391,8 +402,9 @@ class Solver:
         st = [np.zeros(sh) for sh in shapes] if state else None
         sarr = (C.POINTER(C.c_double) * 5)(*[_dp(g) for g in st]) if state else None
         J = C.c_double()
-        _ok(lib().tw_adjoint_gradient(self.h, nt, _dp(o), ckpt_every, C.byref(J), garr,
-                                      *[(_dp(m) if m is not None else None) for m in mdl], sarr), "tw_adjoint_gradient")
+        fn, arg = (lib().tw_adjoint_gradient_revolve, slots) if slots > 0 else (lib().tw_adjoint_gradient, ckpt_every)
+        _ok(fn(self.h, nt, _dp(o), arg, C.byref(J), garr, *[(_dp(m) if m is not None else None) for m in mdl], sarr),
+            "tw_adjoint_gradient")
         out["misfit"] = J.value
         if model:
             out["rho"], out["vp"], out["vs"] = mdl

@@ -348,11 +348,13 @@ AcShot<S, C> acoustic_shot(const tw_solver *s, int parity)
     return a;
 }
 
-// one fused elastic step from the buffers fin (rin) into fout (rout)
+// one fused elastic step from the buffers fin (rin) into fout (rout); with_energy false: the step
+// adds nothing to the energy records (a recomputed step of the adjoint's checkpointing)
 template <class S, class C>
 void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *const *rin, void *const *rout,
-                      cudaStream_t st)
+                      cudaStream_t st, bool with_energy = true)
 {
+    const bool energy = with_energy && s->d.energy != 0;
     FusedArgs<S, C> a{};
     for (int k = 0; k < 5; k++) {
         a.in[k] = (const S *)fin[k];
@@ -412,11 +414,11 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
             a.n_ostrip = s->n_ostrip;
             a.n_octa = s->n_int_cta;
             a.y_tma_end = s->y_tma_end;
-            launch_tma<S, C>(a, s->tmaps[fin == s->f ? 0 : 1], s->d.energy != 0, st);
+            launch_tma<S, C>(a, s->tmaps[fin == s->f ? 0 : 1], energy, st);
             return;
         }
     }
-    launch_fused<S, C>(a, s->d.cpst, s->d.energy != 0, s->d.coef_fp16 != 0, st);
+    launch_fused<S, C>(a, s->d.cpst, energy, s->d.coef_fp16 != 0, st);
 }
 
 // one fused elastic step from the current buffers into the other ones
@@ -1797,18 +1799,179 @@ struct DevBuf {
     }
 };
 
+// ---- binomial checkpointing (revolve-style) with a fixed number of state slots
+//
+// Reversing n steps l..r-1 with the state at l in a slot and c free slots: advance a steps into a
+// free slot, reverse the upper part with c - 1 free slots, then the lower part with c (binomial
+// checkpointing, Griewank's revolve schedule family). Each adjoint step n needs the forward
+// states n and n + 1: the end state is made by one more forward step, unless a lower part of one
+// step finds it still in the slot the upper part started from. With no free slot every step's
+// states are recomputed from the slot. The first advance a minimises the forward steps
+// F(n, c) = min_a a + F(n - a, c - 1) + (a == 1 ? 0 : F(a, c)), F(1, c) = 1, F(n, 0) = n (n + 1) / 2,
+// by dynamic programming when the table is small (n^2 c <= 4e8); otherwise it is taken from the
+// binomial bound with s = c + 1 snapshots (the start state's included): t the smallest number with
+// C(s + t, s) >= n, a = max(C(s + t - 2, s), n - C(s - 1 + t, s - 1)), within a fraction of the
+// optimum.
+struct RvAction {
+    int kind;        // RV_FWD: advance state t0 by n steps from buffer a into buffer b;
+                     // RV_FIN: buffer a holds the final state (residuals, first injection);
+                     // RV_ADJ: adjoint step t0 with state t0 in a and t0 + 1 in b
+    int a, b, t0, n;
+};
+enum { RV_FWD = 0, RV_FIN = 1, RV_ADJ = 2 };
+
+long binom_capped(int c, int t, long cap)   // C(c + t, c), saturated above cap
+{
+    double v = 1.0;
+    for (int k = 1; k <= c; k++) {
+        v = v * (double)(t + k) / (double)k;
+        if (v > (double)cap) return cap + 1;
+    }
+    return (long)(v + 0.5);
+}
+
+// optimal first advances by dynamic programming (rows c = 0..cmax, columns n = 0..nmax)
+struct RvTable {
+    int nmax = 0, cmax = -1;
+    std::vector<long> F;
+    std::vector<int> A;
+    long &f(int n, int c) { return F[(size_t)c * (nmax + 1) + n]; }
+    int &a(int n, int c) { return A[(size_t)c * (nmax + 1) + n]; }
+    void build(int n_, int c_)
+    {
+        nmax = n_;
+        cmax = c_;
+        F.assign((size_t)(cmax + 1) * (nmax + 1), 0);
+        A.assign(F.size(), 1);
+        for (int c = 0; c <= cmax; c++)
+            for (int n = 1; n <= nmax; n++) {
+                if (n == 1) { f(n, c) = 1; continue; }
+                if (c == 0) { f(n, c) = (long)n * (n + 1) / 2; continue; }
+                long best = -1;
+                int arg = 1;
+                for (int a_ = 1; a_ < n; a_++) {
+                    const long v = a_ + f(n - a_, c - 1) + (a_ == 1 ? 0 : f(a_, c));
+                    if (best < 0 || v < best) { best = v; arg = a_; }
+                }
+                f(n, c) = best;
+                a(n, c) = arg;
+            }
+    }
+};
+
+struct RvPlan {
+    int nt, TA, TB;
+    bool fin_done = false;
+    std::vector<RvAction> acts;
+    RvTable *tab = nullptr;   // optimal advances, when computed
+    long first_advance(int n, int c)
+    {
+        if (tab && n <= tab->nmax && c <= tab->cmax) return tab->a(n, c);
+        const int s = c + 1;
+        int t = 1;
+        while (binom_capped(s, t, n) < n) t++;
+        const long lo = t >= 2 ? binom_capped(s, t - 2, n) : 0;
+        const long hi = binom_capped(s - 1, t, n);
+        return std::max(1L, std::min((long)n - 1, std::max(lo, (long)n - hi)));
+    }
+    void reverse(int l, int r, int p, std::vector<int> &free_slots)
+    {
+        const int n = r - l;
+        if (n == 1) {
+            acts.push_back({RV_FWD, p, TB, l, 1});
+            if (!fin_done && r == nt) { acts.push_back({RV_FIN, TB, 0, nt, 0}); fin_done = true; }
+            acts.push_back({RV_ADJ, p, TB, l, 0});
+            return;
+        }
+        const int c = (int)free_slots.size();
+        if (c == 0) {
+            for (int k = r - 1; k >= l; k--) {
+                int src = p;
+                if (k > l) { acts.push_back({RV_FWD, p, TA, l, k - l}); src = TA; }
+                acts.push_back({RV_FWD, src, TB, k, 1});
+                if (!fin_done && k + 1 == nt) { acts.push_back({RV_FIN, TB, 0, nt, 0}); fin_done = true; }
+                acts.push_back({RV_ADJ, src, TB, k, 0});
+            }
+            return;
+        }
+        const long a = first_advance(n, c);
+        const int m = l + (int)a, q = free_slots.back();
+        free_slots.pop_back();
+        acts.push_back({RV_FWD, p, q, l, (int)a});
+        reverse(m, r, q, free_slots);
+        if (a == 1) {   // the lower part is one step whose end state is still in slot q
+            acts.push_back({RV_ADJ, p, q, l, 0});
+            free_slots.push_back(q);
+            return;
+        }
+        free_slots.push_back(q);
+        reverse(l, m, p, free_slots);
+    }
+};
+
+// the action list for nt steps with `slots` state slots (slot 0 holds the initial state); buffers
+// 0..slots-1 are the slots, slots and slots + 1 two more states
+std::vector<RvAction> revolve_plan(int nt, int slots)
+{
+    RvPlan pl;
+    pl.nt = nt;
+    pl.TA = slots;
+    pl.TB = slots + 1;
+    std::vector<int> free_slots;
+    for (int k = slots - 1; k >= 1; k--) free_slots.push_back(k);
+    RvTable tab;
+    const int c = slots - 1;
+    if (c >= 1 && c < nt - 1 && (double)nt * nt * c <= 4e8) {
+        tab.build(nt, c);
+        pl.tab = &tab;
+    }
+    pl.reverse(0, nt, 0, free_slots);
+    return pl.acts;
+}
+
+// replay a plan on labels: every buffer read holds the state the action expects, the final state
+// is announced once before the first adjoint step, adjoint steps run nt - 1 down to 0 once each;
+// returns the forward steps taken, or -1
+long revolve_check(const std::vector<RvAction> &acts, int nt, int slots)
+{
+    std::vector<int> lab(slots + 2, -1);
+    lab[0] = 0;
+    long fwd = 0;
+    int next_adj = nt - 1;
+    bool fin = false;
+    for (const RvAction &x : acts) {
+        if (x.a < 0 || x.a >= slots + 2) return -1;
+        if (x.kind == RV_FWD) {
+            if (x.b < 0 || x.b >= slots + 2 || x.b == x.a || lab[x.a] != x.t0 || x.n < 1) return -1;
+            lab[x.b] = x.t0 + x.n;
+            fwd += x.n;
+        } else if (x.kind == RV_FIN) {
+            if (fin || lab[x.a] != nt || next_adj != nt - 1) return -1;
+            fin = true;
+        } else {
+            if (!fin || x.t0 != next_adj || lab[x.a] != x.t0 || lab[x.b] != x.t0 + 1) return -1;
+            next_adj--;
+        }
+    }
+    return (fin && next_adj == -1) ? fwd : -1;
+}
+
+// the gradient call. K > 0: checkpoints every K steps, each segment recomputed into a buffer of
+// K + 1 states; K == 0: binomial checkpointing in `slots` state slots
 template <class C>
-int adjoint_t(tw_solver *s, int nt, const double *obs, int K, double *misfit, double *const *g_grid, double *g_rho,
-              double *g_vp, double *g_vs, double *const *g_state)
+int adjoint_t(tw_solver *s, int nt, const double *obs, int K, int slots, double *misfit, double *const *g_grid,
+              double *g_rho, double *g_vp, double *g_vs, double *const *g_state)
 {
     const size_t fsz[5] = {(size_t)s->rows[0] * s->pitch, (size_t)s->rows[1] * s->pitch, (size_t)s->rows[2] * s->pitch,
                            (size_t)s->rows[3] * s->pitch, (size_t)s->rows[4] * s->pitch};
-    const int n_ck = (nt + K - 1) / K;
+    const bool periodic = K > 0;
+    const int n_ck = periodic ? (nt + K - 1) / K : 0;
     const int n_rcv = (int)(s->rcv_tab.size() / 4);
     DevBuf mem(s->st);
     int rc;
-    // checkpoints every K steps, the states of one segment, the final state
-    std::vector<std::array<void *, 5>> ck(n_ck), seg(K + 1);
+    // periodic: checkpoints every K steps and the states of one segment; revolve: the slots, two
+    // states of the plan and two scratch states for multi-step advances; both: the final state
+    std::vector<std::array<void *, 5>> ck(periodic ? n_ck : slots + 2), seg(periodic ? K + 1 : 2);
     std::array<void *, 5> fin{};
     AdjArgs<C> a{};
     double *d_res = nullptr, *gq[5] = {}, *nd = nullptr;
@@ -1836,35 +1999,6 @@ int adjoint_t(tw_solver *s, int nt, const double *obs, int K, double *misfit, do
         for (int k = 0; k < 5; k++) c[k] = cur_f(s, k);
         return c;
     };
-
-    // forward sweep, keeping a checkpoint every K steps
-    for (int c = 0; c < n_ck; c++) {
-        if ((rc = copy_state(s, ck[c].data(), cur().data())) != TW_OK) return rc;
-        const int n = std::min(K, nt - c * K);
-        enqueue(s, n, s->st);
-        s->steps_done += n;
-    }
-    if ((rc = copy_state(s, fin.data(), cur().data())) != TW_OK) return rc;
-    TW_CUDA(cudaGetLastError());
-    // residuals and misfit on the host (FP64)
-    std::vector<double> tr(2 * (size_t)n_rcv * nt), res(tr.size());
-    double J = 0.;
-    if (n_rcv > 0) {
-        TW_CUDA(cudaMemcpy2DAsync(tr.data(), sizeof(double) * nt, s->d_traces, sizeof(double) * s->d.max_steps,
-                                  sizeof(double) * nt, 2 * (size_t)n_rcv, cudaMemcpyDeviceToHost, s->st));
-        TW_CUDA(cudaStreamSynchronize(s->st));
-        for (int q = 0; q < n_rcv; q++)
-            for (int f = 0; f < 2; f++) {
-                const bool has = s->rcv_tab[4 * q + f] >= 0;
-                for (int it = 0; it < nt; it++) {
-                    const size_t i = (2 * (size_t)q + f) * nt + it;
-                    res[i] = has ? tr[i] - obs[i] : 0.;
-                    J += 0.5 * res[i] * res[i];
-                }
-            }
-        TW_CUDA(cudaMemcpyAsync(d_res, res.data(), sizeof(double) * res.size(), cudaMemcpyHostToDevice, s->st));
-    }
-    if (misfit) *misfit = J;
     a.pitch = s->pitch;
     a.Mx = (int)s->d.Mx;
     a.My = (int)s->d.My;
@@ -1873,27 +2007,94 @@ int adjoint_t(tw_solver *s, int nt, const double *obs, int K, double *misfit, do
     a.n_rcv = n_rcv;
     a.resid = d_res;
     a.nt = nt;
-
-    // backward sweep: lam_nt = R^T r_{nt-1}; per segment, recompute its states from the
-    // checkpoint, then step the adjoint back through it
-    launch_adjoint_inject<C>(a, nt - 1, s->st);
-    for (int c = n_ck - 1; c >= 0; c--) {
-        const int k0 = c * K, k1 = std::min(nt, k0 + K);
-        TW_CUDA(cudaMemcpyAsync(s->d_step, &k0, sizeof(int), cudaMemcpyHostToDevice, s->st));
-        if ((rc = copy_state(s, seg[0].data(), ck[c].data())) != TW_OK) return rc;
-        void *const none[5] = {};
-        for (int k = k0; k < k1; k++)   // step k: segment state k - k0 -> k - k0 + 1
-            enqueue_fused_io<C, C>(s, seg[k - k0].data(), seg[k - k0 + 1].data(), none, none, s->st);
-        for (int n = k1 - 1; n >= k0; n--) {
-            for (int k = 0; k < 5; k++) {
-                a.u0[k] = (const C *)seg[n - k0][k];
-                a.u1[k] = (const C *)seg[n + 1 - k0][k];
-            }
-            launch_adjoint_step<C>(a, s->st);
-            if (n >= 1) launch_adjoint_inject<C>(a, n - 1, s->st);
+    // residuals and misfit on the host (FP64) from the recorded traces, and the first injection
+    // lam_nt = R^T r_{nt-1}
+    double J = 0.;
+    auto residuals = [&]() -> int {
+        std::vector<double> tr(2 * (size_t)n_rcv * nt), res(tr.size());
+        if (n_rcv > 0) {
+            TW_CUDA(cudaMemcpy2DAsync(tr.data(), sizeof(double) * nt, s->d_traces, sizeof(double) * s->d.max_steps,
+                                      sizeof(double) * nt, 2 * (size_t)n_rcv, cudaMemcpyDeviceToHost, s->st));
+            TW_CUDA(cudaStreamSynchronize(s->st));
+            for (int q = 0; q < n_rcv; q++)
+                for (int f = 0; f < 2; f++) {
+                    const bool has = s->rcv_tab[4 * q + f] >= 0;
+                    for (int it = 0; it < nt; it++) {
+                        const size_t i = (2 * (size_t)q + f) * nt + it;
+                        res[i] = has ? tr[i] - obs[i] : 0.;
+                        J += 0.5 * res[i] * res[i];
+                    }
+                }
+            TW_CUDA(cudaMemcpyAsync(d_res, res.data(), sizeof(double) * res.size(), cudaMemcpyHostToDevice, s->st));
+            TW_CUDA(cudaStreamSynchronize(s->st));   // the host vector leaves scope
         }
+        launch_adjoint_inject<C>(a, nt - 1, s->st);
+        return TW_OK;
+    };
+    // one adjoint step n with the forward states n (u0) and n + 1 (u1), then the injection of n - 1
+    auto adjoint_step = [&](int n, void *const *u0, void *const *u1) {
+        for (int k = 0; k < 5; k++) {
+            a.u0[k] = (const C *)u0[k];
+            a.u1[k] = (const C *)u1[k];
+        }
+        launch_adjoint_step<C>(a, s->st);
+        if (n >= 1) launch_adjoint_inject<C>(a, n - 1, s->st);
+    };
+    void *const none[5] = {};
+
+    if (periodic) {
+        // forward sweep, keeping a checkpoint every K steps
+        for (int c = 0; c < n_ck; c++) {
+            if ((rc = copy_state(s, ck[c].data(), cur().data())) != TW_OK) return rc;
+            const int n = std::min(K, nt - c * K);
+            enqueue(s, n, s->st);
+            s->steps_done += n;
+        }
+        if ((rc = copy_state(s, fin.data(), cur().data())) != TW_OK) return rc;
         TW_CUDA(cudaGetLastError());
+        if ((rc = residuals()) != TW_OK) return rc;
+        // backward sweep: per segment, recompute its states from the checkpoint, then step the
+        // adjoint back through it
+        for (int c = n_ck - 1; c >= 0; c--) {
+            const int k0 = c * K, k1 = std::min(nt, k0 + K);
+            TW_CUDA(cudaMemcpyAsync(s->d_step, &k0, sizeof(int), cudaMemcpyHostToDevice, s->st));
+            if ((rc = copy_state(s, seg[0].data(), ck[c].data())) != TW_OK) return rc;
+            for (int k = k0; k < k1; k++)   // step k: segment state k - k0 -> k - k0 + 1 (recomputed: no energy)
+                enqueue_fused_io<C, C>(s, seg[k - k0].data(), seg[k - k0 + 1].data(), none, none, s->st, false);
+            for (int n = k1 - 1; n >= k0; n--) adjoint_step(n, seg[n - k0].data(), seg[n + 1 - k0].data());
+            TW_CUDA(cudaGetLastError());
+        }
+    } else {
+        // slot 0 holds the initial state; the plan's first forward steps are the forward sweep
+        // (traces and energies recorded once, at the steps not computed before), the rest
+        // recompute states from the slots
+        if ((rc = copy_state(s, ck[0].data(), cur().data())) != TW_OK) return rc;
+        const std::vector<RvAction> plan = revolve_plan(nt, slots);
+        if (revolve_check(plan, nt, slots) < 0) return TW_ERR_INVALID;   // (the plan is checked on labels)
+        auto buf = [&](int b) { return ck[b].data(); };
+        int hw = 0;   // steps [0, hw) have been computed once
+        for (const RvAction &x : plan) {
+            if (x.kind == RV_FWD) {
+                const bool first = x.t0 >= hw;   // (a forward advance is new or wholly recomputed)
+                TW_CUDA(cudaMemcpyAsync(s->d_step, &x.t0, sizeof(int), cudaMemcpyHostToDevice, s->st));
+                for (int k = 0; k < x.n; k++) {
+                    void *const *in = k == 0 ? buf(x.a) : seg[(k - 1) & 1].data();
+                    void *const *out = k == x.n - 1 ? buf(x.b) : seg[k & 1].data();
+                    enqueue_fused_io<C, C>(s, in, out, none, none, s->st, first);
+                }
+                if (first) hw = x.t0 + x.n;
+            } else if (x.kind == RV_FIN) {
+                if ((rc = copy_state(s, fin.data(), buf(x.a))) != TW_OK) return rc;
+                TW_CUDA(cudaGetLastError());
+                if ((rc = residuals()) != TW_OK) return rc;
+            } else {
+                adjoint_step(x.t0, buf(x.a), buf(x.b));
+            }
+            TW_CUDA(cudaGetLastError());
+        }
+        s->steps_done += nt;
     }
+    if (misfit) *misfit = J;
     // leave the handle as tw_step(nt) would: the final state, the step counter at nt
     if ((rc = copy_state(s, cur().data(), fin.data())) != TW_OK) return rc;
     TW_CUDA(cudaMemcpyAsync(s->d_step, &nt, sizeof(int), cudaMemcpyHostToDevice, s->st));
@@ -1950,13 +2151,10 @@ int adjoint_t(tw_solver *s, int nt, const double *obs, int K, double *misfit, do
     return TW_OK;
 }
 
-}  // namespace
-
-extern "C" int tw_adjoint_gradient(tw_solver *s, int nt, const double *obs, int ckpt_every, double *misfit,
-                                   double *const *g_grid, double *g_rho, double *g_vp, double *g_vs,
-                                   double *const *g_state)
+// the checks both gradient entry points share
+int adjoint_args(tw_solver *s, int nt, const double *obs, double *g_rho, double *g_vp, double *g_vs)
 {
-    if (check(s) || nt < 1 || ckpt_every < 1 || (!obs && !s->rcv_tab.empty())) return TW_ERR_INVALID;
+    if (check(s) || nt < 1 || (!obs && !s->rcv_tab.empty())) return TW_ERR_INVALID;
     if (!s->elastic || s->d.cpst != TW_CPST_00 || (s->d.precision != TW_FP64 && s->d.precision != TW_FP32) ||
         s->d.coef_fp16 || s->bnd)
         return TW_ERR_UNSUPPORTED;
@@ -1964,11 +2162,49 @@ extern "C" int tw_adjoint_gradient(tw_solver *s, int nt, const double *obs, int 
     if (s->steps_done != 0) return TW_ERR_STATE;   // the forward sweep starts at step 0
     if (nt > s->d.max_steps) return TW_ERR_RECORD_FULL;
     if ((g_rho || g_vp || g_vs) && !s->model_set) return TW_ERR_STATE;
+    return TW_OK;
+}
+
+}  // namespace
+
+extern "C" int tw_adjoint_gradient(tw_solver *s, int nt, const double *obs, int ckpt_every, double *misfit,
+                                   double *const *g_grid, double *g_rho, double *g_vp, double *g_vs,
+                                   double *const *g_state)
+{
+    int rc = adjoint_args(s, nt, obs, g_rho, g_vp, g_vs);
+    if (rc != TW_OK) return rc;
+    if (ckpt_every < 1) return TW_ERR_INVALID;
     TW_CUDA(cudaSetDevice(s->d.device));
     TW_CUDA(cudaStreamSynchronize(s->st));
     const int K = std::min(ckpt_every, nt);
-    return s->d.precision == TW_FP64 ? adjoint_t<double>(s, nt, obs, K, misfit, g_grid, g_rho, g_vp, g_vs, g_state)
-                                     : adjoint_t<float>(s, nt, obs, K, misfit, g_grid, g_rho, g_vp, g_vs, g_state);
+    return s->d.precision == TW_FP64 ? adjoint_t<double>(s, nt, obs, K, 0, misfit, g_grid, g_rho, g_vp, g_vs, g_state)
+                                     : adjoint_t<float>(s, nt, obs, K, 0, misfit, g_grid, g_rho, g_vp, g_vs, g_state);
+}
+
+extern "C" int tw_adjoint_gradient_revolve(tw_solver *s, int nt, const double *obs, int slots, double *misfit,
+                                           double *const *g_grid, double *g_rho, double *g_vp, double *g_vs,
+                                           double *const *g_state)
+{
+    int rc = adjoint_args(s, nt, obs, g_rho, g_vp, g_vs);
+    if (rc != TW_OK) return rc;
+    if (slots < 1) return TW_ERR_INVALID;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    TW_CUDA(cudaStreamSynchronize(s->st));
+    const int S = std::min(slots, nt);
+    return s->d.precision == TW_FP64 ? adjoint_t<double>(s, nt, obs, 0, S, misfit, g_grid, g_rho, g_vp, g_vs, g_state)
+                                     : adjoint_t<float>(s, nt, obs, 0, S, misfit, g_grid, g_rho, g_vp, g_vs, g_state);
+}
+
+extern "C" int tw_revolve_plan(int nt, int slots, long *forward_steps, int *n_actions)
+{
+    if (nt < 1 || slots < 1 || !forward_steps) return TW_ERR_INVALID;
+    const int S = std::min(slots, nt);
+    const std::vector<RvAction> plan = revolve_plan(nt, S);
+    const long f = revolve_check(plan, nt, S);
+    if (f < 0) return TW_ERR_INVALID;
+    *forward_steps = f;
+    if (n_actions) *n_actions = (int)plan.size();
+    return TW_OK;
 }
 
 // ======================================================================== batched shots
