@@ -155,79 +155,101 @@ class Dist:
 # ---------------------------------------------------------------- clocks during the timed region
 class ClockSampler:
     """SM clocks and clock-event reasons of one GPU, polled through NVML about every millisecond
-    by a background thread (reading only; nothing is set). `window(t0, t1)` summarises the
-    samples taken between two host times (time.perf_counter), so that a timed region of a few
-    milliseconds still carries samples; nvidia-smi at its fastest period (100 ms) is the fallback
-    when NVML cannot be loaded."""
-    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"),
-               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
-               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"),
-               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
-               ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown"))
+    by a separate process (reading only; nothing is set), each sample stamped with the system-wide
+    monotonic clock; `window(t0, t1)` summarises the samples between two time.monotonic() stamps
+    of this process, so that a timed region of a few milliseconds still carries samples (a thread
+    of this process would wait on the interpreter lock while the timed calls run). nvidia-smi at
+    its fastest period (100 ms) is the fallback when NVML cannot be loaded."""
+    CHILD = r"""
+import sys, time, pynvml as nv
+nv.nvmlInit()
+try:
+    h = nv.nvmlDeviceGetHandleByPciBusId(sys.argv[1])
+except Exception:
+    h = nv.nvmlDeviceGetHandleByIndex(int(sys.argv[2]))
+names = [("hw_slowdown", "nvmlClocksEventReasonHwSlowdown"), ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown"),
+         ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown"), ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap"),
+         ("hw_power_brake_slowdown", "nvmlClocksEventReasonHwPowerBrakeSlowdown")]
+masks = [(n, getattr(nv, c)) for n, c in names if hasattr(nv, c)]
+smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+while True:
+    t = time.monotonic()
+    sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+    print(t, sm, smax, ",".join(n for n, m in masks if r & m) or "-", flush=True)
+    time.sleep(0.001)
+"""
 
-    def __init__(self, device: int, period_s: float = 0.001):
+    def __init__(self, device: int):
         self.device = device
-        self.period = period_s
-        self.samples = []      # (host time, sm MHz, max sm MHz, [reason names])
-        self.thread = None
-        self.stop_flag = False
-        self.source = None
+        self.samples = []      # (monotonic time, sm MHz, max sm MHz, [reason names])
         self.proc = None
+        self.out = None
+        self.source = None
 
-    def _nvml_handle(self):
-        import pynvml
-        pynvml.nvmlInit()
+    def start(self):
         try:
             import torch
             p = torch.cuda.get_device_properties(self.device)
             bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
-            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
         except Exception:
-            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.device)
-
-    def _run(self, nv, h):
-        masks = [(name, getattr(nv, const)) for name, const in self.REASONS if hasattr(nv, const)]
-        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
-        while not self.stop_flag:
-            t = time.perf_counter()
-            try:
-                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
-                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
-                self.samples.append((t, float(sm), float(smax), [n for n, m in masks if r & m]))
-            except Exception:
-                pass
-            time.sleep(self.period)
-
-    def start(self):
-        import threading
+            bus = ""
+        self.out = tempfile.TemporaryFile(mode="w+")
         try:
-            nv, h = self._nvml_handle()
-            self.source = "nvml, ~1 ms period"
-            self.thread = threading.Thread(target=self._run, args=(nv, h), daemon=True)
-            self.thread.start()
-        except Exception:
-            self.source = "nvidia-smi, 100 ms period"
+            self.proc = subprocess.Popen([sys.executable, "-c", self.CHILD, bus, str(self.device)], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+            self.source = "nvml in a separate process, ~1 ms period"
+            t0 = time.monotonic()   # the timed region must not begin before sampling does
+            while time.monotonic() - t0 < 10.0 and self.proc.poll() is None:
+                self.out.seek(0, io.SEEK_END)
+                if self.out.tell() > 0:
+                    break
+                time.sleep(0.01)
+            if self.proc.poll() is not None:
+                raise OSError("nvml sampler exited")
+        except OSError:
+            self.proc = None
             self._start_smi()
 
     def _start_smi(self):
         q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        self.source = "nvidia-smi, 100 ms period"
+        self.out = tempfile.TemporaryFile(mode="w+")
         try:
-            self.out = tempfile.TemporaryFile(mode="w+")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
-                                         stdout=self.out, stderr=subprocess.DEVNULL)
-            self.t_smi = time.perf_counter()
+            self.smi = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                         "--format=csv,noheader,nounits", "-lms", "100"],
+                                        stdout=self.out, stderr=subprocess.DEVNULL)
+            self.t_smi = time.monotonic()
         except OSError:
-            self.proc = None
+            self.smi = None
+
+    def _refresh(self):
+        """Parse the complete lines the sampling process has written since the last call."""
+        if not self.proc:
+            return
+        self.out.seek(getattr(self, "_pos", 0))
+        text = self.out.read()
+        cut = text.rfind("\n") + 1
+        self._pos = getattr(self, "_pos", 0) + len(text[:cut].encode())
+        for line in text[:cut].splitlines():
+            f = line.split()
+            if len(f) != 4:
+                continue
+            try:
+                self.samples.append((float(f[0]), float(f[1]), float(f[2]), [] if f[3] == "-" else f[3].split(",")))
+            except ValueError:
+                pass
 
     def stop(self):
-        self.stop_flag = True
-        if self.thread:
-            self.thread.join()
         if self.proc:
             self.proc.terminate()
             self.proc.wait()
+            self._refresh()
+            self.proc = None
+        elif getattr(self, "smi", None):
+            self.smi.terminate()
+            self.smi.wait()
             self.out.seek(0)
             names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
             rows = [r for r in csv.reader(io.StringIO(self.out.read())) if len(r) >= 6]
@@ -243,6 +265,8 @@ class ClockSampler:
         region too short for `min_samples` samples is widened symmetrically, 10 ms at a time up
         to 200 ms on each side (the GPU is busy with the warm-up before it and the per-kernel
         timing after it), and the margin is reported."""
+        time.sleep(0.005)   # the samples just after the region
+        self._refresh()
         margin = 0.0
         inside = [x for x in self.samples if t0 <= x[0] <= t1]
         while len(inside) < min_samples and margin < 0.2:
@@ -409,14 +433,14 @@ def run_ours(args, dist: Dist):
     dist.barrier()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    th0 = time.perf_counter()
+    th0 = time.monotonic()
     e0.record(stream)
     s.step(K)
     e1.record(stream)
     e1.synchronize()
     s.sync()
     torch.cuda.synchronize()
-    th1 = time.perf_counter()
+    th1 = time.monotonic()
     dist.barrier()
     clk = clocks.window(th0, th1)
     ms = e0.elapsed_time(e1)
@@ -425,10 +449,16 @@ def run_ours(args, dist: Dist):
     value = updates / (ms_max / 1e3) / 1e9
 
     # per-kernel durations (CUDA events around each launch on the solver's stream)
+    info = s.info()
     prof = s.profile(P)
-    if prof[1] == 0.0:
-        # fused path: the whole step is one launch; compulsory bytes = 5 fields read and written
-        # once + 5 coefficients read once = 60 B per cell in FP32
+    if info.step_kind == 2:
+        # TMA-staged step: two launches side by side (the TMA strips and the boundary / seam
+        # CTAs), timed together; compulsory bytes = 5 fields read and written once + 5
+        # coefficients read once = 60 B per cell in FP32
+        name, alg, ms_k = "k_elastic_tma + k_elastic_side (one step)", MX * MY * 60, float(prof[0])
+        launches_per_step = 2
+    elif prof[1] == 0.0:
+        # fused path: the whole step is one launch
         name, alg, ms_k = "k_elastic_fused", MX * MY * 60, float(prof[0])
         launches_per_step = 1
     else:
@@ -439,8 +469,9 @@ def run_ours(args, dist: Dist):
         launches_per_step = 3
     achieved = alg / (ms_k / 1e3) / 1e9
     peak, peak_note = measured_peaks()
+    tkey = "tma_step@2048" if info.step_kind == 2 else name
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": ncu_traffic(name), "kernel": name, "peak_source": peak_note,
+                "traffic": ncu_traffic(tkey), "kernel": name, "peak_source": peak_note,
                 "algorithmic_bytes_per_launch": alg, "ms_per_launch": ms_k,
                 "ms_per_launch_all": [float(x) for x in prof], "step_bytes_algorithmic_per_update": 60,
                 "frac_of_step_time": alg / (ms_max / K / 1e3) / 1e9 / peak}
@@ -483,13 +514,13 @@ def run_e2e(args, dist: Dist, tw, torch, clocks, model):
     K = args.steps
     dev = dist.local
 
-    t0 = time.perf_counter()
+    t0 = time.monotonic()
     pins = []
     for a in (rho, vp, vs):   # the caller's model in pinned host memory (staged once, reported)
         t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
         t.numpy()[...] = a
         pins.append(t)
-    staging_s = time.perf_counter() - t0
+    staging_s = time.monotonic() - t0
     host = [p.numpy() for p in pins]
 
     def one_pass(breakdown: bool):
@@ -498,8 +529,8 @@ def run_e2e(args, dist: Dist, tw, torch, clocks, model):
         def mark(name):
             if breakdown:
                 torch.cuda.synchronize(dev)
-                marks.append((name, time.perf_counter()))
-        t0 = time.perf_counter()
+                marks.append((name, time.monotonic()))
+        t0 = time.monotonic()
         s2 = tw.Solver(MX, MY, 1, DEN_DX, dt, physics=tw.ELASTIC, precision="f32", cpst="00", central_f=F0,
                        time_delay=DELAY, max_steps=K, energy=True, device=dev)
         mark("create")
@@ -510,11 +541,11 @@ def run_e2e(args, dist: Dist, tw, torch, clocks, model):
         mark("source table and receivers")
         s2.step(K)
         if breakdown:
-            marks.append(("steps enqueued (graph capture and launches, host side)", time.perf_counter()))
+            marks.append(("steps enqueued (graph capture and launches, host side)", time.monotonic()))
         mark("steps run (energy every step)")
         traces = s2.read_receivers()
         energy = s2.read_energy()
-        t1 = time.perf_counter()
+        t1 = time.monotonic()
         mark("trace and energy readback")
         s2.close()
         phases = {}
@@ -527,9 +558,9 @@ def run_e2e(args, dist: Dist, tw, torch, clocks, model):
     one_pass(False)
     torch.cuda.synchronize()
     dist.barrier()
-    th0 = time.perf_counter()
+    th0 = time.monotonic()
     secs, traces, energy, _ = one_pass(False)
-    th1 = time.perf_counter()
+    th1 = time.monotonic()
     clk = clocks.window(th0, th1)
     _, _, _, phases = one_pass(True)
     del pins, host
@@ -559,24 +590,28 @@ def run_target_8192(args, tw, torch, clocks, dev: int):
     s.run(W)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    th0 = time.perf_counter()
+    th0 = time.monotonic()
     e0.record(stream)
     s.step(T)
     e1.record(stream)
     e1.synchronize()
     s.sync()
-    th1 = time.perf_counter()
+    th1 = time.monotonic()
     ms = e0.elapsed_time(e1)
+    tma = s.info().step_kind == 2
     prof = s.profile(8)
     s.close()
     peak, peak_note = measured_peaks()
     alg = n * n * 60
     ms_k = float(prof[0])
+    kname = "k_elastic_tma + k_elastic_side (one step)" if tma else "k_elastic_fused"
     return {"workload": f"elastic {n}x{n} FP32, the same 8-layer medium, energy off, 16 receivers",
             "steps": T, "warmup": W, "ms_per_step": ms / T, "gpts": n * n * T / (ms / 1e3) / 1e9,
-            "roofline": {"kernel": "k_elastic_fused", "algorithmic_bytes_per_launch": alg, "ms_per_launch": ms_k,
+            "roofline": {"kernel": kname, "algorithmic_bytes_per_launch": alg, "ms_per_launch": ms_k,
                          "achieved": alg / (ms_k / 1e3) / 1e9, "peak": peak, "peak_source": peak_note,
-                         "frac": alg / (ms_k / 1e3) / 1e9 / peak, "traffic": ncu_traffic("k_elastic_fused@8192")},
+                         "frac": alg / (ms_k / 1e3) / 1e9 / peak,
+                         "frac_of_step_time": alg / (ms / T / 1e3) / 1e9 / peak,
+                         "traffic": ncu_traffic("tma_step@8192" if tma else "k_elastic_fused@8192")},
             "clocks": clocks.window(th0, th1), "l2": "inputs far larger than L2 (4 GB a step), no flush"}
 
 
@@ -725,10 +760,10 @@ def run_batch(args):
         s.run(warm)
         s.reset()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    t0 = time.monotonic()
     for s in shots:
         s.run(K)
-    t_seq = time.perf_counter() - t0
+    t_seq = time.monotonic() - t0
     seq_traces = [s.read_receivers() for s in shots]
     for s in shots:
         s.reset()
@@ -741,9 +776,9 @@ def run_batch(args):
     clocks = ClockSampler(0)
     clocks.start()
     torch.cuda.synchronize()
-    t0 = time.perf_counter()
+    t0 = time.monotonic()
     b.run(K)
-    t1 = time.perf_counter()
+    t1 = time.monotonic()
     t_bat = t1 - t0
     clocks.stop()
     clk = clocks.window(t0, t1)
@@ -903,9 +938,9 @@ def run_adjoint(args):
     for src, o in zip(shots, obs):
         s = make("f32", rho, vp, vs, src)
         torch.cuda.synchronize()
-        t0 = time.perf_counter()
+        t0 = time.monotonic()
         out = s.adjoint_gradient(K, o, ckpt_every=50)
-        t_grad += time.perf_counter() - t0
+        t_grad += time.monotonic() - t0
         s.close()
         J0 += out["misfit"]
         for k in g:

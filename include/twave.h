@@ -106,6 +106,10 @@ typedef struct {
     long row_off;                  /* a slab: global row of its local row 0 (0 otherwise) */
     long own_rows[2];              /* a slab: the global rows [own_rows[0], own_rows[1]) it owns */
     long Mx_glob;                  /* cells along x of the whole grid */
+    int step_kind;                 /* how a step runs: 0 the per-point kernels (three or more launches),
+                                      1 the one-launch fused step, 2 the TMA-staged step (two launches
+                                      side by side), 3 the fused periodic acoustic step */
+    int launches_per_step;         /* kernels one step launches */
 } tw_info;
 
 typedef struct tw_solver tw_solver;

@@ -51,7 +51,8 @@ class GridDesc(C.Structure):
 class Info(C.Structure):
     _fields_ = [("rows", C.c_long * 4), ("cols", C.c_long * 4), ("pitch", C.c_long), ("steps_done", C.c_int),
                 ("n_rcv", C.c_int), ("bytes_per_update", C.c_double), ("device_bytes", C.c_double),
-                ("row_off", C.c_long), ("own_rows", C.c_long * 2), ("Mx_glob", C.c_long)]
+                ("row_off", C.c_long), ("own_rows", C.c_long * 2), ("Mx_glob", C.c_long),
+                ("step_kind", C.c_int), ("launches_per_step", C.c_int)]
 
 
 _lib = None

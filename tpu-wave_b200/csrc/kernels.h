@@ -169,6 +169,9 @@ struct FusedArgs {
     int n_tseg, n_tstrip, n_tcta;
     int n_oseg, n_ostrip, n_octa;
     int y_tma_end;
+    int *work;                // the TMA strips' next work item (a persistent CTA takes items until
+                              // n_tcta are taken; zero between steps)
+    int n_all_ctas;           // CTAs of both launches of the TMA-staged step
 };
 template <class S, class C>
 void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, bool coef16, cudaStream_t st);
@@ -189,8 +192,10 @@ enum { TM_NN = 0, TM_MN, TM_NM, TM_MM0, TM_MM1, TM_PMN, TM_PNM, TM_MU, TM_LAM, T
 int tma_strips(long My);
 template <class S, class C>
 cudaError_t prepare_tma();
+// st: the handle's stream; side: a second stream of the handle; fork, join: two events of it
 template <class S, class C>
-void launch_tma(const FusedArgs<S, C> &a, const TmaMaps &maps, bool energy, cudaStream_t st);
+void launch_tma(FusedArgs<S, C> a, const TmaMaps &maps, bool energy, cudaStream_t st, cudaStream_t side,
+                cudaEvent_t fork, cudaEvent_t join);
 
 // free y ends on the fused step (ysat_fix.cu): the fused kernel steps every column with the
 // periodic y rule; these two launches then recompute, from the step's input buffers, the points

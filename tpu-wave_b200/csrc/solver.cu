@@ -134,6 +134,8 @@ struct tw_solver {
     bool tma = false;
     int n_tseg = 0, n_tstrip = 0, n_tcta = 0, n_ostrip = 0, y_tma_end = 0;
     TmaMaps *tmaps = nullptr;
+    cudaStream_t st_side = nullptr;   // the side launch's stream, forked from st and joined back
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int ir0 = FS_ZONE, zone_kind[2] = {0, 1};
     // a slab of a larger grid (slab decomposition along x): local row r is global row r + row_off
     // of a grid of Mx_glob cells; it owns global rows [own0, own1) of every grid (plus the last
@@ -202,6 +204,9 @@ tw_solver::~tw_solver()
     release(d_traces); release(d_energy);
     cudaStreamSynchronize(st);   // the buffers are back in the pool before the next handle asks
     cudaStreamDestroy(st);
+    if (st_side) cudaStreamDestroy(st_side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
 }
 
 namespace {
@@ -414,7 +419,8 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
             a.n_ostrip = s->n_ostrip;
             a.n_octa = s->n_int_cta;
             a.y_tma_end = s->y_tma_end;
-            launch_tma<S, C>(a, s->tmaps[fin == s->f ? 0 : 1], energy, st);
+            a.work = s->d_done + 1;
+            launch_tma<S, C>(a, s->tmaps[fin == s->f ? 0 : 1], energy, st, s->st_side, s->ev_fork, s->ev_join);
             return;
         }
     }
@@ -998,11 +1004,14 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
         }
         // the TMA-staged step (tma_step.cuh): FP32 fields and coefficients, plain update, the
         // reference's x ends, a handle of its own (not a linked slab), at least one TMA strip.
-        // TW_TMA=1 in the environment selects it (default: the per-warp kernel);
-        // TW_TMA_CTAS_PER_SM sets the CTAs of work per SM its row segmentation aims at.
+        // With the energy every step its 40 bytes of FP64 weights per point halve the resident CTAs
+        // and it is slower than the per-warp kernel (117 against 108 us at 2048^2), so by default it
+        // steps handles with the energy off; TW_TMA=1 / 0 in the environment selects it / the
+        // per-warp kernel for every handle (for comparisons);
+        // its work items and side segments have TW_TMA_SEG_ROWS / TW_TMA_SIDE_ROWS rows (below).
         const int nts = tma_strips(My);
         if (d.precision == TW_FP32 && d.cpst == TW_CPST_00 && !d.coef_fp16 && !s->slab && !(s->bnd & BND_X_IF) &&
-            s->n_int_seg > 0 && nts > 0 && env_int("TW_TMA", 0) != 0) {
+            s->n_int_seg > 0 && nts > 0 && env_int("TW_TMA", d.energy ? 0 : 1) != 0) {
             int n_sm = 148;
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, d.device);
             s->tma = true;
@@ -1010,14 +1019,23 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             s->y_tma_end = TMA_Y0 + TMA_CORE * nts;
             // warp strips: the first at column 0, the others from y_tma_end to the seam column My
             s->n_ostrip = 1 + (int)((My + 1 - s->y_tma_end + FS_WARP_CORE - 1) / FS_WARP_CORE);
-            const int per_sm = std::max(1, env_int("TW_TMA_CTAS_PER_SM", 8));
+            // work items of about TW_TMA_SEG_ROWS rows (default 32) for the persistent TMA CTAs
+            const int seg_rows = std::max(8, env_int("TW_TMA_SEG_ROWS", 32));
             const int max_seg = std::max(1, s->int_rows / 8);
-            s->n_tseg = std::max(1, std::min(max_seg, (n_sm * per_sm + nts / 2) / nts));
-            s->n_int_seg = std::max(1, std::min(max_seg, 2 * s->n_tseg));
+            s->n_tseg = std::max(1, std::min(max_seg, (s->int_rows + seg_rows / 2) / seg_rows));
+            (void)n_sm;
+            // the warp strips run beside the TMA strips, latency-bound at about two microseconds a
+            // row: short segments (TW_TMA_SIDE_ROWS rows, default 8) keep them shorter than a TMA CTA
+            const int side_rows = std::max(8, env_int("TW_TMA_SIDE_ROWS", 8));
+            s->n_int_seg = std::max(1, std::min(max_seg, s->int_rows / side_rows));
             s->n_int_cta = (s->n_int_seg * s->n_ostrip + FS_WARPS - 1) / FS_WARPS;
             s->n_tcta = s->n_tseg * s->n_tstrip;
             e = prepare_tma<float, float>();
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
+            if ((e = cudaStreamCreateWithFlags(&s->st_side, cudaStreamNonBlocking)) != cudaSuccess ||
+                (e = cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming)) != cudaSuccess ||
+                (e = cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming)) != cudaSuccess)
+                return fail(cuda_fail(e, "side stream"));
             s->tmaps = new (std::nothrow) TmaMaps[2];
             if (!s->tmaps) return fail(TW_ERR_NOMEM);
             // maps by field slot: the fields of buffer `par`, the coefficients, the energy weights
@@ -1034,8 +1052,9 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
                 }
         }
         const int nctas = s->n_int_cta + s->n_zone * s->n_bstrip + s->n_tcta;
-        if ((rc_ = s->alloc((void **)&s->d_done, sizeof(int))) != TW_OK) return fail(rc_);
-        cudaMemsetAsync(s->d_done, 0, sizeof(int), s->st);
+        // d_done[0]: CTAs finished in this step; d_done[1]: the TMA strips' next work item
+        if ((rc_ = s->alloc((void **)&s->d_done, 2 * sizeof(int))) != TW_OK) return fail(rc_);
+        cudaMemsetAsync(s->d_done, 0, 2 * sizeof(int), s->st);
         if ((rc_ = s->alloc((void **)&s->d_rcv_off, sizeof(int) * (nctas + 1))) != TW_OK) return fail(rc_);
         cudaMemsetAsync(s->d_rcv_off, 0, sizeof(int) * (nctas + 1), s->st);
     }
@@ -1275,7 +1294,7 @@ int tw_reset(tw_solver *s)
         if (s->f2[k]) TW_CUDA(cudaMemsetAsync(s->f2[k], 0, n, s->st));
         if (s->res2[k]) TW_CUDA(cudaMemsetAsync(s->res2[k], 0, n, s->st));
     }
-    if (s->d_done) TW_CUDA(cudaMemsetAsync(s->d_done, 0, sizeof(int), s->st));
+    if (s->d_done) TW_CUDA(cudaMemsetAsync(s->d_done, 0, (s->fused ? 2 : 1) * sizeof(int), s->st));
     s->parity = 0;
     TW_CUDA(cudaMemsetAsync(s->d_energy, 0, sizeof(double) * 3 * s->d.max_steps, s->st));
     if (s->d_traces) TW_CUDA(cudaMemsetAsync(s->d_traces, 0, sizeof(double) * 2 * (size_t)s->rcv_cap * s->d.max_steps, s->st));
@@ -1695,6 +1714,9 @@ int tw_get_info(tw_solver *s, tw_info *info)
     info->own_rows[0] = s->own0;
     info->own_rows[1] = s->own1;
     info->Mx_glob = s->Mx_glob;
+    info->step_kind = s->tma ? 2 : (s->fused ? 1 : (s->afused ? 3 : 0));
+    info->launches_per_step = s->tma ? 2 : ((s->fused || s->afused) ? 1 : 3);
+    if (s->fused && (s->bnd & BND_Y_SAT)) info->launches_per_step += 2;   // the y-end recomputation
     return TW_OK;
 }
 

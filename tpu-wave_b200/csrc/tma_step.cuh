@@ -2,7 +2,7 @@
 // update): one launch per step, every field read once and written once, bit-identical to the
 // per-point kernels (hence to the reference's CPU solver, forward_simulation.cpp:38-113).
 //
-// Three kinds of CTA (4 warps each) share the launch:
+// Three kinds of CTA (4 warps each) make the step, in two launches (see k_elastic_side):
 // * boundary CTAs (the FS_ZONE rows at each free surface): boundary_cta of fused_step.cuh;
 // * warp-strip CTAs: interior_warp of fused_step.cuh over the interior columns that the TMA
 //   strips leave, among them the periodic seam (its reads follow the seam rule column by column);
@@ -462,36 +462,11 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
     }
 }
 
+// the CTA's energy sums into the step's records (red: 3 x FS_WARPS doubles of shared memory)
 template <bool ENERGY>
-__global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
-    k_elastic_tma(FusedArgs<float, float> a, const __grid_constant__ TmaMaps maps)
+__device__ __forceinline__ void cta_energy(const FusedArgs<float, float> &a, const EAcc &E, double *red, int it)
 {
-    extern __shared__ __align__(128) unsigned char tma_smem_raw[];
-    unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<unsigned long>(tma_smem_raw) + 127) & ~127ul);
-    const int it = *a.step;
-    const int cta = blockIdx.x;
-    const int rcv_b = a.rcv_off[cta], rcv_e = a.rcv_off[cta + 1];
-    EAcc E;
-    const int n_bnd = a.n_zone * a.n_bstrip;
-    if (cta < n_bnd) {
-        boundary_cta<float, float, 0, ENERGY, float, false>(a, cta % a.n_bstrip, cta / a.n_bstrip, it, rcv_b, rcv_e,
-                                                           reinterpret_cast<float *>(base), E);
-    } else if (cta < n_bnd + a.n_octa) {
-        // warp strips: segments of the interior rows (a.n_int_seg of them) x a.n_ostrip strips
-        const int gw = (cta - n_bnd) * FS_WARPS + (threadIdx.x >> 5);
-        if (gw < a.n_int_seg * a.n_ostrip) {
-            const int seg = gw / a.n_ostrip, os = gw - seg * a.n_ostrip;
-            const int y0 = os == 0 ? 0 : a.y_tma_end + (os - 1) * FS_WARP_CORE;
-            unsigned char *ring = base + (threadIdx.x >> 5) * RingLayout<float, float, 0, ENERGY, float>::warp;
-            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<float, float, 0, ENERGY, false, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
-            else interior_warp<float, float, 0, ENERGY, true, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
-        }
-    } else {
-        const int t = cta - n_bnd - a.n_octa;
-        tma_strip_cta<ENERGY>(a, maps, t % a.n_tstrip, t / a.n_tstrip, it, rcv_b, rcv_e, E, base);
-    }
-    if (ENERGY) {
-        double *red = reinterpret_cast<double *>(base + TmaLayout<ENERGY>::o_bar + 32);   // 3 x 4 doubles
+    if constexpr (ENERGY) {
         __syncthreads();   // every thread is past its use of the shared rings and tiles
         double e3[3] = {E.p0, E.k, E.p1};
 #pragma unroll
@@ -508,17 +483,83 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
             if (it < a.max_steps && v != 0.) atomicAdd(a.energy + (long)threadIdx.x * a.max_steps + it, 0.5 * v);
         }
     }
-    // the last CTA to finish advances the step counter
+}
+
+// The step is two launches that run side by side, on two streams forked from and joined into the
+// handle's stream (two parallel branches in a captured graph): k_elastic_side holds the boundary
+// CTAs and the warp strips (latency-bound, few), k_elastic_tma the TMA strips. Neither reads
+// what the other writes: both read only the step's input buffers and write disjoint parts of its
+// output buffers. Every CTA of either counts itself done at its end; the last of all of them
+// advances the step counter (and clears the TMA strips' item counter), after every CTA of the
+// step has read it. Kept apart, each SM runs one hot loop most of the time, and the TMA strips
+// fill whatever slots the side CTAs leave.
+__device__ __forceinline__ void step_done(const FusedArgs<float, float> &a, int it)
+{
     __syncthreads();
     if (threadIdx.x == 0) {
         __threadfence();
         const int ticket = atomicAdd(a.done, 1);
-        if (ticket == gridDim.x - 1) {
+        if (ticket == a.n_all_ctas - 1) {
             *a.done = 0;
+            *a.work = 0;
             *a.step = it + 1;
             __threadfence();
         }
     }
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<float, ENERGY>())
+    k_elastic_side(FusedArgs<float, float> a)
+{
+    extern __shared__ __align__(16) unsigned char side_smem_raw[];
+    __shared__ double red[3 * FS_WARPS];
+    const int it = *a.step;
+    const int cta = blockIdx.x;
+    const int rcv_b = a.rcv_off[cta], rcv_e = a.rcv_off[cta + 1];
+    EAcc E;
+    const int n_bnd = a.n_zone * a.n_bstrip;
+    if (cta < n_bnd) {
+        boundary_cta<float, float, 0, ENERGY, float, false>(a, cta % a.n_bstrip, cta / a.n_bstrip, it, rcv_b, rcv_e,
+                                                           reinterpret_cast<float *>(side_smem_raw), E);
+    } else {
+        // warp strips: segments of the interior rows (a.n_int_seg of them) x a.n_ostrip strips
+        const int gw = (cta - n_bnd) * FS_WARPS + (threadIdx.x >> 5);
+        if (gw < a.n_int_seg * a.n_ostrip) {
+            const int seg = gw / a.n_ostrip, os = gw - seg * a.n_ostrip;
+            const int y0 = os == 0 ? 0 : a.y_tma_end + (os - 1) * FS_WARP_CORE;
+            unsigned char *ring = side_smem_raw + (threadIdx.x >> 5) * RingLayout<float, float, 0, ENERGY, float>::warp;
+            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<float, float, 0, ENERGY, false, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
+            else interior_warp<float, float, 0, ENERGY, true, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
+        }
+    }
+    cta_energy<ENERGY>(a, E, red, it);
+    step_done(a, it);
+}
+
+template <bool ENERGY>
+__global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
+    k_elastic_tma(FusedArgs<float, float> a, const __grid_constant__ TmaMaps maps)
+{
+    extern __shared__ __align__(128) unsigned char tma_smem_raw[];
+    unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<unsigned long>(tma_smem_raw) + 127) & ~127ul);
+    const int it = *a.step;
+    const int n_side = a.n_zone * a.n_bstrip + a.n_octa;   // receiver lists: the side CTAs' come first
+    int *item_s = reinterpret_cast<int *>(base + TmaLayout<ENERGY>::o_bar + 24);
+    EAcc E;
+    // a persistent grid: each CTA takes (segment, strip) items until none is left, so CTAs that
+    // find their SM busy with side CTAs at first simply take fewer items
+    for (;;) {
+        if (threadIdx.x == 0) *item_s = atomicAdd(a.work, 1);
+        __syncthreads();
+        const int t = *item_s;
+        __syncthreads();
+        if (t >= a.n_tcta) break;
+        const int rcv_b = a.rcv_off[n_side + t], rcv_e = a.rcv_off[n_side + t + 1];
+        if (!tma_strip_cta<ENERGY>(a, maps, t % a.n_tstrip, t / a.n_tstrip, it, rcv_b, rcv_e, E, base)) break;
+    }
+    cta_energy<ENERGY>(a, E, reinterpret_cast<double *>(base + TmaLayout<ENERGY>::o_bar + 32), it);
+    step_done(a, it);
 }
 
 }  // namespace tw
