@@ -649,22 +649,24 @@ def run_mixed(args):
     dt = CFL * dx / (np.sqrt(2.0) * vp.max())
     # 64 receivers on the NM grid along a row 160 cells from the source, within reach in 2000 steps
     rx, ry = np.full(64, n // 2 - 160), n // 2 - 320 + 10 * np.arange(64)
-    # (storage, compensation, FP16 coefficients, algorithmic bytes per update)
-    variants = [("f64", "00", False, 120), ("f32", "00", False, 60), ("f32", "00", True, 50),
-                ("bf16", "00", False, 40), ("bf16", "split", False, 60), ("fp16", "00", False, 40),
-                ("fp16", "split", False, 60), ("fp16", "split", True, 50)]
-    if args.variant:   # e.g. "f32-00" or "fp16-split-c16": run only these (errors need "f64-00" first)
+    # (storage, compensation, coefficient storage, algorithmic bytes per update); coefficients:
+    # "full" = the compute type, "c16" = FP16, "q16" = 16-bit fixed-point codes on a per-array map
+    variants = [("f64", "00", "full", 120), ("f32", "00", "full", 60), ("f32", "00", "q16", 50),
+                ("f32", "00", "c16", 50), ("bf16", "00", "full", 40), ("bf16", "split", "full", 60),
+                ("fp16", "00", "full", 40), ("fp16", "split", "full", 60), ("fp16", "split", "c16", 50)]
+    if args.variant:   # e.g. "f32-00" or "f32-00-q16": run only these (errors need "f64-00" first)
         names = args.variant.split(",")
-        variants = [v for v in variants if f"{v[0]}-{v[1]}" + ("-c16" if v[2] else "") in names]
+        variants = [v for v in variants if f"{v[0]}-{v[1]}" + ("" if v[2] == "full" else "-" + v[2]) in names]
         if not variants:
             raise SystemExit(f"--variant {args.variant}: no such variant")
     peak, peak_note = measured_peaks()
     keys = [(tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)]
     ref = None
     out = []
-    for prec, cpst, c16, bpu in variants:
+    for prec, cpst, cstore, bpu in variants:
         s = tw.Solver(n, n, 1, DEN_DX, dt, physics=tw.ELASTIC, precision=prec, cpst=cpst, central_f=F0,
-                      time_delay=DELAY, max_steps=args.warmup + K, energy=False, coef_fp16=c16)
+                      time_delay=DELAY, max_steps=args.warmup + K, energy=False, coef_fp16=cstore == "c16",
+                      coef_q16=cstore == "q16")
         s.set_material_model(rho, vp, vs)
         s.set_source(tw.MM, n // 2, n // 2)
         s.add_receivers(tw.NM, rx, ry)
@@ -682,9 +684,12 @@ def run_mixed(args):
         ms = e0.elapsed_time(e1)
         fields = [s.read_field(g, f) for g, f in keys]
         traces = s.read_receivers()
+        kind = s.info().step_kind
         s.close()
         gpts = n * n * K / (ms / 1e3) / 1e9
-        row = {"precision": prec, "compensation": cpst, "coefficients": "fp16" if c16 else "compute type",
+        row = {"precision": prec, "compensation": cpst,
+               "coefficients": {"full": "compute type", "c16": "fp16", "q16": "16-bit fixed point"}[cstore],
+               "step": {2: "TMA-staged (two launches)", 1: "one-launch per-warp kernel"}.get(kind, "other"),
                "gpts": gpts, "ms_per_step": ms / K,
                "bytes_per_update": bpu, "hbm_frac": gpts * bpu / peak}
         if prec != "f64" and ref is None:
@@ -701,8 +706,9 @@ def run_mixed(args):
                         "trace_err": float(np.linalg.norm(traces - ref[1]) / np.linalg.norm(ref[1]))})
         del fields, traces
         out.append(row)
-    best = max((r for r in out if (r["precision"] in ("bf16", "fp16") or r["coefficients"] == "fp16")
+    best = max((r for r in out if (r["precision"] in ("bf16", "fp16") or r["coefficients"] != "compute type")
                 and r["l2_err"] is not None and r["l2_err"] <= 1e-4), key=lambda r: r["gpts"], default=None)
+    f32 = next((r for r in out if r["precision"] == "f32" and r["coefficients"] == "compute type"), None)
     line = {"metric": METRIC, "value": best["gpts"] if best else None, "unit": UNIT, "n_gpus": 1, "steps": K,
             "warmup": args.warmup, "higher_is_better": True,
             "dtype": f"{best['precision']} fields, {best['coefficients']} coefficients, f32 arithmetic" if best else None,
@@ -712,7 +718,8 @@ def run_mixed(args):
                                    f"CFL 0.4, Ricker f0=15 at the centre, 64 receivers on an NM row 160 cells from it",
                        "errors": "relative L2 over all five fields, Linf / max |FP64|, trace L2, vs the FP64 run",
                        "l2": f"inputs far larger than L2, no flush", "peak": f"{peak} GB/s {peak_note}"},
-            "variants": out}
+            "variants": out,
+            "best_mixed_over_plain_fp32": (best["gpts"] / f32["gpts"]) if best and f32 else None}
     print(json.dumps(line), flush=True)
 
 

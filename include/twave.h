@@ -88,7 +88,14 @@ typedef struct {
     int device;             /* CUDA device ordinal (ns_input::device_number) */
     int coef_fp16;          /* 1: store the stepping coefficients in FP16 (elastic, FP32 arithmetic; no
                                reference counterpart): 10 B less per update; the medium is quantised to
-                               FP16, and coefficients outside its normal range are TW_ERR_UNSUPPORTED */
+                               FP16, and coefficients outside its normal range are TW_ERR_UNSUPPORTED.
+                               2: store them as 16-bit fixed-point codes, each array on its own affine
+                               map c = lo + step * code (lo its smallest value, step its range / 65535,
+                               FP32 arithmetic): 16 significant bits across the array's range, 10 B less
+                               per update (50 B with FP32 fields). Elastic, FP32 fields, TW_CPST_00, the
+                               reference's boundaries, My >= 180 (the TMA-staged step reads the codes;
+                               the other parts of the step read the decoded values). No reference
+                               counterpart. tw_read_coefficients returns the values the step uses. */
     int sat_y;              /* 1: SBP-SAT free surfaces on the two y ends too (all four sides free with
                                bc_x TW_BC_SAT_FREE): closures and penalties along y with the x tables,
                                energy norm along y as along x; no reference run (its y is periodic).
@@ -141,6 +148,12 @@ TW_API int tw_set_material_model(tw_solver *s, const double *rho, const double *
  * that prepare coefficients themselves (the single-core tree sets them directly,
  * cpu_acoustic.cpp:178-180). */
 TW_API int tw_set_material_grid(tw_solver *s, int grid, int idx, const double *coef, long ld);
+
+/* The stepping coefficients the handle steps with, at reference sizes (row stride ld): NN idx 0
+ * mu, MN / NM idx 0 1/rho, MM idx 0 lambda (acoustic: kappa), idx 1 2mu - the reference's
+ * Vec_prmt after make_density_reciprocal (grid_parameter.cpp:131-160), rounded to the storage of
+ * the handle (decoded from 16-bit codes with coef_fp16 = 2). */
+TW_API int tw_read_coefficients(tw_solver *s, int grid, int idx, double *host, long ld);
 
 /* Source: Class_Forward_Specs::process_src_locations (forward.cpp:10-100) with the location
  * given as rationals per data direction (struct_src_input, src_rcv.hpp:6-11). */

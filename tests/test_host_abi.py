@@ -70,7 +70,9 @@ def _desc(tw, **kw):
     (dict(precision=2, cpst=4), -10),               # 16-bit storage: plain or split only
     (dict(precision=1, cpst=7), -10),               # the split pair needs 16-bit storage
     (dict(physics=1, precision=3), -10),            # 16-bit storage is elastic only
-    (dict(coef_fp16=2), -1),
+    (dict(coef_fp16=3), -1),
+    (dict(coef_fp16=2), -10),                       # 16-bit coefficient codes need a TMA strip (My >= 180)
+    (dict(coef_fp16=2, precision=0, My=256), -10),  # ... and FP32 fields
     (dict(coef_fp16=1, precision=0), -10),          # FP16 coefficients need FP32 arithmetic
     (dict(coef_fp16=1, cpst=6), -10),               # ... and the plain update
     (dict(coef_fp16=1, physics=1, bc_x=1), -10),    # ... and the elastic stepper

@@ -139,3 +139,53 @@ def test_fp16_coefficients_reject_a_medium_outside_their_range():
         s.set_material_model(case.rho.reshape(shp), case.vp.reshape(shp) * 1000, case.vs.reshape(shp) * 1000)
     assert e.value.code == -10
     s.close()
+
+
+@pytest.mark.parametrize("energy", [False, True])
+@pytest.mark.parametrize("Mx,My", [(40, 300), (57, 421)])
+def test_fixed_point_coefficients_match_oracle(Mx, My, energy):
+    """Coefficients stored as 16-bit codes on a per-array affine map (coef_fp16 = 2): every decoded
+    value lies within half a step of the FP32 coefficient, and the run equals the restatement given
+    the decoded coefficients bit for bit (fields, traces; energies to 1e-12)."""
+    tw = load_twave()
+    den = max(Mx, My)
+    rcvs = [("N", "M", 9, den, 2 * 100 + 1, 2 * den), ("M", "M", 2 * (Mx // 2) + 1, 2 * den, 2 * 177 + 1, 2 * den),
+            ("N", "N", Mx // 3, den, My, den), ("M", "N", 2 * 11 + 1, 2 * den, 0, 1)]
+    case = elastic_case(Mx, My, seed=Mx * My, Nt=5, rcvs=rcvs, den_dx=den)
+    shp = (Mx + 2, My + 2)
+    keys = [(tw.NN, 0, "NN_mu"), (tw.MN, 0, "MN_irho"), (tw.NM, 0, "NM_irho"), (tw.MM, 0, "MM_lambda"), (tw.MM, 1, "MM_2mu")]
+
+    def handle(q16):
+        s = tw.Solver(Mx, My, 1, den, case.dt, precision="f32", cpst="00", central_f=case.central_f,
+                      time_delay=case.time_delay, max_steps=case.Nt, energy=energy, coef_q16=q16)
+        s.set_material_model(case.rho.reshape(shp), case.vp.reshape(shp), case.vs.reshape(shp))
+        s.set_source_location(*case.src)
+        for r in case.rcvs:
+            s.add_receiver_location(*r)
+        return s
+    plain = handle(False)
+    full = {name: plain.read_coefficients(g, i) for g, i, name in keys}
+    plain.close()
+    s = handle(True)
+    try:
+        dec = {name: s.read_coefficients(g, i) for g, i, name in keys}
+        for name in dec:
+            lo, hi = full[name].min(), full[name].max()
+            step = np.float32((hi - lo) / 65535.0)
+            assert np.abs(dec[name] - full[name]).max() <= 0.5 * step * (1 + 1e-3) + 4 * np.spacing(np.float32(hi)), name
+        f0 = [(a * 0.1).astype(np.float32).astype(np.float64) for a in _state(Mx, My, 7, "f32", "split")]
+        for (g, f), a in zip([(tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)], f0):
+            s.write_field(g, f, a)
+        s.run(case.Nt)
+        got = [s.read_field(g, f) for g, f in [(tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1)]]
+        traces = s.read_receivers()
+        E = s.read_energy() if energy else None
+    finally:
+        s.close()
+    want = orc.elastic_run(case, "f32", fields0=f0, coefs=dec)
+    for k, v in zip(KEYS, got):
+        assert np.array_equal(v, want.fields[k]), k
+    assert np.array_equal(traces, want.traces)
+    if energy:
+        for k, v in zip(("E_k", "E_p0", "E_p1"), E):
+            assert energy_close(v, getattr(want, k)), k

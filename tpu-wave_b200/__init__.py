@@ -99,6 +99,7 @@ def lib() -> C.CDLL:
         for name in ("tw_read_field", "tw_write_field", "tw_read_resid", "tw_write_resid"):
             getattr(L, name).argtypes = [vp, C.c_int, C.c_int, dp, C.c_long]
         L.tw_read_receivers.argtypes = [vp, dp]
+        L.tw_read_coefficients.argtypes = [vp, C.c_int, C.c_int, dp, C.c_long]
         L.tw_read_energy.argtypes = [vp, dp, dp, dp]
         L.tw_get_info.argtypes = [vp, C.POINTER(Info)]
         L.tw_get_stream.argtypes = [vp, C.POINTER(vp)]
@@ -202,10 +203,13 @@ class Solver:
     def __init__(self, Mx: int, My: int, num_dx: int, den_dx: int, dt: float, *, physics: int = ELASTIC,
                  bc_x: int = SAT_FREE, precision: str = "f32", cpst: str = "00", central_f: float = 5.0,
                  time_delay: float = 0.25, source_scaling: float = 1.0, max_steps: int = 1000,
-                 energy: bool = True, device: int = 0, coef_fp16: bool = False, sat_y: bool = False):
+                 energy: bool = True, device: int = 0, coef_fp16: bool = False, sat_y: bool = False,
+                 coef_q16: bool = False):
+        """coef_fp16: stepping coefficients stored in FP16; coef_q16: stored as 16-bit fixed-point
+        codes on a per-array affine map (tw_grid_desc.coef_fp16 = 1 / 2)."""
         self.desc = GridDesc(physics, bc_x, PRECISION[precision], CPST[cpst], Mx, My, num_dx, den_dx, dt,
                              central_f, time_delay, source_scaling, max_steps, 1 if energy else 0, device,
-                             1 if coef_fp16 else 0, 1 if sat_y else 0)
+                             2 if coef_q16 else (1 if coef_fp16 else 0), 1 if sat_y else 0)
         self.h = C.c_void_p()
         _ok(lib().tw_create(C.byref(self.h), C.byref(self.desc)), "tw_create")
         self.Mx, self.My, self.physics, self.bc_x = Mx, My, physics, bc_x
@@ -349,6 +353,13 @@ class Solver:
         if a.shape != (r, c):
             raise ValueError(f"expected shape {(r, c)}")
         _ok(lib().tw_write_field(self.h, grid, field, _dp(a), c), "tw_write_field")
+
+    def read_coefficients(self, grid: int, idx: int = 0) -> np.ndarray:
+        """The stepping coefficient the handle steps with (tw_read_coefficients): NN mu, MN / NM
+        1/rho, MM lambda (idx 0) and 2mu (idx 1), at reference sizes."""
+        out = np.zeros(self.shape(grid))
+        _ok(lib().tw_read_coefficients(self.h, grid, idx, _dp(out), out.shape[1]), "tw_read_coefficients")
+        return out
 
     def read_resid(self, grid: int, field: int = 0) -> np.ndarray:
         r, c = self.shape(grid)

@@ -1,5 +1,6 @@
 // Set-up and bookkeeping kernels: FP64 material interpolation, stepping coefficients and energy
 // weights, the discrete energy reductions and the receiver gather.
+#include <cstring>
 #include "kernels.h"
 
 namespace tw {
@@ -185,6 +186,76 @@ void launch_material_finalize(const MaterialArgs &m, cudaStream_t st)
 template void launch_material_finalize<double, double>(const MaterialArgs &, cudaStream_t);
 template void launch_material_finalize<float, float>(const MaterialArgs &, cudaStream_t);
 template void launch_material_finalize<float, __half>(const MaterialArgs &, cudaStream_t);
+
+// ---------------------------------------------------------------- 16-bit fixed-point coefficients
+// (coef_fp16 = 2) Each coefficient array is stored as codes k in [0, 65535] on an affine map
+// c = lo + step * k, lo its smallest value, step its range / 65535; every part of the step uses the
+// decoded FP32 value fl(lo + fl(step * k)), which replaces the array's FP32 coefficient.
+
+// an order-preserving unsigned image of a float (and back), for min / max by integer atomics
+__device__ __forceinline__ unsigned f2ord(float f)
+{
+    const unsigned u = __float_as_uint(f);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+static float ord2f(unsigned u)
+{
+    u = (u & 0x80000000u) ? (u & 0x7fffffffu) : ~u;
+    float f;
+    memcpy(&f, &u, 4);
+    return f;
+}
+
+__global__ void k_minmax(const float *a, int rows, int cols, long pitch, unsigned *mm)
+{
+    unsigned lo = 0xffffffffu, hi = 0u;
+    const long n = (long)rows * cols;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const unsigned o = f2ord(a[(i / cols) * pitch + i % cols]);
+        lo = o < lo ? o : lo;
+        hi = o > hi ? o : hi;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned l2 = __shfl_down_sync(0xffffffffu, lo, o), h2 = __shfl_down_sync(0xffffffffu, hi, o);
+        lo = l2 < lo ? l2 : lo;
+        hi = h2 > hi ? h2 : hi;
+    }
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(mm, lo);
+        atomicMax(mm + 1, hi);
+    }
+}
+
+__global__ void k_quantize16(float *a, unsigned short *codes, int rows, int cols, long pitch, float lo, float step)
+{
+    const long n = (long)rows * cols;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const long o = (i / cols) * pitch + i % cols;
+        float k = step > 0.f ? rintf(__fdiv_rn(__fsub_rn(a[o], lo), step)) : 0.f;
+        k = fminf(fmaxf(k, 0.f), 65535.f);
+        codes[o] = (unsigned short)k;
+        a[o] = __fadd_rn(lo, __fmul_rn(step, k));
+    }
+}
+
+int quantize_coefficients16(float *coef, unsigned short *codes, int rows, int cols, long pitch, unsigned *d_mm,
+                            float *lo, float *step, cudaStream_t st)
+{
+    const unsigned init[2] = {0xffffffffu, 0u};
+    unsigned mm[2];
+    if (cudaMemcpyAsync(d_mm, init, sizeof(init), cudaMemcpyHostToDevice, st) != cudaSuccess) return -1;
+    k_minmax<<<592, 256, 0, st>>>(coef, rows, cols, pitch, d_mm);
+    if (cudaMemcpyAsync(mm, d_mm, sizeof(mm), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaStreamSynchronize(st) != cudaSuccess)
+        return -1;
+    const float l = ord2f(mm[0]), h = ord2f(mm[1]);
+    if (!(l <= h)) return -1;   // no value, or not a number
+    *lo = l;
+    *step = (float)(((double)h - (double)l) / 65535.0);
+    k_quantize16<<<592, 256, 0, st>>>(coef, codes, rows, cols, pitch, l, *step);
+    return cudaGetLastError() == cudaSuccess ? 0 : -1;
+}
 
 // ---------------------------------------------------------------- discrete energy (FP64)
 __device__ __forceinline__ double warp_sum(double v)

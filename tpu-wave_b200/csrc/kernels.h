@@ -66,6 +66,12 @@ struct MaterialArgs {
 template <class C, class K = C>
 void launch_material_finalize(const MaterialArgs &m, cudaStream_t st);
 
+// 16-bit fixed-point coefficients (coef_fp16 = 2): codes of the FP32 array `coef` (rows x cols of
+// a pitched array) on the map c = lo + step * code, lo the smallest value, step the range / 65535;
+// `coef` is overwritten with the decoded values. d_mm: two unsigned of device scratch. 0 on success.
+int quantize_coefficients16(float *coef, unsigned short *codes, int rows, int cols, long pitch, unsigned *d_mm,
+                            float *lo, float *step, cudaStream_t st);
+
 template <class S, class C>
 struct EnergyArgs {
     const S *a[4];            // up to four terms sum_i a_i w_i b_i over rows x My
@@ -172,6 +178,10 @@ struct FusedArgs {
     int *work;                // the TMA strips' next work item (a persistent CTA takes items until
                               // n_tcta are taken; zero between steps)
     int n_all_ctas;           // CTAs of both launches of the TMA-staged step
+    // 16-bit fixed-point coefficients (coef_fp16 = 2): the TMA strips read codes (maps of the codes)
+    // and decode c = qlo + qstep * code by field slot; everything else reads `coef` (decoded FP32)
+    int q16;
+    float qlo[5], qstep[5];
 };
 template <class S, class C>
 void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, bool coef16, cudaStream_t st);
@@ -196,6 +206,8 @@ cudaError_t prepare_tma();
 template <class S, class C>
 void launch_tma(FusedArgs<S, C> a, const TmaMaps &maps, bool energy, cudaStream_t st, cudaStream_t side,
                 cudaEvent_t fork, cudaEvent_t join);
+constexpr int TMA_QW = TMA_W + 8;    // columns of a 16-bit coefficient box: from 8 before the strip's core
+                                     // (a 16-byte boundary) to 4 beyond the 128 loaded field columns
 
 // free y ends on the fused step (ysat_fix.cu): the fused kernel steps every column with the
 // periodic y rule; these two launches then recompute, from the step's input buffers, the points

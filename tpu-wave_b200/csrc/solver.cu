@@ -136,6 +136,12 @@ struct tw_solver {
     TmaMaps *tmaps = nullptr;
     cudaStream_t st_side = nullptr;   // the side launch's stream, forked from st and joined back
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // 16-bit fixed-point coefficients (coef_fp16 = 2): the codes the TMA strips read, each array's
+    // map (coef holds the decoded FP32 values for every other reader), two words of scratch
+    bool q16 = false;
+    unsigned short *coefq[5] = {};
+    float qlo[5] = {}, qstep[5] = {};
+    unsigned *d_mm = nullptr;
     int ir0 = FS_ZONE, zone_kind[2] = {0, 1};
     // a slab of a larger grid (slab decomposition along x): local row r is global row r + row_off
     // of a grid of Mx_glob cells; it owns global rows [own0, own1) of every grid (plus the last
@@ -202,6 +208,8 @@ tw_solver::~tw_solver()
     release(d_done); release(d_rcv_off); release(d_rcv_list); release(model);
     release(src_inc); release(d_step); release(d_flags); release(d_rcv); release(d_err);
     release(d_traces); release(d_energy);
+    for (int k = 0; k < 5; k++) release(coefq[k]);
+    release(d_mm);
     cudaStreamSynchronize(st);   // the buffers are back in the pool before the next handle asks
     cudaStreamDestroy(st);
     if (st_side) cudaStreamDestroy(st_side);
@@ -420,11 +428,13 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
             a.n_octa = s->n_int_cta;
             a.y_tma_end = s->y_tma_end;
             a.work = s->d_done + 1;
+            a.q16 = s->q16 ? 1 : 0;
+            for (int k = 0; k < 5; k++) { a.qlo[k] = s->qlo[k]; a.qstep[k] = s->qstep[k]; }
             launch_tma<S, C>(a, s->tmaps[fin == s->f ? 0 : 1], energy, st, s->st_side, s->ev_fork, s->ev_join);
             return;
         }
     }
-    launch_fused<S, C>(a, s->d.cpst, energy, s->d.coef_fp16 != 0, st);
+    launch_fused<S, C>(a, s->d.cpst, energy, s->d.coef_fp16 == 1, st);
 }
 
 // one fused elastic step from the current buffers into the other ones
@@ -553,13 +563,18 @@ int finalize_material(tw_solver *s)
     m.err = s->d_err;
     TW_CUDA(cudaMemsetAsync(s->d_err, 0, sizeof(int), s->st));
     if (f64) launch_material_finalize<double, double>(m, s->st);
-    else if (s->d.coef_fp16) launch_material_finalize<float, __half>(m, s->st);
+    else if (s->d.coef_fp16 == 1) launch_material_finalize<float, __half>(m, s->st);
     else launch_material_finalize<float, float>(m, s->st);
     TW_CUDA(cudaGetLastError());
     int herr = 0;
     TW_CUDA(cudaMemcpyAsync(&herr, s->d_err, sizeof(int), cudaMemcpyDeviceToHost, s->st));
     TW_CUDA(cudaStreamSynchronize(s->st));
     if (herr & 2) return TW_ERR_UNSUPPORTED;   // a coefficient outside the normal FP16 range
+    if (s->q16)   // the codes, each array's map, and the decoded values in place of the FP32 ones
+        for (int k = 0; k < 5; k++)
+            if (quantize_coefficients16((float *)s->coef[k], s->coefq[k], s->rows[k], s->cols[k], s->pitch, s->d_mm,
+                                        &s->qlo[k], &s->qstep[k], s->st) != 0)
+                return cuda_fail(cudaGetLastError(), "coefficient codes");
     s->mat_dirty = false;
     s->mat_ready = true;
     return TW_OK;
@@ -755,16 +770,17 @@ PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder()
 }
 
 // a tensor map over `rows` rows of `pitch` elements (FP32 or FP64) with boxes of TMA_W x TMA_ROWS
-int encode_rows(unsigned char *out, const void *ptr, bool f64, long rows, long pitch)
+int encode_rows(unsigned char *out, const void *ptr, int esize, long rows, long pitch, int box_w = TMA_W)
 {
     const auto enc = tensor_map_encoder();
     if (!enc) return TW_ERR_UNSUPPORTED;
     const cuuint64_t dims[2] = {(cuuint64_t)pitch, (cuuint64_t)rows};
-    const cuuint64_t strides[1] = {(cuuint64_t)pitch * (f64 ? 8 : 4)};
-    const cuuint32_t box[2] = {(cuuint32_t)TMA_W, (cuuint32_t)TMA_ROWS};
+    const cuuint64_t strides[1] = {(cuuint64_t)pitch * esize};
+    const cuuint32_t box[2] = {(cuuint32_t)box_w, (cuuint32_t)TMA_ROWS};
     const cuuint32_t es[2] = {1, 1};
     const CUresult r = enc(reinterpret_cast<CUtensorMap *>(out),
-                           f64 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2,
+                           esize == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                      : (esize == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16), 2,
                            const_cast<void *>(ptr), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
                            CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -886,6 +902,12 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
     if ((d.bc_x == TW_BC_SAT_INTERFACE || d.sat_y) &&
         (d.bc_x == TW_BC_PERIODIC || d.precision == TW_BF16 || d.precision == TW_FP16 || d.coef_fp16))
         return TW_ERR_UNSUPPORTED;
+    // 16-bit fixed-point coefficients: read by the TMA-staged step (FP32 fields, plain update, the
+    // reference's boundaries, a handle of its own, at least one TMA strip)
+    if (d.coef_fp16 == 2 && (d.physics != TW_ELASTIC || d.precision != TW_FP32 || d.cpst != TW_CPST_00 ||
+                             d.bc_x != TW_BC_SAT_FREE || d.sat_y || sl.on || d.Mx < FS_SMALL_MX ||
+                             tma_strips(d.My) < 1))
+        return TW_ERR_UNSUPPORTED;
     if (d.sat_y && d.My < 8) return TW_ERR_INVALID;
     if (d.precision < TW_FP64 || d.precision > TW_FP16) return TW_ERR_INVALID;
     if (d.cpst < TW_CPST_00 || d.cpst > TW_CPST_SPLIT) return TW_ERR_INVALID;
@@ -894,7 +916,7 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
     // storage type narrower than the FP32 compute type
     if (narrow && (d.physics != TW_ELASTIC || (d.cpst != TW_CPST_00 && d.cpst != TW_CPST_SPLIT))) return TW_ERR_UNSUPPORTED;
     if (!narrow && d.cpst == TW_CPST_SPLIT) return TW_ERR_UNSUPPORTED;
-    if (d.coef_fp16 != 0 && d.coef_fp16 != 1) return TW_ERR_INVALID;
+    if (d.coef_fp16 < 0 || d.coef_fp16 > 2) return TW_ERR_INVALID;
     // FP16 coefficients: elastic with FP32 arithmetic, plain update (or the split pair)
     if (d.coef_fp16 && (d.physics != TW_ELASTIC || d.precision == TW_FP64 ||
                         (d.cpst != TW_CPST_00 && d.cpst != TW_CPST_SPLIT)))
@@ -937,7 +959,7 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaSetDevice"));
     e = cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking);
     if (e != cudaSuccess) return fail(cuda_fail(e, "cudaStreamCreate"));
-    const size_t csz = d.precision == TW_FP64 ? 8 : (d.coef_fp16 ? 2 : 4);
+    const size_t csz = d.precision == TW_FP64 ? 8 : (d.coef_fp16 == 1 ? 2 : 4);   // (16-bit codes: beside)
     const bool cp = d.cpst != TW_CPST_00;
     for (int k = 0; k < 5; k++) {
         if (!s->has_slot(k)) continue;
@@ -1010,8 +1032,9 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
         // per-warp kernel for every handle (for comparisons);
         // its work items and side segments have TW_TMA_SEG_ROWS / TW_TMA_SIDE_ROWS rows (below).
         const int nts = tma_strips(My);
-        if (d.precision == TW_FP32 && d.cpst == TW_CPST_00 && !d.coef_fp16 && !s->slab && !(s->bnd & BND_X_IF) &&
-            s->n_int_seg > 0 && nts > 0 && env_int("TW_TMA", d.energy ? 0 : 1) != 0) {
+        s->q16 = d.coef_fp16 == 2;
+        if (d.precision == TW_FP32 && d.cpst == TW_CPST_00 && d.coef_fp16 != 1 && !s->slab && !(s->bnd & BND_X_IF) &&
+            s->n_int_seg > 0 && nts > 0 && (s->q16 || env_int("TW_TMA", d.energy ? 0 : 1) != 0)) {
             int n_sm = 148;
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, d.device);
             s->tma = true;
@@ -1038,6 +1061,14 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
                 return fail(cuda_fail(e, "side stream"));
             s->tmaps = new (std::nothrow) TmaMaps[2];
             if (!s->tmaps) return fail(TW_ERR_NOMEM);
+            if (s->q16) {
+                for (int k = 0; k < 5; k++) {
+                    const size_t n = (size_t)s->rows[k] * s->pitch;
+                    if ((rc_ = s->alloc((void **)&s->coefq[k], n * 2)) != TW_OK) return fail(rc_);
+                    cudaMemsetAsync(s->coefq[k], 0, n * 2, s->st);
+                }
+                if ((rc_ = s->alloc((void **)&s->d_mm, 2 * sizeof(unsigned))) != TW_OK) return fail(rc_);
+            }
             // maps by field slot: the fields of buffer `par`, the coefficients, the energy weights
             const int fmap[5] = {TM_NN, TM_MN, TM_NM, TM_MM0, TM_MM1};
             const int cmap[5] = {TM_MU, TM_PMN, TM_PNM, TM_LAM, TM_M2};
@@ -1045,9 +1076,10 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             for (int par = 0; par < 2; par++)
                 for (int k = 0; k < 5; k++) {
                     TmaMaps &m = s->tmaps[par];
-                    if ((rc_ = encode_rows(m.m[fmap[k]], par ? s->f2[k] : s->f[k], false, s->rows[k], s->pitch)) != TW_OK ||
-                        (rc_ = encode_rows(m.m[cmap[k]], s->coef[k], false, s->rows[k], s->pitch)) != TW_OK ||
-                        (rc_ = encode_rows(m.m[wmap[k]], s->w[k], true, s->rows[k], s->pitch)) != TW_OK)
+                    if ((rc_ = encode_rows(m.m[fmap[k]], par ? s->f2[k] : s->f[k], 4, s->rows[k], s->pitch)) != TW_OK ||
+                        (rc_ = s->q16 ? encode_rows(m.m[cmap[k]], s->coefq[k], 2, s->rows[k], s->pitch, TMA_QW)
+                                      : encode_rows(m.m[cmap[k]], s->coef[k], 4, s->rows[k], s->pitch)) != TW_OK ||
+                        (rc_ = encode_rows(m.m[wmap[k]], s->w[k], 8, s->rows[k], s->pitch)) != TW_OK)
                         return fail(rc_);
                 }
         }
@@ -1374,6 +1406,18 @@ int tw_read_field(tw_solver *s, int grid, int field, double *host, long ld)
     TW_CUDA(cudaSetDevice(s->d.device));
     return read_device_array(s, cur_f(s, slot), s->d.precision, s->esz, slot, host, ld,
                              s->d.cpst == TW_CPST_SPLIT ? cur_res(s, slot) : nullptr);
+}
+
+int tw_read_coefficients(tw_solver *s, int grid, int idx, double *host, long ld)
+{
+    if (check(s) || !host || grid < 0 || grid > 3) return TW_ERR_INVALID;
+    const int slot = slot_of(s, grid, idx);
+    if (slot < 0 || ld < s->ref_cols[grid]) return TW_ERR_INVALID;
+    if (!s->mat_ready) return TW_ERR_STATE;
+    TW_CUDA(cudaSetDevice(s->d.device));
+    const int prec = s->d.precision == TW_FP64 ? TW_FP64 : (s->d.coef_fp16 == 1 ? TW_FP16 : TW_FP32);
+    const int esz = prec == TW_FP64 ? 8 : (prec == TW_FP16 ? 2 : 4);
+    return read_device_array(s, s->coef[slot], prec, esz, slot, host, ld);
 }
 
 int tw_write_field(tw_solver *s, int grid, int field, const double *host, long ld)

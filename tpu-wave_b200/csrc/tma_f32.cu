@@ -13,10 +13,10 @@ int tma_strips(long My)
     return My >= need ? (int)((My - need) / TMA_CORE) + 1 : 0;
 }
 
-template <bool ENERGY>
+template <bool ENERGY, bool Q16 = false>
 static size_t tma_smem()
 {
-    return (size_t)TmaLayout<ENERGY>::bytes;
+    return (size_t)TmaLayout<ENERGY, Q16>::bytes;
 }
 
 // dynamic shared memory of the side launch: the boundary CTAs' velocity tile or four warp rings
@@ -26,16 +26,40 @@ static size_t side_smem(int tile_rows)
     return fused_smem_bytes<float, float, 0, ENERGY, float>(tile_rows);
 }
 
+template <bool ENERGY, bool Q16>
+static cudaError_t tma_attr()
+{
+    return cudaFuncSetAttribute(k_elastic_tma<ENERGY, Q16>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)tma_smem<ENERGY, Q16>());
+}
+
 template <>
 cudaError_t prepare_tma<float, float>()
 {
-    cudaError_t e = cudaFuncSetAttribute(k_elastic_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem<false>());
-    if (e != cudaSuccess) return e;
-    e = cudaFuncSetAttribute(k_elastic_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tma_smem<true>());
-    if (e != cudaSuccess) return e;
+    cudaError_t e;
+    if ((e = tma_attr<false, false>()) != cudaSuccess || (e = tma_attr<true, false>()) != cudaSuccess ||
+        (e = tma_attr<false, true>()) != cudaSuccess || (e = tma_attr<true, true>()) != cudaSuccess)
+        return e;
     e = cudaFuncSetAttribute(k_elastic_side<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)side_smem<false>(FS_SMALL_MX + 1));
     if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(k_elastic_side<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)side_smem<true>(FS_SMALL_MX + 1));
+}
+
+// the TMA strips of one variant: a persistent grid of as many CTAs as fit on the device at once
+template <bool ENERGY, bool Q16>
+static void launch_strips(FusedArgs<float, float> &a, const TmaMaps &maps, int n_side, cudaStream_t st, bool go)
+{
+    static int resident = 0, n_sm = 0;
+    if (!n_sm) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident, k_elastic_tma<ENERGY, Q16>, FS_THREADS_MAX,
+                                                      tma_smem<ENERGY, Q16>());
+        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
+    }
+    const int n_strips = std::min(a.n_tcta, std::max(1, resident) * n_sm);
+    a.n_all_ctas = n_side + n_strips;
+    if (go) k_elastic_tma<ENERGY, Q16><<<n_strips, FS_THREADS_MAX, tma_smem<ENERGY, Q16>(), st>>>(a, maps);
 }
 
 // the side launch on a second stream forked from the handle's stream, the TMA strips on the
@@ -44,27 +68,23 @@ template <>
 void launch_tma<float, float>(FusedArgs<float, float> a, const TmaMaps &maps, bool energy, cudaStream_t st,
                               cudaStream_t side_st, cudaEvent_t fork, cudaEvent_t join)
 {
-    // the TMA strips' persistent grid: as many CTAs as fit on the device at once, at most one per item
-    static int resident[2] = {0, 0}, n_sm = 0;
-    if (!n_sm) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident[0], k_elastic_tma<false>, FS_THREADS_MAX, tma_smem<false>());
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&resident[1], k_elastic_tma<true>, FS_THREADS_MAX, tma_smem<true>());
-    }
-    const int per_sm = std::max(1, resident[energy ? 1 : 0]);
-    const int n_side = a.n_zone * a.n_bstrip + a.n_octa, n_strips = std::min(a.n_tcta, per_sm * n_sm);
-    a.n_all_ctas = n_side + n_strips;
-    const dim3 block(FS_THREADS_MAX);
-    cudaEventRecord(fork, st);
-    cudaStreamWaitEvent(side_st, fork, 0);
-    if (energy) {
-        k_elastic_side<true><<<n_side, block, side_smem<true>(a.tile_rows), side_st>>>(a);
-        k_elastic_tma<true><<<n_strips, block, tma_smem<true>(), st>>>(a, maps);
-    } else {
-        k_elastic_side<false><<<n_side, block, side_smem<false>(a.tile_rows), side_st>>>(a);
-        k_elastic_tma<false><<<n_strips, block, tma_smem<false>(), st>>>(a, maps);
+    const int n_side = a.n_zone * a.n_bstrip + a.n_octa;
+    const int v = (energy ? 1 : 0) + (a.q16 ? 2 : 0);
+    // first the strips' grid size (it sets the CTA count the last CTA waits for), then the launches
+    for (int pass = 0; pass < 2; pass++) {
+        const bool go = pass == 1;
+        if (go) {
+            cudaEventRecord(fork, st);
+            cudaStreamWaitEvent(side_st, fork, 0);
+            if (energy) k_elastic_side<true><<<n_side, FS_THREADS_MAX, side_smem<true>(a.tile_rows), side_st>>>(a);
+            else k_elastic_side<false><<<n_side, FS_THREADS_MAX, side_smem<false>(a.tile_rows), side_st>>>(a);
+        }
+        switch (v) {
+        case 0: launch_strips<false, false>(a, maps, n_side, st, go); break;
+        case 1: launch_strips<true, false>(a, maps, n_side, st, go); break;
+        case 2: launch_strips<false, true>(a, maps, n_side, st, go); break;
+        default: launch_strips<true, true>(a, maps, n_side, st, go); break;
+        }
     }
     cudaEventRecord(join, side_st);
     cudaStreamWaitEvent(st, join, 0);

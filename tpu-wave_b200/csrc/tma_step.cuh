@@ -19,10 +19,14 @@
 // Row bookkeeping of a segment [x0, x1) (stress rows): velocity rows j = x0 - 2 + 4q + warp and
 // stress rows i = j - 2 in step q = 0 .. Q-1, Q = ceil((x1 - x0 + 4) / 4). Arrays whose x
 // stencils reach around the row (NN, MM0, MM1) sit in 3-block rings based at row x0 - 4; the
-// velocity fields and coefficients in 2-block rings based at x0 - 2, the stress coefficients
-// (and energy weights) in 2-block rings based at x0 - 4. Copy group G = 0 carries the first
-// block of NN, MM0, MM1; group G >= 1 their block G and block G - 1 of every other array. Step q
-// consumes group q + 1; group q + 2 is issued when step q starts, into slots step q - 1 freed.
+// velocity fields and coefficients in 2-block rings based at x0 - 2, the stress coefficients (and
+// energy weights) in 2-block rings based at x0 - 4. Copy group G = 0 carries the first block of
+// NN, MM0, MM1; group G >= 1 their block G and block G - 1 of every other array. Step q consumes
+// groups q and q + 1; group q + 2 is issued when step q starts, into the slots step q - 1 freed.
+// (Issuing two steps ahead needs 4- and 3-block rings: 3 CTAs fit on an SM instead of 4, and the
+// step is about 12 % slower. Carrying the pipeline on from one item into the next gains nothing
+// with these rings: an item consumes one group more than it has steps, so the next item's group 1
+// cannot be issued before that item starts.)
 // Every wait on an mbarrier gives up after about a second and raises FLAG_TIMEOUT.
 #pragma once
 #include "fused_step.cuh"
@@ -80,24 +84,34 @@ __device__ __forceinline__ void tma_load_2d(void *dst, const void *map, int x, i
 
 constexpr long long TMA_WAIT_LIMIT = 2000000000LL;   // SM cycles: about one second
 
-// shared memory of a TMA strip CTA (byte offsets from a 128-byte aligned base)
-template <bool ENERGY>
+// shared memory of a TMA strip CTA (byte offsets from a 128-byte aligned base). Q16: the
+// coefficients arrive as 16-bit codes in rows of TMA_QW columns (from 8 columns before the strip's
+// core), each block padded to a multiple of 128 bytes (TMA destinations are 128-byte aligned)
+template <bool ENERGY, bool Q16 = false>
 struct TmaLayout {
+    // ring lengths in blocks: the arrays whose x stencils reach around the row, the other loaded
+    // arrays; NB mbarriers track the copy groups in flight
+    static constexpr int R3 = 3, R2 = 2, NB = 3;
     static constexpr int ROW = TMA_W * 4;              // one FP32 row of the strip
     static constexpr int BLK = TMA_ROWS * ROW;         // one block of rows
+    static constexpr int CROW = Q16 ? TMA_QW * 2 : ROW;                       // one coefficient row
+    static constexpr int CBOX = TMA_ROWS * CROW;                              // bytes a coefficient copy lands
+    static constexpr int CBLK = (CBOX + 127) / 128 * 128;                     // one coefficient block
     static constexpr int WBLK = TMA_ROWS * TMA_W * 8;  // one block of FP64 energy weights
     static constexpr int PAD = 128;                    // lanes 0 / 31 read up to 8 bytes beyond a row
-    static constexpr int o_nn = PAD, o_mm0 = o_nn + 3 * BLK, o_mm1 = o_mm0 + 3 * BLK;
-    static constexpr int o_mn = o_mm1 + 3 * BLK, o_nm = o_mn + 2 * BLK, o_pmn = o_nm + 2 * BLK,
-                         o_pnm = o_pmn + 2 * BLK, o_mu = o_pnm + 2 * BLK, o_lam = o_mu + 2 * BLK,
-                         o_m2 = o_lam + 2 * BLK;
-    static constexpr int o_vmn = o_m2 + 2 * BLK, o_vnm = o_vmn + 2 * BLK;   // new velocities
-    static constexpr int o_w = o_vnm + 2 * BLK;                              // 5 weight rings
-    // 3 mbarriers at o_bar, the energy reduction's 3 x FS_WARPS doubles at o_bar + 32
-    static constexpr int o_bar = o_w + (ENERGY ? 5 * 2 * WBLK : 0) + PAD;
-    static constexpr int bytes = o_bar + 128 + 128;                         // + alignment slack
+    static constexpr int o_nn = PAD, o_mm0 = o_nn + R3 * BLK, o_mm1 = o_mm0 + R3 * BLK;
+    static constexpr int o_mn = o_mm1 + R3 * BLK, o_nm = o_mn + R2 * BLK, o_pmn = o_nm + R2 * BLK,
+                         o_pnm = o_pmn + R2 * CBLK, o_mu = o_pnm + R2 * CBLK, o_lam = o_mu + R2 * CBLK,
+                         o_m2 = o_lam + R2 * CBLK;
+    static constexpr int o_vmn = o_m2 + R2 * CBLK, o_vnm = o_vmn + 2 * BLK;  // new velocities (2 blocks)
+    static constexpr int o_w = o_vnm + 2 * BLK;                               // 5 weight rings
+    // NB mbarriers at o_bar, the item index at o_item, the energy reduction's 3 x FS_WARPS doubles
+    // at o_red
+    static constexpr int o_bar = o_w + (ENERGY ? 5 * R2 * WBLK : 0) + PAD;
+    static constexpr int o_item = o_bar + 64, o_red = o_bar + 72;
+    static constexpr int bytes = o_red + 8 * 3 * FS_WARPS + 128;              // + alignment slack
     static constexpr unsigned tx0 = 3 * BLK;                                // group 0
-    static constexpr unsigned tx = 10 * BLK + (ENERGY ? 5 * WBLK : 0);      // groups >= 1
+    static constexpr unsigned tx = 5 * BLK + 5 * CBOX + (ENERGY ? 5 * WBLK : 0);   // groups >= 1
 };
 
 __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
@@ -121,11 +135,12 @@ __device__ __forceinline__ float f4(const float4 &v, int e) { return e == 0 ? v.
 }  // namespace
 
 // one TMA strip CTA: strip `tstrip`, row segment `tseg`; returns false if a copy timed out
-template <bool ENERGY>
+template <bool ENERGY, bool Q16>
 __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &maps, int tstrip, int tseg, int it,
                               int rcv_b, int rcv_e, EAcc &E, unsigned char *base)
 {
-    using L = TmaLayout<ENERGY>;
+    using L = TmaLayout<ENERGY, Q16>;
+    constexpr int R3 = L::R3, R2 = L::R2, NB = L::NB;
     using C = float;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int y0 = TMA_Y0 + tstrip * TMA_CORE;   // the strip's first core column
@@ -172,41 +187,58 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
 
     const unsigned char *mp = maps.m[0];
     auto map = [&](int k) { return static_cast<const void *>(mp + 128 * k); };
-    // copy group G (see the head of the file); one thread issues it
+    // copy group G (see the head of the file): lane 0 of every warp issues its share of the copies
+    // (so that no warp arrives at the CTA's barriers much later than the others), warp 0 also the
+    // group's expected bytes on its mbarrier (a copy may complete before them: the phase waits for
+    // that one arrival)
     auto issue = [&](int G) {
-        unsigned long long *b = bar + G % 3;
-        const int s3 = G % 3;
-        mbar_expect_tx(b, G == 0 ? L::tx0 : L::tx);
+        unsigned long long *b = bar + G % NB;
+        const int s3 = G % R3;
         const int rs = x0 - 4 + 4 * G;
-        tma_load_2d(base + L::o_nn + s3 * L::BLK, map(TM_NN), xs, rs, b);
-        tma_load_2d(base + L::o_mm0 + s3 * L::BLK, map(TM_MM0), xs, rs, b);
-        tma_load_2d(base + L::o_mm1 + s3 * L::BLK, map(TM_MM1), xs, rs, b);
-        if (G == 0) return;
-        const int g = G - 1, s2 = g & 1;
+        const int g = G - 1, s2 = (G + 1) % R2;   // (g mod 2, for g >= 0)
         const int rv = x0 - 2 + 4 * g, rt = x0 - 4 + 4 * g;
-        tma_load_2d(base + L::o_mn + s2 * L::BLK, map(TM_MN), xs, rv, b);
-        tma_load_2d(base + L::o_nm + s2 * L::BLK, map(TM_NM), xs, rv, b);
-        tma_load_2d(base + L::o_pmn + s2 * L::BLK, map(TM_PMN), xs, rv, b);
-        tma_load_2d(base + L::o_pnm + s2 * L::BLK, map(TM_PNM), xs, rv, b);
-        tma_load_2d(base + L::o_mu + s2 * L::BLK, map(TM_MU), xs, rt, b);
-        tma_load_2d(base + L::o_lam + s2 * L::BLK, map(TM_LAM), xs, rt, b);
-        tma_load_2d(base + L::o_m2 + s2 * L::BLK, map(TM_M2), xs, rt, b);
-        if constexpr (ENERGY) {
-            tma_load_2d(base + L::o_w + (0 * 2 + s2) * L::WBLK, map(TM_WMN), xs, rv, b);
-            tma_load_2d(base + L::o_w + (1 * 2 + s2) * L::WBLK, map(TM_WNM), xs, rv, b);
-            tma_load_2d(base + L::o_w + (2 * 2 + s2) * L::WBLK, map(TM_WNN), xs, rt, b);
-            tma_load_2d(base + L::o_w + (3 * 2 + s2) * L::WBLK, map(TM_WM3), xs, rt, b);
-            tma_load_2d(base + L::o_w + (4 * 2 + s2) * L::WBLK, map(TM_WM4), xs, rt, b);
+        const int xc = Q16 ? y0 - 8 : xs;   // (16-bit codes: x on a 16-byte boundary)
+        switch (warp) {
+        case 0:
+            mbar_expect_tx(b, G == 0 ? L::tx0 : L::tx);
+            tma_load_2d(base + L::o_nn + s3 * L::BLK, map(TM_NN), xs, rs, b);
+            if (G == 0) break;
+            tma_load_2d(base + L::o_pmn + s2 * L::CBLK, map(TM_PMN), xc, rv, b);
+            tma_load_2d(base + L::o_pnm + s2 * L::CBLK, map(TM_PNM), xc, rv, b);
+            if constexpr (ENERGY) tma_load_2d(base + L::o_w + (3 * R2 + s2) * L::WBLK, map(TM_WM3), xs, rt, b);
+            break;
+        case 1:
+            tma_load_2d(base + L::o_mm0 + s3 * L::BLK, map(TM_MM0), xs, rs, b);
+            if (G == 0) break;
+            tma_load_2d(base + L::o_mu + s2 * L::CBLK, map(TM_MU), xc, rt, b);
+            tma_load_2d(base + L::o_lam + s2 * L::CBLK, map(TM_LAM), xc, rt, b);
+            if constexpr (ENERGY) tma_load_2d(base + L::o_w + (4 * R2 + s2) * L::WBLK, map(TM_WM4), xs, rt, b);
+            break;
+        case 2:
+            tma_load_2d(base + L::o_mm1 + s3 * L::BLK, map(TM_MM1), xs, rs, b);
+            if (G == 0) break;
+            tma_load_2d(base + L::o_m2 + s2 * L::CBLK, map(TM_M2), xc, rt, b);
+            if constexpr (ENERGY) {
+                tma_load_2d(base + L::o_w + (0 * R2 + s2) * L::WBLK, map(TM_WMN), xs, rv, b);
+                tma_load_2d(base + L::o_w + (2 * R2 + s2) * L::WBLK, map(TM_WNN), xs, rt, b);
+            }
+            break;
+        default:
+            if (G == 0) break;
+            tma_load_2d(base + L::o_mn + s2 * L::BLK, map(TM_MN), xs, rv, b);
+            tma_load_2d(base + L::o_nm + s2 * L::BLK, map(TM_NM), xs, rv, b);
+            if constexpr (ENERGY) tma_load_2d(base + L::o_w + (1 * R2 + s2) * L::WBLK, map(TM_WNM), xs, rv, b);
+            break;
         }
     };
 
     if (threadIdx.x == 0) {
-        for (int k = 0; k < 3; k++) mbar_init(bar + k, 1);
+        for (int k = 0; k < NB; k++) mbar_init(bar + k, 1);
         mbar_init_fence();
     }
     __syncthreads();
-    int issued = -1;   // (thread 0) the last group issued
-    if (threadIdx.x == 0) {
+    int issued = -1;   // (lane 0 of each warp) the last group issued
+    if (lane == 0) {
         for (int G = 0; G <= 2 && G <= Q; G++) issue(G);
         issued = Q < 2 ? Q : 2;
     }
@@ -215,7 +247,20 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
     bool bad = false;
     const float st0 = op.st[0], st1 = op.st[1], st2 = op.st[2], st3 = op.st[3];
     auto rowp = [&](int off, int slot) { return reinterpret_cast<const float *>(base + off) + slot * TMA_W; };
-    auto wrowp = [&](int k, int slot) { return reinterpret_cast<const double *>(base + L::o_w + k * 2 * L::WBLK) + slot * TMA_W; };
+    // this thread's 4 coefficients of ring row `row` (0..7: block row) of the ring at `off`, of
+    // field slot f: FP32 values, or 16-bit codes decoded as qlo + qstep * code
+    auto coef4 = [&](int off, int row, int f) -> float4 {
+        if constexpr (Q16) {
+            const unsigned char *r = base + off + (row >> 2) * L::CBLK + (row & 3) * L::CROW;
+            const uint2 u = *reinterpret_cast<const uint2 *>(r + 2 * (cl + 4));
+            const float lo = a.qlo[f], st = a.qstep[f];
+            return make_float4(add(lo, mul(st, (float)(u.x & 0xffffu))), add(lo, mul(st, (float)(u.x >> 16))),
+                               add(lo, mul(st, (float)(u.y & 0xffffu))), add(lo, mul(st, (float)(u.y >> 16))));
+        } else {
+            return lds4(rowp(off, row) + cl);
+        }
+    };
+    auto wrowp = [&](int k, int slot) { return reinterpret_cast<const double *>(base + L::o_w + k * R2 * L::WBLK) + slot * TMA_W; };
     auto st4 = [&](int f, int row, const float (&v)[4]) {
         *reinterpret_cast<float4 *>(a.out[f] + row * pitch + c0) = make_float4(v[0], v[1], v[2], v[3]);
     };
@@ -228,16 +273,18 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
     };
 
     for (int q = 0; q < Q; q++) {
-        if (threadIdx.x == 0 && q >= 1 && q + 2 <= Q) {   // into the slots step q - 1 freed
+        if (lane == 0 && q >= 1 && q + 2 <= Q) {   // into the slots step q - 1 freed
             fence_proxy_async();
             issue(q + 2);
             issued = q + 2;
         }
         for (int G = waited + 1; G <= q + 1 && !bad; G++) {
-            bad = !mbar_wait(bar + G % 3, (unsigned)((G / 3) & 1), TMA_WAIT_LIMIT);
+            bad = !mbar_wait(bar + G % NB, (unsigned)((G / NB) & 1), TMA_WAIT_LIMIT);
             if (!bad) waited = G;
         }
-        const int s3a = q % 3, s3b = (q + 1) % 3, s2 = q & 1, s2p = s2 ^ 1;
+        // 3-block rings: blocks q, q + 1; other loaded rings: block q (slot sl); new-velocity
+        // rings: block q (slot s2) and q - 1 (s2p)
+        const int s3a = q % R3, s3b = (q + 1) % R3, sl = q % R2, s2 = q & 1, s2p = s2 ^ 1;
         // window row k (0..7) of a 3-block ring: rows x0 - 4 + 4q + k
         auto w3 = [&](int off, int k) { return rowp(off, (k < 4 ? s3a : s3b) * 4 + (k & 3)); };
         // row k (-4..3) of a new-velocity ring relative to row x0 - 2 + 4q
@@ -253,18 +300,19 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                 const float *m1row = w3(L::o_mm1, warp + 2);
                 float t[7];
                 taps_left2(m1row, cl, t, lds4(m1row + cl));
-                const float4 old = lds4(rowp(L::o_mn, s2 * 4 + warp) + cl);
-                const float4 p = lds4(rowp(L::o_pmn, s2 * 4 + warp) + cl);
+                const float4 old = lds4(rowp(L::o_mn, sl * 4 + warp) + cl);
+                const float4 p = coef4(L::o_pmn, sl * 4 + warp, F_MN);
                 float v[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
-                    float vx = 0.f;
-                    vx = add(vx, mul(f4(n1, e), st0));
+                    // the reference sums from 0: 0 + x differs from x only for x = -0, and a
+                    // difference in the sign of a zero sum vanishes in r = 0 + vx * p below (and
+                    // in any later sum that has a non-zero term): bit-identical results
+                    float vx = mul(f4(n1, e), st0);
                     vx = add(vx, mul(f4(n2, e), st1));
                     vx = add(vx, mul(f4(n3, e), st2));
                     vx = add(vx, mul(f4(n4, e), st3));
-                    float vy = 0.f;
-                    vy = add(vy, mul(t[e], st0));
+                    float vy = mul(t[e], st0);
                     vy = add(vy, mul(t[e + 1], st1));
                     vy = add(vy, mul(t[e + 2], st2));
                     vy = add(vy, mul(t[e + 3], st3));
@@ -281,7 +329,7 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                     for (int e = 0; e < 4; e++) nf = __fmaf_rn(v[e], 0.f, nf);
                     if (nr > 0 || rmany) record(F_MN, j, v);
                     if constexpr (ENERGY) {
-                        const double *wr = wrowp(0, s2 * 4 + warp) + cl;
+                        const double *wr = wrowp(0, sl * 4 + warp) + cl;
 #pragma unroll
                         for (int e = 0; e < 4; e++) E.k = add(E.k, mul(mul((double)v[e], wr[e]), (double)v[e]));
                     }
@@ -294,18 +342,16 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                 const float *nrow = w3(L::o_nn, warp + 2);
                 float t[7];
                 taps_left1(nrow, cl, t, lds4(nrow + cl));
-                const float4 old = lds4(rowp(L::o_nm, s2 * 4 + warp) + cl);
-                const float4 p = lds4(rowp(L::o_pnm, s2 * 4 + warp) + cl);
+                const float4 old = lds4(rowp(L::o_nm, sl * 4 + warp) + cl);
+                const float4 p = coef4(L::o_pnm, sl * 4 + warp, F_NM);
                 float v[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
-                    float vy = 0.f;
-                    vy = add(vy, mul(t[e], st0));
+                    float vy = mul(t[e], st0);
                     vy = add(vy, mul(t[e + 1], st1));
                     vy = add(vy, mul(t[e + 2], st2));
                     vy = add(vy, mul(t[e + 3], st3));
-                    float vx = 0.f;
-                    vx = add(vx, mul(f4(a0, e), st0));
+                    float vx = mul(f4(a0, e), st0);
                     vx = add(vx, mul(f4(a1, e), st1));
                     vx = add(vx, mul(f4(a2, e), st2));
                     vx = add(vx, mul(f4(a3, e), st3));
@@ -322,7 +368,7 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                     for (int e = 0; e < 4; e++) nf = __fmaf_rn(v[e], 0.f, nf);
                     if (nr > 0 || rmany) record(F_NM, j, v);
                     if constexpr (ENERGY) {
-                        const double *wr = wrowp(1, s2 * 4 + warp) + cl;
+                        const double *wr = wrowp(1, sl * 4 + warp) + cl;
 #pragma unroll
                         for (int e = 0; e < 4; e++) E.k = add(E.k, mul(mul((double)v[e], wr[e]), (double)v[e]));
                     }
@@ -344,17 +390,15 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                 float t[7];
                 taps_left2(nmrow, cl, t, lds4(nmrow + cl));
                 const float4 old = lds4(w3(L::o_nn, warp) + cl);
-                const float4 mu = lds4(rowp(L::o_mu, s2 * 4 + warp) + cl);
+                const float4 mu = coef4(L::o_mu, sl * 4 + warp, F_NN);
                 float v[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
-                    float vx = 0.f;
-                    vx = add(vx, mul(f4(m0, e), st0));
+                    float vx = mul(f4(m0, e), st0);
                     vx = add(vx, mul(f4(m1, e), st1));
                     vx = add(vx, mul(f4(m2, e), st2));
                     vx = add(vx, mul(f4(m3, e), st3));
-                    float vy = 0.f;
-                    vy = add(vy, mul(t[e], st0));
+                    float vy = mul(t[e], st0);
                     vy = add(vy, mul(t[e + 1], st1));
                     vy = add(vy, mul(t[e + 2], st2));
                     vy = add(vy, mul(t[e + 3], st3));
@@ -369,7 +413,7 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                 for (int e = 0; e < 4; e++) nf = __fmaf_rn(v[e], 0.f, nf);
                 if (nr > 0 || rmany) record(F_NN, i, v);
                 if constexpr (ENERGY) {
-                    const double *wr = wrowp(2, s2 * 4 + warp) + cl;
+                    const double *wr = wrowp(2, sl * 4 + warp) + cl;
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
                         E.p0 = add(E.p0, mul(mul((double)f4(old, e), wr[e]), (double)f4(old, e)));
@@ -384,17 +428,15 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                 float t[7];
                 taps_left1(mnrow, cl, t, lds4(mnrow + cl));
                 const float4 o0 = lds4(w3(L::o_mm0, warp) + cl), o1 = lds4(w3(L::o_mm1, warp) + cl);
-                const float4 lam = lds4(rowp(L::o_lam, s2 * 4 + warp) + cl), m2c = lds4(rowp(L::o_m2, s2 * 4 + warp) + cl);
+                const float4 lam = coef4(L::o_lam, sl * 4 + warp, F_MM0), m2c = coef4(L::o_m2, sl * 4 + warp, F_MM1);
                 float s0[4], s1[4];
 #pragma unroll
                 for (int e = 0; e < 4; e++) {
-                    float vx = 0.f;
-                    vx = add(vx, mul(f4(n0, e), st0));
+                    float vx = mul(f4(n0, e), st0);
                     vx = add(vx, mul(f4(n1, e), st1));
                     vx = add(vx, mul(f4(n2, e), st2));
                     vx = add(vx, mul(f4(n3, e), st3));
-                    float vy = 0.f;
-                    vy = add(vy, mul(t[e], st0));
+                    float vy = mul(t[e], st0);
                     vy = add(vy, mul(t[e + 1], st1));
                     vy = add(vy, mul(t[e + 2], st2));
                     vy = add(vy, mul(t[e + 3], st3));
@@ -423,7 +465,7 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                     record(F_MM1, i, s1);
                 }
                 if constexpr (ENERGY) {
-                    const double *w3r = wrowp(3, s2 * 4 + warp) + cl, *w4r = wrowp(4, s2 * 4 + warp) + cl;
+                    const double *w3r = wrowp(3, sl * 4 + warp) + cl, *w4r = wrowp(4, sl * 4 + warp) + cl;
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
                         const double a0 = f4(o0, e), a1 = f4(o1, e), b0 = s0[e], b1 = s1[e];
@@ -442,7 +484,7 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
     if (nf != 0.f) atomicOr(a.flags, FLAG_NONFINITE);
     if (!bad) {   // every copy has landed and every thread is past the last barrier
         if (threadIdx.x == 0)
-            for (int k = 0; k < 3; k++) mbar_inval(bar + k);
+            for (int k = 0; k < NB; k++) mbar_inval(bar + k);
         return true;
     }
     {
@@ -452,12 +494,12 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
             atomicOr(a.flags, FLAG_TIMEOUT);
             // the last group issued on each barrier (the earlier ones on it completed before it
             // was issued)
-            for (int G = issued - 2 > 0 ? issued - 2 : 0; G <= issued; G++)
-                mbar_wait(bar + G % 3, (unsigned)((G / 3) & 1), TMA_WAIT_LIMIT);
+            for (int G = issued - NB + 1 > 0 ? issued - NB + 1 : 0; G <= issued; G++)
+                mbar_wait(bar + G % NB, (unsigned)((G / NB) & 1), TMA_WAIT_LIMIT);
         }
         __syncthreads();
         if (threadIdx.x == 0)
-            for (int k = 0; k < 3; k++) mbar_inval(bar + k);
+            for (int k = 0; k < NB; k++) mbar_inval(bar + k);
         return false;
     }
 }
@@ -537,7 +579,7 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<float, ENERGY>()
     step_done(a, it);
 }
 
-template <bool ENERGY>
+template <bool ENERGY, bool Q16 = false>
 __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
     k_elastic_tma(FusedArgs<float, float> a, const __grid_constant__ TmaMaps maps)
 {
@@ -545,7 +587,7 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
     unsigned char *base = reinterpret_cast<unsigned char *>((reinterpret_cast<unsigned long>(tma_smem_raw) + 127) & ~127ul);
     const int it = *a.step;
     const int n_side = a.n_zone * a.n_bstrip + a.n_octa;   // receiver lists: the side CTAs' come first
-    int *item_s = reinterpret_cast<int *>(base + TmaLayout<ENERGY>::o_bar + 24);
+    int *item_s = reinterpret_cast<int *>(base + TmaLayout<ENERGY, Q16>::o_item);
     EAcc E;
     // a persistent grid: each CTA takes (segment, strip) items until none is left, so CTAs that
     // find their SM busy with side CTAs at first simply take fewer items
@@ -556,9 +598,9 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
         __syncthreads();
         if (t >= a.n_tcta) break;
         const int rcv_b = a.rcv_off[n_side + t], rcv_e = a.rcv_off[n_side + t + 1];
-        if (!tma_strip_cta<ENERGY>(a, maps, t % a.n_tstrip, t / a.n_tstrip, it, rcv_b, rcv_e, E, base)) break;
+        if (!tma_strip_cta<ENERGY, Q16>(a, maps, t % a.n_tstrip, t / a.n_tstrip, it, rcv_b, rcv_e, E, base)) break;
     }
-    cta_energy<ENERGY>(a, E, reinterpret_cast<double *>(base + TmaLayout<ENERGY>::o_bar + 32), it);
+    cta_energy<ENERGY>(a, E, reinterpret_cast<double *>(base + TmaLayout<ENERGY, Q16>::o_red), it);
     step_done(a, it);
 }
 
