@@ -386,7 +386,25 @@ def run_reference_arm(args, dist: Dist):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": workload_desc(),
             "cpu_baseline": {"value": gpts, "unit": UNIT, "cores": procs, "kind": kind, "sample": sample},
             "e2e": {"value": gpts, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if not args.no_ref_gpu:
+        line["gpu_executable"] = reference_gpu_executable()
     print(json.dumps(line), flush=True)
+
+
+def reference_gpu_executable():
+    """The reference's own GPU program (nvcc_device_FDM_2D.cu, unmodified, built for sm_100a) on
+    the 2048^2 grid at the workload's dt, energy on as it requires: ms per step from two runs of
+    200 and 1200 steps (context beside the CPU arm, not its value)."""
+    import shutil
+    if shutil.which("nvidia-smi") is None:
+        return {"unavailable": "no GPU visible"}
+    try:
+        from oracle import ref_gpu_timing
+        dt = float(build_model(0, MX)[3])
+        rec = ref_gpu_timing.time_reference_gpu(MX, DEN_DX, dt, F0, DELAY, (200, 1200))
+    except Exception as e:  # a failed run is reported, not fatal to the CPU arm
+        return {"unavailable": f"{type(e).__name__}: {e}"[:200]}
+    return rec if rec is not None else {"unavailable": "oracle/_ref/twref_elastic_gpu_f32 not built"}
 
 
 # ---------------------------------------------------------------- our arm
@@ -1071,6 +1089,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=30)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-target", action="store_true", help="skip the 8192^2 sub-record of the default run")
+    ap.add_argument("--no-ref-gpu", action="store_true", help="reference arm: skip timing the reference's GPU program")
     ap.add_argument("--variant", default="", help="mixed workload: comma-separated variants to run "
                     "(storage-compensation[-c16], e.g. f32-00); all by default")
     ap.add_argument("--workload", choices=["elastic2048", "acoustic512", "mixed", "batch", "adjoint", "variants"],
