@@ -1,6 +1,7 @@
-"""Host logic of the rank-parallel slab decomposition (no GPU): the cuts, the deadlock-free
-exchange schedule, and three `gloo` ranks swapping halo rows through the same code path with a
-host stand-in for the library's slab handle (pack / unpack of four rows per edge)."""
+"""Host logic of the rank-parallel slab decomposition (no GPU): the cuts, the edges and message
+tags, and three `gloo` ranks swapping halo rows through the same code path (one batch of
+non-blocking sends and receives straight between the arrays' rows) with a host stand-in for the
+library's slab handle. Not run on several GPUs: NCCL needs one GPU per rank."""
 import importlib.util
 import os
 import socket
@@ -31,50 +32,50 @@ def test_partition():
         sl.partition(40, 3)
 
 
-def test_schedule_pairs_every_edge_once_per_phase():
+def test_edges_and_tags_pair_every_send_with_one_receive():
     sl = load_slabs()
     for world in (1, 2, 3, 4, 7):
-        seen = {}
+        sends, recvs = [], []
         for r in range(world):
-            for phase, peer, side in sl.schedule(r, world):
-                seen.setdefault((phase, min(r, peer), max(r, peer)), []).append((r, side))
-        assert len(seen) == world - 1
-        for (phase, a, b), ends in seen.items():
-            assert b == a + 1 and phase == a % 2 and sorted(ends) == [(a, 1), (b, 0)]
+            for side, peer in sl.edges(r, world):
+                assert peer == (r - 1 if side == 0 else r + 1)
+                for f in (0, 3, 7):
+                    sends.append((r, peer, sl.tag(f, downward=side == 1)))
+                    recvs.append((peer, r, sl.tag(f, downward=side == 0)))
+        assert sorted(sends) == sorted(recvs) and len(set(sends)) == len(sends)
 
 
 class FakeSlab:
-    """Host stand-in: local rows [off, off + n) of a global (Mx, W) array of float64."""
+    """Host stand-in: local rows [off, off + n) of global (Mx, W) arrays of float64, one per slot
+    (two slots of different widths, so that a send paired with the wrong receive shows)."""
 
-    def __init__(self, glob, r0, r1):
-        Mx = glob.shape[0]
+    WIDTHS = {0: 5, 3: 7}
+
+    def __init__(self, globs, r0, r1):
+        Mx = globs[0].shape[0]
         self.off = r0 - H if r0 > 0 else 0
         end = r1 + H if r1 < Mx else Mx
         self.own0, self.own1 = r0 - self.off, r1 - self.off
-        self.a = np.full((end - self.off, glob.shape[1]), np.nan)
-        self.a[self.own0:self.own1] = glob[r0:r1]   # halos unknown until exchanged
-
-    def halo_bytes(self, side):
-        return H * self.a.shape[1] * 8
+        self.a = {}
+        for f, g in globs.items():
+            a = np.full((end - self.off, g.shape[1]), np.nan)
+            a[self.own0:self.own1] = g[r0:r1]   # halos unknown until exchanged
+            self.a[f] = a
 
     def rows(self, side, recv):
         if side == 0:
             return slice(self.own0 - H, self.own0) if recv else slice(self.own0, self.own0 + H)
         return slice(self.own1, self.own1 + H) if recv else slice(self.own1 - H, self.own1)
 
-    def pack(self, side, ptr):
-        import ctypes
-        blk = np.ascontiguousarray(self.a[self.rows(side, 0)])
-        ctypes.memmove(ptr, blk.ctypes.data, blk.nbytes)
-
-    def unpack(self, side, ptr):
-        import ctypes
-        blk = np.empty_like(self.a[self.rows(side, 1)])
-        ctypes.memmove(blk.ctypes.data, ptr, blk.nbytes)
-        self.a[self.rows(side, 1)] = blk
+    def halo_spans(self, side, recv):
+        return [(f, a[self.rows(side, recv)].reshape(-1).view(np.uint8)) for f, a in self.a.items()]
 
     def sync(self):
         pass
+
+
+def _globs(Mx):
+    return {f: np.arange(Mx * w, dtype=np.float64).reshape(Mx, w) * (f + 1) for f, w in FakeSlab.WIDTHS.items()}
 
 
 def _rank_main(rank, world, port, q):
@@ -82,11 +83,10 @@ def _rank_main(rank, world, port, q):
     import torch.distributed as dist
     dist.init_process_group("gloo", rank=rank, world_size=world)
     sl = load_slabs()
-    Mx, W = 72, 5
-    glob = np.arange(Mx * W, dtype=np.float64).reshape(Mx, W)
+    Mx = 72
     cuts = sl.partition(Mx, world)
-    fake = FakeSlab(glob, cuts[rank], cuts[rank + 1])
-    run = sl.SlabRun(None, dist, Mx, W, 1, Mx, 1e-3, slab=fake, device=None)
+    fake = FakeSlab(_globs(Mx), cuts[rank], cuts[rank + 1])
+    run = sl.SlabRun(None, dist, Mx, 5, 1, Mx, 1e-3, slab=fake, device=None)
     run.exchange()
     dist.destroy_process_group()
     q.put((rank, fake.off, fake.a))
@@ -105,6 +105,7 @@ def test_three_gloo_ranks_fill_their_halos():
     for p in procs:
         p.join(90)
         assert p.exitcode == 0
-    glob = np.arange(72 * 5, dtype=np.float64).reshape(72, 5)
-    for rank, off, a in (q.get() for _ in range(3)):
-        assert np.array_equal(a, glob[off:off + a.shape[0]]), rank   # owned rows and both halos
+    globs = _globs(72)
+    for rank, off, arrs in (q.get() for _ in range(3)):
+        for f, a in arrs.items():
+            assert np.array_equal(a, globs[f][off:off + a.shape[0]]), (rank, f)   # owned rows and both halos

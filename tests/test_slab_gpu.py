@@ -1,7 +1,7 @@
 """Slab decomposition of one elastic grid (tw_create_slab / tw_slab_exchange / tw_slab_run), on
 one GPU: the grid cut into slabs along x, every slab stepped and the halos exchanged after each
-step (by copies, by packed buffers, or by the step kernel's own stores into the neighbours' halo
-rows), must give the whole grid's fields on every owned row and its traces bit for bit, and its
+step (by copies, by packed buffers, by copies between the per-array spans the rank-parallel
+driver hands to NCCL, or by the step kernel's own stores into the neighbours' halo rows), must give the whole grid's fields on every owned row and its traces bit for bit, and its
 energies to 1e-12 (sums in another order). Covers the free-surface zones of the first and last
 slab, open inner edges, compensation arrays in the halo, sources and receivers in any slab."""
 import numpy as np
@@ -34,6 +34,30 @@ def packed_exchange(up, lo):
     lo.sync()
 
 
+def spans_exchange(up, lo):
+    """The halo swap the rank-parallel driver makes with NCCL (tpu-wave_b200/slabs.py): every
+    array's rows straight from the owned span into the neighbour's halo span, here by device
+    copies between the same zero-copy views."""
+    import importlib.util
+    import os
+    import torch
+    spec = importlib.util.spec_from_file_location(
+        "twave_slabs", os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tpu-wave_b200", "slabs.py"))
+    sl = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(sl)
+    up.sync()
+    lo.sync()
+    for src_h, src_side, dst_h, dst_side in ((up, 1, lo, 0), (lo, 0, up, 1)):
+        src, dst = dict(src_h.halo_spans(src_side, 0)), dict(dst_h.halo_spans(dst_side, 1))
+        assert src.keys() == dst.keys() and len(src) in (5, 10)
+        for f in src:
+            assert src[f][1] == dst[f][1]
+            a = torch.as_tensor(sl._DeviceSpan(*src[f]), device="cuda:0")
+            b = torch.as_tensor(sl._DeviceSpan(*dst[f]), device="cuda:0")
+            b.copy_(a)
+    torch.cuda.synchronize()
+
+
 def run(tw, case, prec, cuts, f0, r0, Nt, slab=True, mode="copy"):
     shp = (case.Mx + 2, case.My + 2)
     kw = dict(precision=prec, cpst=case.cpst, central_f=case.central_f, time_delay=case.time_delay, max_steps=Nt)
@@ -62,6 +86,8 @@ def run(tw, case, prec, cuts, f0, r0, Nt, slab=True, mode="copy"):
         for up, lo in zip(hs[:-1], hs[1:]):
             if mode == "packed":
                 packed_exchange(up, lo)
+            elif mode == "spans":
+                spans_exchange(up, lo)
             else:
                 up.exchange(lo)
     if mode != "fused":   # after a linked run each handle alone is ordered after its neighbours' stores
@@ -82,7 +108,7 @@ def run(tw, case, prec, cuts, f0, r0, Nt, slab=True, mode="copy"):
     return fields, traces, energy
 
 
-@pytest.mark.parametrize("mode", ["copy", "packed", "fused"])
+@pytest.mark.parametrize("mode", ["copy", "packed", "spans", "fused"])
 @pytest.mark.parametrize("prec,cpst", [("f32", "00"), ("f64", "6R"), ("f32", "3C")])
 @pytest.mark.parametrize("cuts", [(0, 24, 48, 72), (0, 40, 72), (0, 16, 56, 72)])
 def test_slabs_equal_the_whole_grid(prec, cpst, cuts, mode):

@@ -235,6 +235,22 @@ class Solver:
         self.row_off, self.own = int(inf.row_off), (int(inf.own_rows[0]), int(inf.own_rows[1]))
         return self
 
+    def halo_spans(self, side: int, recv: int) -> list:
+        """(slot, (device pointer, bytes)) of every state array's rows at one edge (tw_slab_halo):
+        the owned rows the neighbour on `side` (0 top, 1 bottom) needs (recv 0) or this slab's halo
+        rows there (recv 1), of the current buffers, each one contiguous span (the rows with the
+        pitch padding between them)."""
+        out = []
+        for f in range(10):
+            ptr, rows, rb, pb = C.c_void_p(), C.c_long(), C.c_long(), C.c_long()
+            rc = lib().tw_slab_halo(self.h, side, recv, f, C.byref(ptr), C.byref(rows), C.byref(rb), C.byref(pb))
+            if rc != 0:
+                if f < 5:
+                    _ok(rc, "tw_slab_halo")
+                continue   # no compensation array in this slot
+            out.append((f, (ptr.value, (rows.value - 1) * pb.value + rb.value)))
+        return out
+
     def halo_bytes(self, side: int) -> int:
         n = C.c_long()
         _ok(lib().tw_slab_pack(self.h, side, None, C.byref(n)), "tw_slab_pack")
