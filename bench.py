@@ -971,6 +971,19 @@ def run_adjoint(args):
         for k in g:
             g[k] = g[k] + out[k]
 
+    # binomial checkpointing in a fixed number of state slots (tw_adjoint_gradient_revolve): the
+    # first shot's gradient with 8 and 24 slots against the checkpoints every 50 steps above
+    revolve = []
+    for n_slots in (8, 24):
+        s = make("f32", rho, vp, vs, shots[0])
+        torch.cuda.synchronize()
+        t0 = time.monotonic()
+        out = s.adjoint_gradient(K, obs[0], slots=n_slots)
+        dt_s = time.monotonic() - t0
+        s.close()
+        fwd_steps, _ = tw.revolve_plan(K, n_slots)
+        revolve.append({"slots": n_slots, "seconds": dt_s, "forward_steps": fwd_steps,
+                        "state_bytes": n_slots * 5 * (n + 1) * (n + 1) * 4})
     # the same gradient in FP64, and central differences of the FP64 misfit along 8 random
     # directions (unit normal perturbations of every node value of rho, vp, vs; h = 1e-3 and 1e-4)
     obs64 = [traces("f64", rho, vp * bump, vs * bump, src) for src in shots]
@@ -1028,6 +1041,7 @@ def run_adjoint(args):
                                 "(forward sweep, segment recomputation, adjoint sweep), summed over the 8 shots"},
             "forward_ms_per_step": fwd_ms / K, "forward_gpts": n * n * K / (fwd_ms / 1e3) / 1e9,
             "gradient_seconds_per_shot": t_grad / len(shots),
+            "revolve_first_shot": revolve,
             "gradient_over_forward_time": (t_grad / len(shots)) / (fwd_ms / 1e3),
             "misfit": J0, "finite_differences": {"field_precision": "f64 (FD and its adjoint); f32 adjoint compared",
                                                  "directions": fd_rows,

@@ -319,3 +319,39 @@ def test_gradient_at_the_c5_size_matches_central_differences():
         print(f"direction {k}: rel err h=1e-3 {e1:.3e}, h=5e-4 {e2:.3e}, Richardson {er:.3e}")
         assert e2 <= e1 * 0.35 + 1e-9          # second-order convergence of the differences
         assert er <= 1e-4, (k, e1, e2, er)      # the extrapolated difference agrees with the adjoint
+
+
+@pytest.mark.parametrize("slots", [0, 4])
+def test_fp32_gradient_on_a_tma_handle_equals_the_per_warp_kernels(slots, monkeypatch):
+    """An FP32 handle wide enough for the TMA-staged step (My >= 180) steps its own buffers with
+    it, while the adjoint's recomputation (and every revolve sweep) steps between other buffers
+    with the per-warp kernel in its own layout. Both kernels give bit-identical states, so the
+    gradient, misfit, traces and final fields must equal those of the same handle made with the
+    TMA step switched off (TW_TMA=0), bit for bit, for checkpoints every 7 steps and for 4 slots."""
+    tw = load_twave()
+    Mx, My, den = 40, 300, 300
+    case = elastic_case(Mx, My, seed=31, Nt=30, rcvs=rcvs_for(Mx, My, den), den_dx=den, src=("M", "M", 2 * 20 + 1, 2 * den, 2 * 150 + 1, 2 * den))
+    ref = solver(tw, case, precision="f32")
+    assert ref.info().step_kind == 2      # the TMA-staged step
+    ref.run(case.Nt)
+    obs = ref.read_receivers() * 0.9
+    ref.close()
+    out = {}
+    for tma in ("1", "0"):
+        monkeypatch.setenv("TW_TMA", tma)
+        s = solver(tw, case, precision="f32")
+        assert s.info().step_kind == (2 if tma == "1" else 1)
+        g = s.adjoint_gradient(case.Nt, obs, ckpt_every=7, slots=slots)
+        g["traces"] = s.read_receivers()
+        g["fields"] = [s.read_field(gr, f) for gr, f in ((tw.NN, 0), (tw.MN, 0), (tw.NM, 0), (tw.MM, 0), (tw.MM, 1))]
+        s.close()
+        out[tma] = g
+    a, b = out["1"], out["0"]
+    assert a["misfit"] == b["misfit"] and a["misfit"] > 0
+    assert np.array_equal(a["traces"], b["traces"])
+    for x, y in zip(a["fields"], b["fields"]):
+        assert np.array_equal(x, y)
+    for k in a["grid"]:
+        assert np.array_equal(a["grid"][k], b["grid"][k]), k
+    for k in ("rho", "vp", "vs"):
+        assert np.array_equal(a[k], b[k]) or np.abs(a[k] - b[k]).max() <= 1e-12 * np.abs(b[k]).max(), k

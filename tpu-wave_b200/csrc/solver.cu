@@ -133,6 +133,12 @@ struct tw_solver {
     // maps per buffer parity (the input fields alternate between f and f2)
     bool tma = false;
     int n_tseg = 0, n_tstrip = 0, n_tcta = 0, n_ostrip = 0, y_tma_end = 0;
+    // the per-warp kernel's own layout on a TMA handle (n_int_seg / n_int_cta above describe the
+    // side launch there), with its per-CTA receiver lists: steps between buffers other than the
+    // handle's two (the adjoint's recomputation and revolve sweeps) run that kernel
+    int w_int_seg = 0, w_int_cta = 0;
+    int *d_rcv_off_w = nullptr, *d_rcv_list_w = nullptr;
+    int rcv_list_cap_w = 0;
     TmaMaps *tmaps = nullptr;
     cudaStream_t st_side = nullptr;   // the side launch's stream, forked from st and joined back
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
@@ -206,6 +212,7 @@ tw_solver::~tw_solver()
     }
     for (int k = 0; k < 5; k++) { release(f2[k]); release(res2[k]); }
     release(d_done); release(d_rcv_off); release(d_rcv_list); release(model);
+    release(d_rcv_off_w); release(d_rcv_list_w);
     release(src_inc); release(d_step); release(d_flags); release(d_rcv); release(d_err);
     release(d_traces); release(d_energy);
     for (int k = 0; k < 5; k++) release(coefq[k]);
@@ -434,6 +441,12 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
             return;
         }
     }
+    if (s->tma) {   // the per-warp kernel on a TMA handle: its own segmentation and receiver lists
+        a.n_int_seg = s->w_int_seg;
+        a.n_int_cta = s->w_int_cta;
+        a.rcv_off = s->d_rcv_off_w;
+        a.rcv = s->d_rcv_list_w;
+    }
     launch_fused<S, C>(a, s->d.cpst, energy, s->d.coef_fp16 == 1, st);
 }
 
@@ -620,56 +633,66 @@ int upload_receivers(tw_solver *s)
         TW_CUDA(cudaMemcpyAsync(s->d_rcv, s->rcv_tab.data(), sizeof(int) * s->rcv_tab.size(), cudaMemcpyHostToDevice, s->st));
     if (s->fused) {
         // per-CTA receiver lists: a receiver belongs to the CTA whose segment owns its row and
-        // whose strip owns its column (fused_step.cu)
-        const int nctas = s->n_int_cta + s->n_zone * s->n_bstrip + s->n_tcta;
-        std::vector<std::vector<int>> per(nctas);
-        const int Mx = (int)s->d.Mx;
-        for (int r = 0; r < n; r++) {
-            const int *q = &s->rcv_tab[4 * r];
-            if (q[0] < 0) continue;   // a receiver of another slab
-            const int row = q[2], col = q[3];
-            int zone = -1;            // the boundary zone holding the row, if any
-            for (int z = 0; z < s->n_zone; z++) {
-                const int k = s->zone_kind[z];
-                if (k == 2 || ((k == 0 || k == 3) && row < FS_ZONE) || ((k == 1 || k == 3) && row >= Mx - FS_ZONE)) zone = z;
+        // whose strip owns its column (fused_step.cu); `warp_layout` numbers the CTAs of the
+        // per-warp kernel on a TMA handle (its fallback for steps between other buffers)
+        auto build = [&](bool warp_layout, int *d_off, int **d_list, int *cap_list) -> int {
+            const bool tma = s->tma && !warp_layout;
+            const int n_int_seg = warp_layout ? s->w_int_seg : s->n_int_seg;
+            const int n_int_cta = warp_layout ? s->w_int_cta : s->n_int_cta;
+            const int nctas = n_int_cta + s->n_zone * s->n_bstrip + (tma ? s->n_tcta : 0);
+            std::vector<std::vector<int>> per(nctas);
+            const int Mx = (int)s->d.Mx;
+            for (int r = 0; r < n; r++) {
+                const int *q = &s->rcv_tab[4 * r];
+                if (q[0] < 0) continue;   // a receiver of another slab
+                const int row = q[2], col = q[3];
+                int zone = -1;            // the boundary zone holding the row, if any
+                for (int z = 0; z < s->n_zone; z++) {
+                    const int k = s->zone_kind[z];
+                    if (k == 2 || ((k == 0 || k == 3) && row < FS_ZONE) || ((k == 1 || k == 3) && row >= Mx - FS_ZONE)) zone = z;
+                }
+                // the balanced segment of n segments of the interior rows holding the row (fused_step.cuh)
+                auto seg_of = [&](int ns) {
+                    int seg = 0;
+                    while (s->ir0 + (int)((long)(seg + 1) * s->int_rows / ns) <= row) seg++;
+                    return seg;
+                };
+                int cta;
+                const int n_bnd = s->n_zone * s->n_bstrip;
+                if (zone >= 0) {
+                    cta = zone * s->n_bstrip + col / FS_BND_TY;
+                } else if (tma && col >= TMA_Y0 && col < s->y_tma_end) {   // a TMA strip CTA
+                    cta = n_bnd + n_int_cta + seg_of(s->n_tseg) * s->n_tstrip + (col - TMA_Y0) / TMA_CORE;
+                } else if (tma) {                                         // a warp strip
+                    const int os = col < TMA_Y0 ? 0 : 1 + (col - s->y_tma_end) / FS_WARP_CORE;
+                    cta = n_bnd + (seg_of(n_int_seg) * s->n_ostrip + os) / FS_WARPS;
+                } else {
+                    cta = n_bnd + (seg_of(n_int_seg) * s->n_wstrip + col / FS_WARP_CORE) / FS_WARPS;
+                }
+                for (int f = 0; f < 2; f++)
+                    if (q[f] >= 0) per[cta].insert(per[cta].end(), {q[f], row, col, 2 * r + f});
             }
-            // the balanced segment of n segments of the interior rows holding the row (fused_step.cuh)
-            auto seg_of = [&](int n) {
-                int seg = 0;
-                while (s->ir0 + (int)((long)(seg + 1) * s->int_rows / n) <= row) seg++;
-                return seg;
-            };
-            int cta;
-            const int n_bnd = s->n_zone * s->n_bstrip;
-            if (zone >= 0) {
-                cta = zone * s->n_bstrip + col / FS_BND_TY;
-            } else if (s->tma && col >= TMA_Y0 && col < s->y_tma_end) {   // a TMA strip CTA
-                cta = n_bnd + s->n_int_cta + seg_of(s->n_tseg) * s->n_tstrip + (col - TMA_Y0) / TMA_CORE;
-            } else if (s->tma) {                                         // a warp strip
-                const int os = col < TMA_Y0 ? 0 : 1 + (col - s->y_tma_end) / FS_WARP_CORE;
-                cta = n_bnd + (seg_of(s->n_int_seg) * s->n_ostrip + os) / FS_WARPS;
-            } else {
-                cta = n_bnd + (seg_of(s->n_int_seg) * s->n_wstrip + col / FS_WARP_CORE) / FS_WARPS;
+            std::vector<int> off(nctas + 1, 0), list;
+            for (int c = 0; c < nctas; c++) {
+                off[c + 1] = off[c] + (int)per[c].size() / 4;
+                list.insert(list.end(), per[c].begin(), per[c].end());
             }
-            for (int f = 0; f < 2; f++)
-                if (q[f] >= 0) per[cta].insert(per[cta].end(), {q[f], row, col, 2 * r + f});
-        }
-        std::vector<int> off(nctas + 1, 0), list;
-        for (int c = 0; c < nctas; c++) {
-            off[c + 1] = off[c] + (int)per[c].size() / 4;
-            list.insert(list.end(), per[c].begin(), per[c].end());
-        }
-        if ((int)list.size() > s->rcv_list_cap) {
-            s->release(s->d_rcv_list);
-            s->d_rcv_list = nullptr;
-            int cap = 64;
-            while (cap < (int)list.size()) cap *= 2;
-            if (s->alloc((void **)&s->d_rcv_list, sizeof(int) * cap) != TW_OK) return TW_ERR_NOMEM;
-            s->rcv_list_cap = cap;
-        }
-        TW_CUDA(cudaMemcpyAsync(s->d_rcv_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, s->st));
-        if (!list.empty())
-            TW_CUDA(cudaMemcpyAsync(s->d_rcv_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, s->st));
+            if ((int)list.size() > *cap_list) {
+                s->release(*d_list);
+                *d_list = nullptr;
+                int cap = 64;
+                while (cap < (int)list.size()) cap *= 2;
+                if (s->alloc((void **)d_list, sizeof(int) * cap) != TW_OK) return TW_ERR_NOMEM;
+                *cap_list = cap;
+            }
+            TW_CUDA(cudaMemcpyAsync(d_off, off.data(), sizeof(int) * off.size(), cudaMemcpyHostToDevice, s->st));
+            if (!list.empty())
+                TW_CUDA(cudaMemcpyAsync(*d_list, list.data(), sizeof(int) * list.size(), cudaMemcpyHostToDevice, s->st));
+            return TW_OK;
+        };
+        int rc = build(false, s->d_rcv_off, &s->d_rcv_list, &s->rcv_list_cap);
+        if (rc == TW_OK && s->tma) rc = build(true, s->d_rcv_off_w, &s->d_rcv_list_w, &s->rcv_list_cap_w);
+        if (rc != TW_OK) return rc;
     }
     if (s->pfuse) {   // (field slot, row, column, trace row) per recorded field, for the fused steps
         std::vector<int> list;
@@ -1038,6 +1061,8 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             int n_sm = 148;
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, d.device);
             s->tma = true;
+            s->w_int_seg = s->n_int_seg;
+            s->w_int_cta = s->n_int_cta;
             s->n_tstrip = nts;
             s->y_tma_end = TMA_Y0 + TMA_CORE * nts;
             // warp strips: the first at column 0, the others from y_tma_end to the seam column My
@@ -1089,6 +1114,11 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
         cudaMemsetAsync(s->d_done, 0, 2 * sizeof(int), s->st);
         if ((rc_ = s->alloc((void **)&s->d_rcv_off, sizeof(int) * (nctas + 1))) != TW_OK) return fail(rc_);
         cudaMemsetAsync(s->d_rcv_off, 0, sizeof(int) * (nctas + 1), s->st);
+        if (s->tma) {
+            const int nw = s->w_int_cta + s->n_zone * s->n_bstrip;
+            if ((rc_ = s->alloc((void **)&s->d_rcv_off_w, sizeof(int) * (nw + 1))) != TW_OK) return fail(rc_);
+            cudaMemsetAsync(s->d_rcv_off_w, 0, sizeof(int) * (nw + 1), s->st);
+        }
     }
     if (!s->elastic && s->periodic && !d.energy) {
         // periodic acoustic with energy off: a second copy of the state, for the fused step of a
