@@ -6,7 +6,8 @@ strip's end at, just below and just above the seam, with one strip or several; r
 many segments. Every field carries random data, receivers sit on both sides of every strip edge,
 on the seam and on segment edges, and the source sits in a strip. Fields, traces and energies are
 compared with the C restatement (bit for bit; energies 1e-12) and with the per-warp kernel
-(TW_TMA=0), which must agree bit for bit too.
+(TW_TMA=0), which must agree bit for bit too. The warp strips run both ways: as the first work
+items of the strips' launch and in the side launch (TW_TMA_WITEMS).
 """
 import os
 
@@ -48,11 +49,13 @@ def _random_state(Mx, My, seed):
     return [(rng.standard_normal(s) * 1e-2).astype(np.float32).astype(np.float64) for s in shapes]
 
 
+@pytest.mark.parametrize("witems", ["1", "0"])
 @pytest.mark.parametrize("energy", [False, True])
 @pytest.mark.parametrize("Mx,My", [(24, 180), (40, 299), (33, 300), (57, 301), (100, 420), (26, 1000), (300, 181)])
-def test_tma_step_matches_restatement_and_warp_kernel(Mx, My, energy):
+def test_tma_step_matches_restatement_and_warp_kernel(Mx, My, energy, witems, monkeypatch):
     case = _case(Mx, My, seed=Mx + 7 * My)
     f0 = _random_state(Mx, My, Mx * My)
+    monkeypatch.setenv("TW_TMA_WITEMS", witems)   # the warp strips in the strips' launch, or the side launch
     want = orc.elastic_run(case, "f32", fields0=f0)
     os.environ["TW_TMA"] = "1"
     try:

@@ -182,6 +182,7 @@ struct FusedArgs {
     // and decode c = qlo + qstep * code by field slot; everything else reads `coef` (decoded FP32)
     int q16;
     float qlo[5], qstep[5];
+    int witems;               // the warp strips run as the first items of the TMA strips' launch
 };
 template <class S, class C>
 void launch_fused(const FusedArgs<S, C> &a, int cpst, bool energy, bool coef16, cudaStream_t st);

@@ -137,6 +137,11 @@ struct tw_solver {
     // side launch there), with its per-CTA receiver lists: steps between buffers other than the
     // handle's two (the adjoint's recomputation and revolve sweeps) run that kernel
     int w_int_seg = 0, w_int_cta = 0;
+    // the warp strips as the first work items of the TMA strips' launch (grids below 2^23 points:
+    // there the side launch's latency-bound warps cost more SM time than they overlap; on larger
+    // grids those items at the head of the queue hold the strips' DRAM stream back), else in the
+    // side launch; TW_TMA_WITEMS=1 / 0 selects either for comparisons
+    bool tma_witems = false;
     int *d_rcv_off_w = nullptr, *d_rcv_list_w = nullptr;
     int rcv_list_cap_w = 0;
     TmaMaps *tmaps = nullptr;
@@ -436,6 +441,7 @@ void enqueue_fused_io(tw_solver *s, void *const *fin, void *const *fout, void *c
             a.y_tma_end = s->y_tma_end;
             a.work = s->d_done + 1;
             a.q16 = s->q16 ? 1 : 0;
+            a.witems = s->tma_witems ? 1 : 0;
             for (int k = 0; k < 5; k++) { a.qlo[k] = s->qlo[k]; a.qstep[k] = s->qstep[k]; }
             launch_tma<S, C>(a, s->tmaps[fin == s->f ? 0 : 1], energy, st, s->st_side, s->ev_fork, s->ev_join);
             return;
@@ -1078,6 +1084,7 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             s->n_int_seg = std::max(1, std::min(max_seg, s->int_rows / side_rows));
             s->n_int_cta = (s->n_int_seg * s->n_ostrip + FS_WARPS - 1) / FS_WARPS;
             s->n_tcta = s->n_tseg * s->n_tstrip;
+            s->tma_witems = env_int("TW_TMA_WITEMS", (long)Mx * My < (1L << 23) ? 1 : 0) != 0;
             e = prepare_tma<float, float>();
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
             if ((e = cudaStreamCreateWithFlags(&s->st_side, cudaStreamNonBlocking)) != cudaSuccess ||

@@ -2,10 +2,12 @@
 // update): one launch per step, every field read once and written once, bit-identical to the
 // per-point kernels (hence to the reference's CPU solver, forward_simulation.cpp:38-113).
 //
-// Three kinds of CTA (4 warps each) make the step, in two launches (see k_elastic_side):
-// * boundary CTAs (the FS_ZONE rows at each free surface): boundary_cta of fused_step.cuh;
-// * warp-strip CTAs: interior_warp of fused_step.cuh over the interior columns that the TMA
-//   strips leave, among them the periodic seam (its reads follow the seam rule column by column);
+// Three kinds of work (4 warps each) make the step, in two launches (see k_elastic_side):
+// * boundary CTAs (the FS_ZONE rows at each free surface): boundary_cta of fused_step.cuh, in
+//   the side launch;
+// * warp-strip items: interior_warp of fused_step.cuh over the interior columns that the TMA
+//   strips leave, among them the periodic seam (its reads follow the seam rule column by column),
+//   the first work items of the TMA strips' persistent CTAs;
 // * TMA strip CTAs: one CTA per (row segment, strip of TMA_CORE = 120 columns). Rows arrive in
 //   blocks of TMA_ROWS = 4 (one per warp): one thread issues, for every array, a 2-D tensor copy
 //   (cp.async.bulk.tensor, 128 columns x 4 rows, no multicast, this GPU's memory only) into a ring
@@ -239,6 +241,7 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
     __syncthreads();
     int issued = -1;   // (lane 0 of each warp) the last group issued
     if (lane == 0) {
+        fence_proxy_async();   // the previous item's accesses to this shared memory come first
         for (int G = 0; G <= 2 && G <= Q; G++) issue(G);
         issued = Q < 2 ? Q : 2;
     }
@@ -550,7 +553,9 @@ __device__ __forceinline__ void step_done(const FusedArgs<float, float> &a, int 
     }
 }
 
-template <bool ENERGY>
+// WITEMS: the warp strips run as items of the strips' launch (this launch holds the boundary CTAs
+// only); a kernel of its own for either case, since code for the other would cost time unused
+template <bool ENERGY, bool WITEMS>
 __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<float, ENERGY>())
     k_elastic_side(FusedArgs<float, float> a)
 {
@@ -561,11 +566,12 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<float, ENERGY>()
     const int rcv_b = a.rcv_off[cta], rcv_e = a.rcv_off[cta + 1];
     EAcc E;
     const int n_bnd = a.n_zone * a.n_bstrip;
-    if (cta < n_bnd) {
+    if (WITEMS || cta < n_bnd) {
         boundary_cta<float, float, 0, ENERGY, float, false>(a, cta % a.n_bstrip, cta / a.n_bstrip, it, rcv_b, rcv_e,
                                                            reinterpret_cast<float *>(side_smem_raw), E);
-    } else {
-        // warp strips: segments of the interior rows (a.n_int_seg of them) x a.n_ostrip strips
+    } else if constexpr (!WITEMS) {
+        // warp strips (when they are not items of the TMA strips' launch): segments of the
+        // interior rows (a.n_int_seg of them) x a.n_ostrip strips
         const int gw = (cta - n_bnd) * FS_WARPS + (threadIdx.x >> 5);
         if (gw < a.n_int_seg * a.n_ostrip) {
             const int seg = gw / a.n_ostrip, os = gw - seg * a.n_ostrip;
@@ -579,7 +585,7 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<float, ENERGY>()
     step_done(a, it);
 }
 
-template <bool ENERGY, bool Q16 = false>
+template <bool ENERGY, bool Q16 = false, bool WITEMS = false>
 __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
     k_elastic_tma(FusedArgs<float, float> a, const __grid_constant__ TmaMaps maps)
 {
@@ -589,16 +595,39 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
     const int n_side = a.n_zone * a.n_bstrip + a.n_octa;   // receiver lists: the side CTAs' come first
     int *item_s = reinterpret_cast<int *>(base + TmaLayout<ENERGY, Q16>::o_item);
     EAcc E;
-    // a persistent grid: each CTA takes (segment, strip) items until none is left, so CTAs that
-    // find their SM busy with side CTAs at first simply take fewer items
+    // a persistent grid: each CTA takes items until none is left, so CTAs that find their SM busy
+    // with side CTAs at first simply take fewer. With WITEMS the first W = n_octa items are
+    // groups of 4 warp strips (latency-bound: taken first, so that none trails at the end; spread
+    // among the TMA items instead, the two loops on one SM were far slower), the rest (segment,
+    // strip) items of the TMA strips; without, the side launch runs the warp strips
+    static_assert(FS_WARPS * RingLayout<float, float, 0, ENERGY, float>::warp <= TmaLayout<ENERGY, Q16>::o_bar,
+                  "the warp strips' rings lie below the TMA strips' barriers");
+    const int n_bnd = a.n_zone * a.n_bstrip;
     for (;;) {
         if (threadIdx.x == 0) *item_s = atomicAdd(a.work, 1);
         __syncthreads();
         const int t = *item_s;
         __syncthreads();
-        if (t >= a.n_tcta) break;
-        const int rcv_b = a.rcv_off[n_side + t], rcv_e = a.rcv_off[n_side + t + 1];
-        if (!tma_strip_cta<ENERGY, Q16>(a, maps, t % a.n_tstrip, t / a.n_tstrip, it, rcv_b, rcv_e, E, base)) break;
+        const int W = WITEMS ? a.n_octa : 0;
+        if (t >= W + a.n_tcta) break;
+        if constexpr (WITEMS) {
+          if (t < W) {   // warp strips: segments of the interior rows x a.n_ostrip strips
+            const int rcv_b = a.rcv_off[n_bnd + t], rcv_e = a.rcv_off[n_bnd + t + 1];
+            const int gw = t * FS_WARPS + (threadIdx.x >> 5);
+            if (gw < a.n_int_seg * a.n_ostrip) {
+                const int seg = gw / a.n_ostrip, os = gw - seg * a.n_ostrip;
+                const int y0 = os == 0 ? 0 : a.y_tma_end + (os - 1) * FS_WARP_CORE;
+                unsigned char *ring = base + (threadIdx.x >> 5) * RingLayout<float, float, 0, ENERGY, float>::warp;
+                if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<float, float, 0, ENERGY, false, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
+                else interior_warp<float, float, 0, ENERGY, true, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
+            }
+            __syncthreads();   // every warp is done with its ring before the shared memory is reused
+            continue;
+          }
+        }
+        const int tt = t - W;
+        const int rcv_b = a.rcv_off[n_side + tt], rcv_e = a.rcv_off[n_side + tt + 1];
+        if (!tma_strip_cta<ENERGY, Q16>(a, maps, tt % a.n_tstrip, tt / a.n_tstrip, it, rcv_b, rcv_e, E, base)) break;
     }
     cta_energy<ENERGY>(a, E, reinterpret_cast<double *>(base + TmaLayout<ENERGY, Q16>::o_red), it);
     step_done(a, it);
