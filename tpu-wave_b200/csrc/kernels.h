@@ -194,6 +194,7 @@ constexpr int TMA_Y0 = FS_WARP_CORE; // the first TMA strip starts after the fir
 constexpr int TMA_W = 128;           // columns a TMA strip loads: 4 halo on each side
 constexpr int TMA_ROWS = 4;          // rows per TMA block: one per warp
 constexpr int TMA_NMAP = 15;         // tensor maps: 5 fields, 5 coefficients, 5 energy weights
+constexpr int TMA_TILE_ROWS = 12;    // the boundary CTAs' tile rows on a TMA handle (free-surface x ends)
 struct TmaMaps {
     alignas(64) unsigned char m[TMA_NMAP][128];   // CUtensorMap objects (opaque, 128 bytes each)
 };

@@ -137,10 +137,11 @@ struct tw_solver {
     // side launch there), with its per-CTA receiver lists: steps between buffers other than the
     // handle's two (the adjoint's recomputation and revolve sweeps) run that kernel
     int w_int_seg = 0, w_int_cta = 0;
-    // the warp strips as the first work items of the TMA strips' launch (grids below 2^23 points:
-    // there the side launch's latency-bound warps cost more SM time than they overlap; on larger
-    // grids those items at the head of the queue hold the strips' DRAM stream back), else in the
-    // side launch; TW_TMA_WITEMS=1 / 0 selects either for comparisons
+    // the boundary CTAs and the warp strips as the first work items of the TMA strips' launch, one
+    // launch a step (grids below 2^23 points: there the side launch's latency-bound CTAs cost more
+    // SM time than they overlap; on larger grids those items at the head of the queue hold the
+    // strips' DRAM stream back), else in the side launch; TW_TMA_WITEMS=1 / 0 selects either for
+    // comparisons
     bool tma_witems = false;
     int *d_rcv_off_w = nullptr, *d_rcv_list_w = nullptr;
     int rcv_list_cap_w = 0;
@@ -1085,6 +1086,7 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             s->n_int_cta = (s->n_int_seg * s->n_ostrip + FS_WARPS - 1) / FS_WARPS;
             s->n_tcta = s->n_tseg * s->n_tstrip;
             s->tma_witems = env_int("TW_TMA_WITEMS", (long)Mx * My < (1L << 23) ? 1 : 0) != 0;
+            if (s->tile_rows != TMA_TILE_ROWS) return fail(TW_ERR_INVALID);   // (the strips' launch holds this tile)
             e = prepare_tma<float, float>();
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
             if ((e = cudaStreamCreateWithFlags(&s->st_side, cudaStreamNonBlocking)) != cudaSuccess ||
@@ -1796,7 +1798,7 @@ int tw_get_info(tw_solver *s, tw_info *info)
     info->own_rows[1] = s->own1;
     info->Mx_glob = s->Mx_glob;
     info->step_kind = s->tma ? 2 : (s->fused ? 1 : (s->afused ? 3 : 0));
-    info->launches_per_step = s->tma ? 2 : ((s->fused || s->afused) ? 1 : 3);
+    info->launches_per_step = s->tma ? (s->tma_witems ? 1 : 2) : ((s->fused || s->afused) ? 1 : 3);
     if (s->fused && (s->bnd & BND_Y_SAT)) info->launches_per_step += 2;   // the y-end recomputation
     return TW_OK;
 }

@@ -33,10 +33,10 @@ static cudaError_t tma_attr()
                                 (int)tma_smem<ENERGY, Q16>());
 }
 
-template <bool ENERGY, bool WITEMS>
+template <bool ENERGY>
 static cudaError_t side_attr()
 {
-    return cudaFuncSetAttribute(k_elastic_side<ENERGY, WITEMS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    return cudaFuncSetAttribute(k_elastic_side<ENERGY>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)side_smem<ENERGY>(FS_SMALL_MX + 1));
 }
 
@@ -49,10 +49,8 @@ cudaError_t prepare_tma<float, float>()
         (e = tma_attr<false, false, true>()) != cudaSuccess || (e = tma_attr<true, false, true>()) != cudaSuccess ||
         (e = tma_attr<false, true, true>()) != cudaSuccess || (e = tma_attr<true, true, true>()) != cudaSuccess)
         return e;
-    if ((e = side_attr<false, false>()) != cudaSuccess || (e = side_attr<true, false>()) != cudaSuccess ||
-        (e = side_attr<false, true>()) != cudaSuccess)
-        return e;
-    return side_attr<true, true>();
+    if ((e = side_attr<false>()) != cudaSuccess) return e;
+    return side_attr<true>();
 }
 
 // the TMA strips of one variant: a persistent grid of as many CTAs as fit on the device at once
@@ -67,25 +65,16 @@ static void launch_strips(FusedArgs<float, float> &a, const TmaMaps &maps, int n
                                                       tma_smem<ENERGY, Q16>());
         cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, dev);
     }
-    const int n_strips = std::min((WITEMS ? a.n_octa : 0) + a.n_tcta, std::max(1, resident) * n_sm);
+    const int n_items = (WITEMS ? a.n_zone * a.n_bstrip + a.n_octa : 0) + a.n_tcta;
+    const int n_strips = std::min(n_items, std::max(1, resident) * n_sm);
     a.n_all_ctas = n_side + n_strips;
     if (go) k_elastic_tma<ENERGY, Q16, WITEMS><<<n_strips, FS_THREADS_MAX, tma_smem<ENERGY, Q16>(), st>>>(a, maps);
 }
 
-template <bool ENERGY, bool WITEMS>
-static void launch_side(const FusedArgs<float, float> &a, int n_side, cudaStream_t side_st)
-{
-    k_elastic_side<ENERGY, WITEMS><<<n_side, FS_THREADS_MAX, side_smem<ENERGY>(a.tile_rows), side_st>>>(a);
-}
-
 template <bool WITEMS>
-static void launch_pair(FusedArgs<float, float> &a, const TmaMaps &maps, bool energy, int n_side, cudaStream_t st,
-                        cudaStream_t side_st, bool go)
+static void launch_strips_of(FusedArgs<float, float> &a, const TmaMaps &maps, bool energy, int n_side, cudaStream_t st,
+                             bool go)
 {
-    if (go) {
-        if (energy) launch_side<true, WITEMS>(a, n_side, side_st);
-        else launch_side<false, WITEMS>(a, n_side, side_st);
-    }
     switch ((energy ? 1 : 0) + (a.q16 ? 2 : 0)) {
     case 0: launch_strips<false, false, WITEMS>(a, maps, n_side, st, go); break;
     case 1: launch_strips<true, false, WITEMS>(a, maps, n_side, st, go); break;
@@ -94,24 +83,24 @@ static void launch_pair(FusedArgs<float, float> &a, const TmaMaps &maps, bool en
     }
 }
 
-// the side launch on a second stream forked from the handle's stream, the TMA strips on the
-// handle's stream, joined back (in a captured graph: two parallel branches)
+// the TMA strips on the handle's stream; the side launch, when there is one, on a second stream
+// forked from it and joined back (in a captured graph: two parallel branches)
 template <>
 void launch_tma<float, float>(FusedArgs<float, float> a, const TmaMaps &maps, bool energy, cudaStream_t st,
                               cudaStream_t side_st, cudaEvent_t fork, cudaEvent_t join)
 {
-    // the boundary CTAs, and the warp strips unless they are items of the strips' launch
-    const int n_side = a.n_zone * a.n_bstrip + (a.witems ? 0 : a.n_octa);
-    // first the strips' grid size (it sets the CTA count the last CTA waits for), then the launches
-    for (int pass = 0; pass < 2; pass++) {
-        const bool go = pass == 1;
-        if (go) {
-            cudaEventRecord(fork, st);
-            cudaStreamWaitEvent(side_st, fork, 0);
-        }
-        if (a.witems) launch_pair<true>(a, maps, energy, n_side, st, side_st, go);
-        else launch_pair<false>(a, maps, energy, n_side, st, side_st, go);
+    if (a.witems) {   // one launch: boundary, warp-strip and TMA items
+        launch_strips_of<true>(a, maps, energy, 0, st, false);   // (sets the CTA count the last CTA waits for)
+        launch_strips_of<true>(a, maps, energy, 0, st, true);
+        return;
     }
+    const int n_side = a.n_zone * a.n_bstrip + a.n_octa;   // the boundary CTAs and the warp strips
+    launch_strips_of<false>(a, maps, energy, n_side, st, false);
+    cudaEventRecord(fork, st);
+    cudaStreamWaitEvent(side_st, fork, 0);
+    if (energy) k_elastic_side<true><<<n_side, FS_THREADS_MAX, side_smem<true>(a.tile_rows), side_st>>>(a);
+    else k_elastic_side<false><<<n_side, FS_THREADS_MAX, side_smem<false>(a.tile_rows), side_st>>>(a);
+    launch_strips_of<false>(a, maps, energy, n_side, st, true);
     cudaEventRecord(join, side_st);
     cudaStreamWaitEvent(st, join, 0);
 }

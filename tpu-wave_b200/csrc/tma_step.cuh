@@ -553,9 +553,7 @@ __device__ __forceinline__ void step_done(const FusedArgs<float, float> &a, int 
     }
 }
 
-// WITEMS: the warp strips run as items of the strips' launch (this launch holds the boundary CTAs
-// only); a kernel of its own for either case, since code for the other would cost time unused
-template <bool ENERGY, bool WITEMS>
+template <bool ENERGY>
 __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<float, ENERGY>())
     k_elastic_side(FusedArgs<float, float> a)
 {
@@ -566,12 +564,11 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<float, ENERGY>()
     const int rcv_b = a.rcv_off[cta], rcv_e = a.rcv_off[cta + 1];
     EAcc E;
     const int n_bnd = a.n_zone * a.n_bstrip;
-    if (WITEMS || cta < n_bnd) {
+    if (cta < n_bnd) {
         boundary_cta<float, float, 0, ENERGY, float, false>(a, cta % a.n_bstrip, cta / a.n_bstrip, it, rcv_b, rcv_e,
                                                            reinterpret_cast<float *>(side_smem_raw), E);
-    } else if constexpr (!WITEMS) {
-        // warp strips (when they are not items of the TMA strips' launch): segments of the
-        // interior rows (a.n_int_seg of them) x a.n_ostrip strips
+    } else {
+        // warp strips: segments of the interior rows (a.n_int_seg of them) x a.n_ostrip strips
         const int gw = (cta - n_bnd) * FS_WARPS + (threadIdx.x >> 5);
         if (gw < a.n_int_seg * a.n_ostrip) {
             const int seg = gw / a.n_ostrip, os = gw - seg * a.n_ostrip;
@@ -596,24 +593,34 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
     int *item_s = reinterpret_cast<int *>(base + TmaLayout<ENERGY, Q16>::o_item);
     EAcc E;
     // a persistent grid: each CTA takes items until none is left, so CTAs that find their SM busy
-    // with side CTAs at first simply take fewer. With WITEMS the first W = n_octa items are
-    // groups of 4 warp strips (latency-bound: taken first, so that none trails at the end; spread
-    // among the TMA items instead, the two loops on one SM were far slower), the rest (segment,
-    // strip) items of the TMA strips; without, the side launch runs the warp strips
+    // with side CTAs at first simply take fewer. With WITEMS the whole step is this launch: the
+    // first n_bnd items are the boundary CTAs' work, the next n_octa groups of 4 warp strips
+    // (both latency-bound: taken first, so that none trails at the end; spread among the TMA
+    // items instead, two loops on one SM were far slower), the rest (segment, strip) items of the
+    // TMA strips; without, the side launch runs the boundary CTAs and the warp strips
     static_assert(FS_WARPS * RingLayout<float, float, 0, ENERGY, float>::warp <= TmaLayout<ENERGY, Q16>::o_bar,
                   "the warp strips' rings lie below the TMA strips' barriers");
+    static_assert(sizeof(float) * 2 * TMA_TILE_ROWS * FS_BND_W <= (size_t)TmaLayout<ENERGY, Q16>::o_bar,
+                  "the boundary CTAs' tile lies below the TMA strips' barriers");
     const int n_bnd = a.n_zone * a.n_bstrip;
     for (;;) {
         if (threadIdx.x == 0) *item_s = atomicAdd(a.work, 1);
         __syncthreads();
         const int t = *item_s;
         __syncthreads();
-        const int W = WITEMS ? a.n_octa : 0;
-        if (t >= W + a.n_tcta) break;
+        const int B = WITEMS ? n_bnd : 0, W = WITEMS ? a.n_octa : 0;
+        if (t >= B + W + a.n_tcta) break;
         if constexpr (WITEMS) {
-          if (t < W) {   // warp strips: segments of the interior rows x a.n_ostrip strips
-            const int rcv_b = a.rcv_off[n_bnd + t], rcv_e = a.rcv_off[n_bnd + t + 1];
-            const int gw = t * FS_WARPS + (threadIdx.x >> 5);
+          if (t < B) {   // a boundary CTA's zone rows (its velocities through a shared tile)
+            boundary_cta<float, float, 0, ENERGY, float, false>(a, t % a.n_bstrip, t / a.n_bstrip, it, a.rcv_off[t],
+                                                               a.rcv_off[t + 1], reinterpret_cast<float *>(base), E);
+            __syncthreads();   // the tile is free before the shared memory is reused
+            continue;
+          }
+          if (t < B + W) {   // warp strips: segments of the interior rows x a.n_ostrip strips
+            const int w = t - B;
+            const int rcv_b = a.rcv_off[n_bnd + w], rcv_e = a.rcv_off[n_bnd + w + 1];
+            const int gw = w * FS_WARPS + (threadIdx.x >> 5);
             if (gw < a.n_int_seg * a.n_ostrip) {
                 const int seg = gw / a.n_ostrip, os = gw - seg * a.n_ostrip;
                 const int y0 = os == 0 ? 0 : a.y_tma_end + (os - 1) * FS_WARP_CORE;
@@ -625,7 +632,7 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
             continue;
           }
         }
-        const int tt = t - W;
+        const int tt = t - B - W;
         const int rcv_b = a.rcv_off[n_side + tt], rcv_e = a.rcv_off[n_side + tt + 1];
         if (!tma_strip_cta<ENERGY, Q16>(a, maps, tt % a.n_tstrip, tt / a.n_tstrip, it, rcv_b, rcv_e, E, base)) break;
     }
