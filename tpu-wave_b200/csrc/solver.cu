@@ -138,10 +138,11 @@ struct tw_solver {
     // handle's two (the adjoint's recomputation and revolve sweeps) run that kernel
     int w_int_seg = 0, w_int_cta = 0;
     // the boundary CTAs and the warp strips as the first work items of the TMA strips' launch, one
-    // launch a step (grids below 2^23 points: there the side launch's latency-bound CTAs cost more
-    // SM time than they overlap; on larger grids those items at the head of the queue hold the
-    // strips' DRAM stream back), else in the side launch; TW_TMA_WITEMS=1 / 0 selects either for
-    // comparisons
+    // launch a step (grids below 2^25 points: there the side launch's latency-bound CTAs cost more
+    // SM time than they overlap; B200, us a step one launch / two: 1024^2 31.3 / 34.6, 3072^2
+    // 112.1 / 127.5, 4096^2 194.1 / 199.1, 6144^2 399.8 / 400.1, 8192^2 691.2 / 688.9, where the
+    // latency-bound items at the head of the queue hold the strips' DRAM stream back), else in the
+    // side launch; TW_TMA_WITEMS=1 / 0 selects either for comparisons
     bool tma_witems = false;
     int *d_rcv_off_w = nullptr, *d_rcv_list_w = nullptr;
     int rcv_list_cap_w = 0;
@@ -1085,7 +1086,7 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             s->n_int_seg = std::max(1, std::min(max_seg, s->int_rows / side_rows));
             s->n_int_cta = (s->n_int_seg * s->n_ostrip + FS_WARPS - 1) / FS_WARPS;
             s->n_tcta = s->n_tseg * s->n_tstrip;
-            s->tma_witems = env_int("TW_TMA_WITEMS", (long)Mx * My < (1L << 23) ? 1 : 0) != 0;
+            s->tma_witems = env_int("TW_TMA_WITEMS", (long)Mx * My < (1L << 25) ? 1 : 0) != 0;
             if (s->tile_rows != TMA_TILE_ROWS) return fail(TW_ERR_INVALID);   // (the strips' launch holds this tile)
             e = prepare_tma<float, float>();
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
