@@ -470,11 +470,13 @@ def run_ours(args, dist: Dist):
     info = s.info()
     prof = s.profile(P)
     if info.step_kind == 2:
-        # TMA-staged step: two launches side by side (the TMA strips and the boundary / seam
-        # CTAs), timed together; compulsory bytes = 5 fields read and written once + 5
-        # coefficients read once = 60 B per cell in FP32
-        name, alg, ms_k = "k_elastic_tma + k_elastic_side (one step)", MX * MY * 60, float(prof[0])
-        launches_per_step = 2
+        # TMA-staged step: one launch (boundary, warp-strip and TMA items of the persistent
+        # strips' grid) or two side by side (the strips and the boundary / seam CTAs), timed
+        # together; compulsory bytes = 5 fields read and written once + 5 coefficients read once
+        # = 60 B per cell in FP32
+        launches_per_step = int(info.launches_per_step)
+        name = "k_elastic_tma (one launch a step)" if launches_per_step == 1 else "k_elastic_tma + k_elastic_side (one step)"
+        alg, ms_k = MX * MY * 60, float(prof[0])
     elif prof[1] == 0.0:
         # fused path: the whole step is one launch
         name, alg, ms_k = "k_elastic_fused", MX * MY * 60, float(prof[0])
@@ -487,7 +489,7 @@ def run_ours(args, dist: Dist):
         launches_per_step = 3
     achieved = alg / (ms_k / 1e3) / 1e9
     peak, peak_note = measured_peaks()
-    tkey = "tma_step@2048" if info.step_kind == 2 else name
+    tkey = name if info.step_kind != 2 else ("tma_step1@2048" if launches_per_step == 1 else "tma_step@2048")
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": ncu_traffic(tkey), "kernel": name, "peak_source": peak_note,
                 "algorithmic_bytes_per_launch": alg, "ms_per_launch": ms_k,
@@ -617,19 +619,20 @@ def run_target_8192(args, tw, torch, clocks, dev: int):
     th1 = time.monotonic()
     ms = e0.elapsed_time(e1)
     tma = s.info().step_kind == 2
+    one = int(s.info().launches_per_step) == 1
     prof = s.profile(8)
     s.close()
     peak, peak_note = measured_peaks()
     alg = n * n * 60
     ms_k = float(prof[0])
-    kname = "k_elastic_tma + k_elastic_side (one step)" if tma else "k_elastic_fused"
+    kname = ("k_elastic_tma (one launch a step)" if one else "k_elastic_tma + k_elastic_side (one step)") if tma else "k_elastic_fused"
     return {"workload": f"elastic {n}x{n} FP32, the same 8-layer medium, energy off, 16 receivers",
             "steps": T, "warmup": W, "ms_per_step": ms / T, "gpts": n * n * T / (ms / 1e3) / 1e9,
             "roofline": {"kernel": kname, "algorithmic_bytes_per_launch": alg, "ms_per_launch": ms_k,
                          "achieved": alg / (ms_k / 1e3) / 1e9, "peak": peak, "peak_source": peak_note,
                          "frac": alg / (ms_k / 1e3) / 1e9 / peak,
                          "frac_of_step_time": alg / (ms / T / 1e3) / 1e9 / peak,
-                         "traffic": ncu_traffic("tma_step@8192" if tma else "k_elastic_fused@8192")},
+                         "traffic": ncu_traffic(("tma_step1@8192" if one else "tma_step@8192") if tma else "k_elastic_fused@8192")},
             "clocks": clocks.window(th0, th1), "l2": "inputs far larger than L2 (4 GB a step), no flush"}
 
 
