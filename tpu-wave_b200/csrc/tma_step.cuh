@@ -625,8 +625,9 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
                 const int seg = gw / a.n_ostrip, os = gw - seg * a.n_ostrip;
                 const int y0 = os == 0 ? 0 : a.y_tma_end + (os - 1) * FS_WARP_CORE;
                 unsigned char *ring = base + (threadIdx.x >> 5) * RingLayout<float, float, 0, ENERGY, float>::warp;
-                if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<float, float, 0, ENERGY, false, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
-                else interior_warp<float, float, 0, ENERGY, true, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
+                // (the seam-aware variant for every strip: a second, faster variant for the strips
+                // away from the seam made the launch's code larger and the step 4 % slower)
+                interior_warp<float, float, 0, ENERGY, true, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
             }
             __syncthreads();   // every warp is done with its ring before the shared memory is reused
             continue;
