@@ -1075,8 +1075,12 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             s->y_tma_end = TMA_Y0 + TMA_CORE * nts;
             // warp strips: the first at column 0, the others from y_tma_end to the seam column My
             s->n_ostrip = 1 + (int)((My + 1 - s->y_tma_end + FS_WARP_CORE - 1) / FS_WARP_CORE);
-            // work items of about TW_TMA_SEG_ROWS rows (default 32) for the persistent TMA CTAs
-            const int seg_rows = std::max(8, env_int("TW_TMA_SEG_ROWS", 32));
+            // the boundary and warp-strip work in the strips' launch (one launch a step) or beside it
+            s->tma_witems = env_int("TW_TMA_WITEMS", (long)Mx * My < (1L << 25) ? 1 : 0) != 0;
+            // work items of about TW_TMA_SEG_ROWS rows for the persistent TMA CTAs (default 24 for
+            // one launch a step, 32 beside a side launch: at 2048^2 / 4096^2, 24 rows gave 63.1 /
+            // 183.9 us a step against 63.4 / 186.9 for 32 and 65.3 / 187.4 for 48)
+            const int seg_rows = std::max(8, env_int("TW_TMA_SEG_ROWS", s->tma_witems ? 24 : 32));
             const int max_seg = std::max(1, s->int_rows / 8);
             s->n_tseg = std::max(1, std::min(max_seg, (s->int_rows + seg_rows / 2) / seg_rows));
             (void)n_sm;
@@ -1086,7 +1090,6 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             s->n_int_seg = std::max(1, std::min(max_seg, s->int_rows / side_rows));
             s->n_int_cta = (s->n_int_seg * s->n_ostrip + FS_WARPS - 1) / FS_WARPS;
             s->n_tcta = s->n_tseg * s->n_tstrip;
-            s->tma_witems = env_int("TW_TMA_WITEMS", (long)Mx * My < (1L << 25) ? 1 : 0) != 0;
             if (s->tile_rows != TMA_TILE_ROWS) return fail(TW_ERR_INVALID);   // (the strips' launch holds this tile)
             e = prepare_tma<float, float>();
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
