@@ -574,8 +574,8 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<float, ENERGY>()
             const int seg = gw / a.n_ostrip, os = gw - seg * a.n_ostrip;
             const int y0 = os == 0 ? 0 : a.y_tma_end + (os - 1) * FS_WARP_CORE;
             unsigned char *ring = side_smem_raw + (threadIdx.x >> 5) * RingLayout<float, float, 0, ENERGY, float>::warp;
-            if (y0 >= 4 && y0 + 60 <= a.My) interior_warp<float, float, 0, ENERGY, false, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
-            else interior_warp<float, float, 0, ENERGY, true, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
+            // (the seam-aware variant for every strip, as in the strips' launch: 1 % faster at 8192^2)
+            interior_warp<float, float, 0, ENERGY, true, float, false>(a, y0, seg, it, rcv_b, rcv_e, E, ring);
         }
     }
     cta_energy<ENERGY>(a, E, red, it);
