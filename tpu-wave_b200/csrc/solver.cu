@@ -1057,15 +1057,17 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
         }
         // the TMA-staged step (tma_step.cuh): FP32 fields and coefficients, plain update, the
         // reference's x ends, a handle of its own (not a linked slab), at least one TMA strip.
-        // With the energy every step its 40 bytes of FP64 weights per point halve the resident CTAs
-        // and it is slower than the per-warp kernel (117 against 108 us at 2048^2), so by default it
-        // steps handles with the energy off; TW_TMA=1 / 0 in the environment selects it / the
-        // per-warp kernel for every handle (for comparisons);
-        // its work items and side segments have TW_TMA_SEG_ROWS / TW_TMA_SIDE_ROWS rows (below).
+        // With the energy every step it stages 40 bytes of FP64 weights per point and fits 3 CTAs
+        // per SM: faster than the per-warp kernel on grids below 2^25 points (98.4 against 107.5
+        // us at 2048^2, 322.7 against 353.3 at 4096^2), slower above (1181 against 1161 at
+        // 8192^2), so energy-on handles take it below that size. TW_TMA=1 / 0 in the environment
+        // selects it / the per-warp kernel for every handle (for comparisons); its work items and
+        // side segments have TW_TMA_SEG_ROWS / TW_TMA_SIDE_ROWS rows (below).
         const int nts = tma_strips(My);
         s->q16 = d.coef_fp16 == 2;
         if (d.precision == TW_FP32 && d.cpst == TW_CPST_00 && d.coef_fp16 != 1 && !s->slab && !(s->bnd & BND_X_IF) &&
-            s->n_int_seg > 0 && nts > 0 && (s->q16 || env_int("TW_TMA", d.energy ? 0 : 1) != 0)) {
+            s->n_int_seg > 0 && nts > 0 &&
+            (s->q16 || env_int("TW_TMA", (!d.energy || (long)Mx * My < (1L << 25)) ? 1 : 0) != 0)) {
             int n_sm = 148;
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, d.device);
             s->tma = true;

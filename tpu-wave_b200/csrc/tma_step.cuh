@@ -99,21 +99,24 @@ struct TmaLayout {
     static constexpr int CROW = Q16 ? TMA_QW * 2 : ROW;                       // one coefficient row
     static constexpr int CBOX = TMA_ROWS * CROW;                              // bytes a coefficient copy lands
     static constexpr int CBLK = (CBOX + 127) / 128 * 128;                     // one coefficient block
-    static constexpr int WBLK = TMA_ROWS * TMA_W * 8;  // one block of FP64 energy weights
+    static constexpr int WROW = TMA_ROWS * TMA_W * 8;  // one block of one FP64 energy-weight array
     static constexpr int PAD = 128;                    // lanes 0 / 31 read up to 8 bytes beyond a row
     static constexpr int o_nn = PAD, o_mm0 = o_nn + R3 * BLK, o_mm1 = o_mm0 + R3 * BLK;
     static constexpr int o_mn = o_mm1 + R3 * BLK, o_nm = o_mn + R2 * BLK, o_pmn = o_nm + R2 * BLK,
                          o_pnm = o_pmn + R2 * CBLK, o_mu = o_pnm + R2 * CBLK, o_lam = o_mu + R2 * CBLK,
                          o_m2 = o_lam + R2 * CBLK;
     static constexpr int o_vmn = o_m2 + R2 * CBLK, o_vnm = o_vmn + 2 * BLK;  // new velocities (2 blocks)
-    static constexpr int o_w = o_vnm + 2 * BLK;                               // 5 weight rings
+    // the energy weights, one slot per block and set: the velocity rows' (MN, NM) at o_vw, the
+    // stress rows' (NN, MM P1, P2) at o_sw, each loaded half a step before its use (see below)
+    static constexpr int o_w = o_vnm + 2 * BLK, o_vw = o_w, o_sw = o_w + 2 * WROW;
     // NB mbarriers at o_bar, the item index at o_item, the energy reduction's 3 x FS_WARPS doubles
     // at o_red
-    static constexpr int o_bar = o_w + (ENERGY ? 5 * R2 * WBLK : 0) + PAD;
+    static constexpr int o_bar = o_w + (ENERGY ? 5 * WROW : 0) + PAD;
+    static constexpr int NBW = NB + (ENERGY ? 2 : 0);   // barriers: the groups', then the two weight sets'
     static constexpr int o_item = o_bar + 64, o_red = o_bar + 72;
     static constexpr int bytes = o_red + 8 * 3 * FS_WARPS + 128;              // + alignment slack
     static constexpr unsigned tx0 = 3 * BLK;                                // group 0
-    static constexpr unsigned tx = 5 * BLK + 5 * CBOX + (ENERGY ? 5 * WBLK : 0);   // groups >= 1
+    static constexpr unsigned tx = 5 * BLK + 5 * CBOX;                      // groups >= 1
 };
 
 __device__ __forceinline__ float4 lds4(const float *p) { return *reinterpret_cast<const float4 *>(p); }
@@ -207,35 +210,51 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
             if (G == 0) break;
             tma_load_2d(base + L::o_pmn + s2 * L::CBLK, map(TM_PMN), xc, rv, b);
             tma_load_2d(base + L::o_pnm + s2 * L::CBLK, map(TM_PNM), xc, rv, b);
-            if constexpr (ENERGY) tma_load_2d(base + L::o_w + (3 * R2 + s2) * L::WBLK, map(TM_WM3), xs, rt, b);
             break;
         case 1:
             tma_load_2d(base + L::o_mm0 + s3 * L::BLK, map(TM_MM0), xs, rs, b);
             if (G == 0) break;
             tma_load_2d(base + L::o_mu + s2 * L::CBLK, map(TM_MU), xc, rt, b);
             tma_load_2d(base + L::o_lam + s2 * L::CBLK, map(TM_LAM), xc, rt, b);
-            if constexpr (ENERGY) tma_load_2d(base + L::o_w + (4 * R2 + s2) * L::WBLK, map(TM_WM4), xs, rt, b);
             break;
         case 2:
             tma_load_2d(base + L::o_mm1 + s3 * L::BLK, map(TM_MM1), xs, rs, b);
             if (G == 0) break;
             tma_load_2d(base + L::o_m2 + s2 * L::CBLK, map(TM_M2), xc, rt, b);
-            if constexpr (ENERGY) {
-                tma_load_2d(base + L::o_w + (0 * R2 + s2) * L::WBLK, map(TM_WMN), xs, rv, b);
-                tma_load_2d(base + L::o_w + (2 * R2 + s2) * L::WBLK, map(TM_WNN), xs, rt, b);
-            }
             break;
         default:
             if (G == 0) break;
             tma_load_2d(base + L::o_mn + s2 * L::BLK, map(TM_MN), xs, rv, b);
             tma_load_2d(base + L::o_nm + s2 * L::BLK, map(TM_NM), xs, rv, b);
-            if constexpr (ENERGY) tma_load_2d(base + L::o_w + (1 * R2 + s2) * L::WBLK, map(TM_WNM), xs, rv, b);
             break;
         }
     };
 
+    // the energy weights of block qq (thread 0): the velocity rows' set is needed in step qq's
+    // first half and loaded during step qq - 1's second half, the stress rows' set is needed in
+    // step qq's second half and loaded during its first half; one slot each suffices, and the
+    // CTA keeps the shared memory of 3 CTAs per SM (a ring of two blocks per array allowed 2)
+    int vw_last = -1, sw_last = -1;   // (thread 0) the last block of each set issued
+    auto issue_vw = [&](int qq) {
+        unsigned long long *b = bar + NB;
+        mbar_expect_tx(b, 2 * L::WROW);
+        const int rv = x0 - 2 + 4 * qq;
+        tma_load_2d(base + L::o_vw, map(TM_WMN), xs, rv, b);
+        tma_load_2d(base + L::o_vw + L::WROW, map(TM_WNM), xs, rv, b);
+        vw_last = qq;
+    };
+    auto issue_sw = [&](int qq) {
+        unsigned long long *b = bar + NB + 1;
+        mbar_expect_tx(b, 3 * L::WROW);
+        const int rt = x0 - 4 + 4 * qq;
+        tma_load_2d(base + L::o_sw, map(TM_WNN), xs, rt, b);
+        tma_load_2d(base + L::o_sw + L::WROW, map(TM_WM3), xs, rt, b);
+        tma_load_2d(base + L::o_sw + 2 * L::WROW, map(TM_WM4), xs, rt, b);
+        sw_last = qq;
+    };
+
     if (threadIdx.x == 0) {
-        for (int k = 0; k < NB; k++) mbar_init(bar + k, 1);
+        for (int k = 0; k < L::NBW; k++) mbar_init(bar + k, 1);
         mbar_init_fence();
     }
     __syncthreads();
@@ -244,6 +263,11 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
         fence_proxy_async();   // the previous item's accesses to this shared memory come first
         for (int G = 0; G <= 2 && G <= Q; G++) issue(G);
         issued = Q < 2 ? Q : 2;
+        if constexpr (ENERGY)
+            if (warp == 0) {
+                issue_vw(0);
+                issue_sw(0);
+            }
     }
     int waited = -1;   // the last group this thread has seen complete
     float nf = 0.f;    // stays 0 unless a stored value is not finite (v * 0 is NaN for Inf / NaN)
@@ -263,7 +287,8 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
             return lds4(rowp(off, row) + cl);
         }
     };
-    auto wrowp = [&](int k, int slot) { return reinterpret_cast<const double *>(base + L::o_w + k * R2 * L::WBLK) + slot * TMA_W; };
+    // this thread's weights in the set at `off` (array k of it), row `warp` of the block
+    auto wrow = [&](int off, int k) { return reinterpret_cast<const double *>(base + off + k * L::WROW) + warp * TMA_W + cl; };
     auto st4 = [&](int f, int row, const float (&v)[4]) {
         *reinterpret_cast<float4 *>(a.out[f] + row * pitch + c0) = make_float4(v[0], v[1], v[2], v[3]);
     };
@@ -281,10 +306,17 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
             issue(q + 2);
             issued = q + 2;
         }
+        if constexpr (ENERGY)
+            if (threadIdx.x == 0 && q >= 1) {   // the stress rows' weights: step q - 1 has read their slot
+                fence_proxy_async();
+                issue_sw(q);
+            }
         for (int G = waited + 1; G <= q + 1 && !bad; G++) {
             bad = !mbar_wait(bar + G % NB, (unsigned)((G / NB) & 1), TMA_WAIT_LIMIT);
             if (!bad) waited = G;
         }
+        if constexpr (ENERGY)
+            if (!bad) bad = !mbar_wait(bar + NB, (unsigned)(q & 1), TMA_WAIT_LIMIT);   // velocity rows' weights
         // 3-block rings: blocks q, q + 1; other loaded rings: block q (slot sl); new-velocity
         // rings: block q (slot s2) and q - 1 (s2p)
         const int s3a = q % R3, s3b = (q + 1) % R3, sl = q % R2, s2 = q & 1, s2p = s2 ^ 1;
@@ -332,7 +364,7 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                     for (int e = 0; e < 4; e++) nf = __fmaf_rn(v[e], 0.f, nf);
                     if (nr > 0 || rmany) record(F_MN, j, v);
                     if constexpr (ENERGY) {
-                        const double *wr = wrowp(0, sl * 4 + warp) + cl;
+                        const double *wr = wrow(L::o_vw, 0);
 #pragma unroll
                         for (int e = 0; e < 4; e++) E.k = add(E.k, mul(mul((double)v[e], wr[e]), (double)v[e]));
                     }
@@ -371,7 +403,7 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                     for (int e = 0; e < 4; e++) nf = __fmaf_rn(v[e], 0.f, nf);
                     if (nr > 0 || rmany) record(F_NM, j, v);
                     if constexpr (ENERGY) {
-                        const double *wr = wrowp(1, sl * 4 + warp) + cl;
+                        const double *wr = wrow(L::o_vw, 1);
 #pragma unroll
                         for (int e = 0; e < 4; e++) E.k = add(E.k, mul(mul((double)v[e], wr[e]), (double)v[e]));
                     }
@@ -382,9 +414,16 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
             bad = true;
             break;
         }
+        if constexpr (ENERGY) {
+            if (threadIdx.x == 0 && q + 1 < Q) {   // the next block's velocity-row weights: this step has read their slot
+                fence_proxy_async();
+                issue_vw(q + 1);
+            }
+            bad = !mbar_wait(bar + NB + 1, (unsigned)(q & 1), TMA_WAIT_LIMIT);   // stress rows' weights
+        }
         // ---- stresses of row i = j - 2 (window row warp of the 3-block rings; new-velocity rows
         // relative to x0 - 2 + 4q: i is warp - 2)
-        if (core && i >= x0 && i < x1) {
+        if (!bad && core && i >= x0 && i < x1) {
             const int ir = warp - 2;
             {   // NN: x from new MN rows i-2..i+1, y from new NM row i (taps c-2..c+1)
                 const float4 m0 = lds4(vr(L::o_vmn, ir - 2) + cl), m1 = lds4(vr(L::o_vmn, ir - 1) + cl),
@@ -416,7 +455,7 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                 for (int e = 0; e < 4; e++) nf = __fmaf_rn(v[e], 0.f, nf);
                 if (nr > 0 || rmany) record(F_NN, i, v);
                 if constexpr (ENERGY) {
-                    const double *wr = wrowp(2, sl * 4 + warp) + cl;
+                    const double *wr = wrow(L::o_sw, 0);
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
                         E.p0 = add(E.p0, mul(mul((double)f4(old, e), wr[e]), (double)f4(old, e)));
@@ -468,7 +507,7 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                     record(F_MM1, i, s1);
                 }
                 if constexpr (ENERGY) {
-                    const double *w3r = wrowp(3, sl * 4 + warp) + cl, *w4r = wrowp(4, sl * 4 + warp) + cl;
+                    const double *w3r = wrow(L::o_sw, 1), *w4r = wrow(L::o_sw, 2);
 #pragma unroll
                     for (int e = 0; e < 4; e++) {
                         const double a0 = f4(o0, e), a1 = f4(o1, e), b0 = s0[e], b1 = s1[e];
@@ -482,12 +521,19 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
                 }
             }
         }
-        __syncthreads();
+        if constexpr (ENERGY) {
+            if (__syncthreads_or(bad)) {   // (a weight copy that timed out ends the item in every thread)
+                bad = true;
+                break;
+            }
+        } else {
+            __syncthreads();
+        }
     }
     if (nf != 0.f) atomicOr(a.flags, FLAG_NONFINITE);
     if (!bad) {   // every copy has landed and every thread is past the last barrier
         if (threadIdx.x == 0)
-            for (int k = 0; k < NB; k++) mbar_inval(bar + k);
+            for (int k = 0; k < L::NBW; k++) mbar_inval(bar + k);
         return true;
     }
     {
@@ -499,10 +545,14 @@ __device__ bool tma_strip_cta(const FusedArgs<float, float> &a, const TmaMaps &m
             // was issued)
             for (int G = issued - NB + 1 > 0 ? issued - NB + 1 : 0; G <= issued; G++)
                 mbar_wait(bar + G % NB, (unsigned)((G / NB) & 1), TMA_WAIT_LIMIT);
+            if constexpr (ENERGY) {   // and the last block of each weight set
+                if (vw_last >= 0) mbar_wait(bar + NB, (unsigned)(vw_last & 1), TMA_WAIT_LIMIT);
+                if (sw_last >= 0) mbar_wait(bar + NB + 1, (unsigned)(sw_last & 1), TMA_WAIT_LIMIT);
+            }
         }
         __syncthreads();
         if (threadIdx.x == 0)
-            for (int k = 0; k < NB; k++) mbar_inval(bar + k);
+            for (int k = 0; k < L::NBW; k++) mbar_inval(bar + k);
         return false;
     }
 }
@@ -583,7 +633,7 @@ __global__ void __launch_bounds__(FS_THREADS_MAX, fs_min_blocks<float, ENERGY>()
 }
 
 template <bool ENERGY, bool Q16 = false, bool WITEMS = false>
-__global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 2 : 4)
+__global__ void __launch_bounds__(FS_THREADS_MAX, ENERGY ? 3 : 4)
     k_elastic_tma(FusedArgs<float, float> a, const __grid_constant__ TmaMaps maps)
 {
     extern __shared__ __align__(128) unsigned char tma_smem_raw[];
