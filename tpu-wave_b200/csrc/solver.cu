@@ -1064,13 +1064,14 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
         // selects it / the per-warp kernel for every handle (for comparisons); its work items and
         // side segments have TW_TMA_SEG_ROWS / TW_TMA_SIDE_ROWS rows (below).
         const int nts = tma_strips(My);
-        s->q16 = d.coef_fp16 == 2;
+        const bool want_q16 = d.coef_fp16 == 2;   // (the codes exist only where the TMA step reads them)
         if (d.precision == TW_FP32 && d.cpst == TW_CPST_00 && d.coef_fp16 != 1 && !s->slab && !(s->bnd & BND_X_IF) &&
-            s->n_int_seg > 0 && nts > 0 &&
-            (s->q16 || env_int("TW_TMA", (!d.energy || (long)Mx * My < (1L << 25)) ? 1 : 0) != 0)) {
+            s->n_int_seg > 0 && nts > 0 && s->tile_rows == TMA_TILE_ROWS &&   // (the strips' launch holds this tile)
+            (want_q16 || env_int("TW_TMA", (!d.energy || (long)Mx * My < (1L << 25)) ? 1 : 0) != 0)) {
             int n_sm = 148;
             cudaDeviceGetAttribute(&n_sm, cudaDevAttrMultiProcessorCount, d.device);
             s->tma = true;
+            s->q16 = want_q16;
             s->w_int_seg = s->n_int_seg;
             s->w_int_cta = s->n_int_cta;
             s->n_tstrip = nts;
@@ -1092,7 +1093,6 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             s->n_int_seg = std::max(1, std::min(max_seg, s->int_rows / side_rows));
             s->n_int_cta = (s->n_int_seg * s->n_ostrip + FS_WARPS - 1) / FS_WARPS;
             s->n_tcta = s->n_tseg * s->n_tstrip;
-            if (s->tile_rows != TMA_TILE_ROWS) return fail(TW_ERR_INVALID);   // (the strips' launch holds this tile)
             e = prepare_tma<float, float>();
             if (e != cudaSuccess) return fail(cuda_fail(e, "cudaFuncSetAttribute"));
             if ((e = cudaStreamCreateWithFlags(&s->st_side, cudaStreamNonBlocking)) != cudaSuccess ||
