@@ -393,15 +393,16 @@ def run_reference_arm(args, dist: Dist):
 
 def reference_gpu_executable():
     """The reference's own GPU program (nvcc_device_FDM_2D.cu, unmodified, built for sm_100a) on
-    the 2048^2 grid at the workload's dt, energy on as it requires: ms per step from two runs of
-    200 and 1200 steps (context beside the CPU arm, not its value)."""
+    the 2048^2 grid at the workload's dt, energy on as it requires: ms per step from runs of 200
+    and 2200 steps (the fastest of two each, after a warm-up run; context beside the CPU arm, not
+    its value)."""
     import shutil
     if shutil.which("nvidia-smi") is None:
         return {"unavailable": "no GPU visible"}
     try:
         from oracle import ref_gpu_timing
         dt = float(build_model(0, MX)[3])
-        rec = ref_gpu_timing.time_reference_gpu(MX, DEN_DX, dt, F0, DELAY, (200, 1200))
+        rec = ref_gpu_timing.time_reference_gpu(MX, DEN_DX, dt, F0, DELAY, (200, 2200))
     except Exception as e:  # a failed run is reported, not fatal to the CPU arm
         return {"unavailable": f"{type(e).__name__}: {e}"[:200]}
     return rec if rec is not None else {"unavailable": "oracle/_ref/twref_elastic_gpu_f32 not built"}

@@ -18,7 +18,7 @@ MM points, dt (passed in) and the Ricker parameters of the 2048^2 elastic worklo
 program's own constant medium (stable at that dt, which was set for a faster medium; the work of
 a step does not depend on the medium's values).
 
-Usage: python oracle/ref_gpu_timing.py --n 2048 --dt 1.2e-4 --steps 200 1200 [--out file.json]
+Usage: python oracle/ref_gpu_timing.py --n 2048 --dt 1.2e-4 --steps 200 2200 [--out file.json]
 """
 import argparse
 import json
@@ -80,21 +80,31 @@ def energy_tail(root: str):
     return None
 
 
-def time_reference_gpu(n: int, den: int, dt: float, f0: float, delay: float, steps=(200, 1200), logdir: str = ""):
-    """The record of one timing (two runs); None when the executable is not built."""
+def time_reference_gpu(n: int, den: int, dt: float, f0: float, delay: float, steps=(200, 2200), logdir: str = "",
+                       repeats: int = 2):
+    """The record of one timing; None when the executable is not built. A first run of the
+    shorter length is discarded (device and file-system warm-up); each length then runs
+    `repeats` times and the fastest counts, since set-up and write-out vary by seconds between
+    runs and would otherwise swamp the difference."""
     if not os.path.exists(BIN):
         return None
     medium = f"grid{n}"
-    times, energies = [], []
-    for nt in steps:
+
+    def one(nt, tag):
         root = tempfile.mkdtemp(prefix="twref_gpu_")
         try:
             write_inputs(os.path.join(root, "data", medium), n, den, dt, f0, delay)
-            log = os.path.join(logdir or root, f"ref_gpu_{n}_{nt}.log")
-            times.append(run_once(root, medium, nt, log))
-            energies.append(energy_tail(root))
+            log = os.path.join(logdir or root, f"ref_gpu_{n}_{nt}_{tag}.log")
+            return run_once(root, medium, nt, log), energy_tail(root)
         finally:
             shutil.rmtree(root, ignore_errors=True)
+
+    one(steps[0], "warmup")
+    times, energies = [], []
+    for nt in steps:
+        runs = [one(nt, str(r)) for r in range(repeats)]
+        times.append(min(t for t, _ in runs))
+        energies.append(runs[-1][1])
     n1, n2 = steps
     ms = (times[1] - times[0]) / (n2 - n1) * 1e3
     rec = {"program": "nvcc_device_FDM_2D.cu (reference, unmodified, sm_100a, FP32 fields)",
@@ -102,10 +112,13 @@ def time_reference_gpu(n: int, den: int, dt: float, f0: float, delay: float, ste
            "medium": "the program's own constant medium (rho 1, vp 2, vs 1)",
            "steps": [n1, n2], "wall_s": [round(t, 3) for t in times],
            "ms_per_step": round(ms, 4), "gpt_per_s": round(n * n / (ms * 1e-3) / 1e9, 4),
-           "method": "difference of two runs' wall-clock times (set-up and write-out cancel)",
+           "method": f"difference of the fastest of {repeats} runs' wall-clock times at each length, after a "
+                     "discarded warm-up run (set-up and write-out cancel)",
            "last_energy_record": energies}
     if any(e is not None and not math.isfinite(e) for e in energies):
         rec["warning"] = "non-finite energy record"
+    if ms <= 0:
+        return {"unavailable": f"run-to-run variance exceeded the extra steps' time (wall {times})"}
     return rec
 
 
@@ -116,7 +129,7 @@ def main():
     ap.add_argument("--dt", type=float, required=True)
     ap.add_argument("--f0", type=float, default=15.0)
     ap.add_argument("--delay", type=float, default=0.1)
-    ap.add_argument("--steps", type=int, nargs=2, default=[200, 1200])
+    ap.add_argument("--steps", type=int, nargs=2, default=[200, 2200])
     ap.add_argument("--out", default="")
     ap.add_argument("--logdir", default="")
     a = ap.parse_args()
