@@ -95,3 +95,28 @@ def test_reference_example_files(tw):
     pts = tw.io_read_srcrcv(os.path.join(REF_DATA, "SrcRcv.txt"))
     assert [(p.src_index, p.rcv_index) for p in pts] == [(1, -1), (1, 1)]
     assert (pts[0].type_x, pts[0].type_y, pts[0].num_y, pts[0].den_y, pts[0].num_x, pts[0].den_x) == (b"N", b"M", 401, 250, 20, 250)
+
+
+def test_reference_gpu_program_inputs(tw, tmp_path):
+    """The InputFile.txt and SrcRcv.txt that oracle/ref_gpu_timing.py writes for the reference's
+    own GPU program read back, through the readers of the reference's formats, as the 2048^2
+    workload meant: grid and spacing, dt = MAXdt x CFL 1, the Ricker parameters, the source on the
+    centre MM point and 16 receivers on MM points."""
+    from oracle import ref_gpu_timing as rg
+    dt = 0.00012871690627155345
+    rg.write_inputs(str(tmp_path), 2048, 500, dt, 15.0, 0.1)
+    r = tw.io_read_input(str(tmp_path / "InputFile.txt"))
+    assert (r.Mx, r.My, r.Mx_prmt, r.My_prmt) == (2048, 2048, 2048, 2048)
+    assert (r.num_dx, r.den_dx, r.num_dxM, r.den_dxM) == (1, 500, 1, 500)
+    assert r.dt == dt and r.central_f == 15.0 and r.time_delay == 0.1
+    pts = tw.io_read_srcrcv(str(tmp_path / "SrcRcv.txt"))
+    assert len(pts) == 17
+    src, rcvs = pts[0], pts[1:]
+    assert (src.rcv_index, src.type_x, src.type_y) == (-1, b"M", b"M")
+    assert tw.location_to_index("M", src.num_x, src.den_x, 1, 500) == 1024
+    assert tw.location_to_index("M", src.num_y, src.den_y, 1, 500) == 1024
+    for k, q in enumerate(rcvs):
+        c = (64 + 128 * k) % 2048
+        assert (q.src_index, q.rcv_index, q.type_x, q.type_y) == (1, k + 1, b"M", b"M")
+        assert tw.location_to_index("M", q.num_x, q.den_x, 1, 500) == c
+        assert tw.location_to_index("M", q.num_y, q.den_y, 1, 500) == c
