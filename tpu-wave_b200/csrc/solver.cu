@@ -1080,10 +1080,12 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             s->n_ostrip = 1 + (int)((My + 1 - s->y_tma_end + FS_WARP_CORE - 1) / FS_WARP_CORE);
             // the boundary and warp-strip work in the strips' launch (one launch a step) or beside it
             s->tma_witems = env_int("TW_TMA_WITEMS", (long)Mx * My < (1L << 25) ? 1 : 0) != 0;
-            // work items of about TW_TMA_SEG_ROWS rows for the persistent TMA CTAs (default 24 for
-            // one launch a step, 32 beside a side launch: at 2048^2 / 4096^2, 24 rows gave 63.1 /
-            // 183.9 us a step against 63.4 / 186.9 for 32 and 65.3 / 187.4 for 48)
-            const int seg_rows = std::max(8, env_int("TW_TMA_SEG_ROWS", s->tma_witems ? 24 : 32));
+            // work items of about TW_TMA_SEG_ROWS rows for the persistent TMA CTAs. Measured, us a
+            // step at 16 / 20 / 24 / 32 / 40 rows: 2048^2 61.65 / 61.3 / 63.3 / 63.4 / -, 4096^2
+            // 195.6 / 188.5 / 184.8 / 186.9 / -, 8192^2 (side launch) - / - / 664.0 / 679.7 / 690.1,
+            // 8192^2 with 16-bit coefficient codes - / - / 671.4 / 646.3 / 634.0
+            const int seg_def = s->tma_witems ? ((long)Mx * My <= (1L << 22) ? 20 : 24) : (s->q16 ? 40 : 24);
+            const int seg_rows = std::max(8, env_int("TW_TMA_SEG_ROWS", seg_def));
             const int max_seg = std::max(1, s->int_rows / 8);
             s->n_tseg = std::max(1, std::min(max_seg, (s->int_rows + seg_rows / 2) / seg_rows));
             (void)n_sm;
