@@ -1083,8 +1083,10 @@ int create_impl(tw_solver **out, const tw_grid_desc *desc, const SlabSpec &sl)
             // work items of about TW_TMA_SEG_ROWS rows for the persistent TMA CTAs. Measured, us a
             // step at 16 / 20 / 24 / 32 / 40 rows: 2048^2 61.65 / 61.3 / 63.3 / 63.4 / -, 4096^2
             // 195.6 / 188.5 / 184.8 / 186.9 / -, 8192^2 (side launch) - / - / 664.0 / 679.7 / 690.1,
-            // 8192^2 with 16-bit coefficient codes - / - / 671.4 / 646.3 / 634.0
-            const int seg_def = s->tma_witems ? ((long)Mx * My <= (1L << 22) ? 20 : 24) : (s->q16 ? 40 : 24);
+            // 8192^2 with 16-bit coefficient codes - / - / 671.4 / 646.3 / 634.0; with the energy
+            // on, 2048^2 99.9 / 97.7 / 97.7 / 95.8 / 102.3
+            const bool small = (long)Mx * My <= (1L << 22);
+            const int seg_def = s->tma_witems ? (small ? (d.energy ? 32 : 20) : 24) : (s->q16 ? 40 : 24);
             const int seg_rows = std::max(8, env_int("TW_TMA_SEG_ROWS", seg_def));
             const int max_seg = std::max(1, s->int_rows / 8);
             s->n_tseg = std::max(1, std::min(max_seg, (s->int_rows + seg_rows / 2) / seg_rows));
